@@ -1,0 +1,382 @@
+"""Benchmark of the sparse x dense execute path on B200.
+
+Default workload (N=1): FP64 SELL-C-sigma SpMV on the power-law matrix
+(n = 4,194,304 rows, Zipf(2) row lengths clipped to [1, 4096] with mean 16,
+uniform unique columns, N(0,1) values, x ~ U[-1,1], seed 1), C and sigma
+picked by the exhaustive autotuner, compared with the plain CSR kernel on
+the same matrix. A step is one y = A*x over the whole matrix with inputs
+resident in HBM (889 MB of algorithmic traffic: larger than the 126 MB L2,
+so no flush is needed between steps).
+
+Reported:
+  value      algorithmic GB/s of the tuned kernel (x, y and the matrix
+             counted once, SELL padding not counted), summed over ranks;
+  e2e        the same metric through the drop-in C call
+             perflibs_spmv_exec_d with host (pinned) x and y: H2D of x and
+             D2H of y inside every timed step;
+  roofline   the dominant kernel's achieved GB/s vs the measured HBM peak;
+  cpu_baseline  the reference library (compiled from its own sources,
+             OpenMP on all host cores) on the same matrix, same metric.
+
+--impl reference times only the reference CPU implementation.
+Multi-GPU (torchrun): independent replicas, one per GPU (the path needs no
+exchange), max time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from perf_libs_sparse_b200 import workloads as W  # noqa: E402
+
+FALLBACK_HBM_GBS = 6650.0
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
+        os.environ.get("LOCAL_RANK", "0"))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for nm, v in zip(names, s[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def load_traffic(workload: str):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get(workload)
+    return None
+
+
+def make_c2():
+    m, n, rp, c, v = W.zipf_rows(4_194_304, seed=1)
+    x = W.uniform_vector(n, 1)
+    return m, n, rp, c, v, x
+
+
+# ------------------------------------------------------------------ CPU leg
+
+
+def cpu_reference_spmv(m, n, rp, c, v, x, reps: int, budget_s: float = 20.0):
+    """The reference library on all host cores: create, hint MANY, optimize
+    (its auditioner), then repeated perflibs_spmv_exec_d. Returns (GB/s,
+    seconds per exec, optimize seconds, threads, kind, sample)."""
+    import oracle
+
+    threads = os.cpu_count() or 1
+    kind = "reference" if oracle.ref_available() else "port"
+    bytes_ = W.algorithmic_bytes_spmv(m, n, int(rp[-1]), 8, 8, False)
+    y = np.zeros(m)
+    if kind == "reference":
+        A = oracle.RefMatrix.csr(m, n, rp, c, v)
+        A.hint(60, 300)
+        A.hint(80, 420)
+        t0 = time.perf_counter()
+        A.optimize()
+        t_opt = time.perf_counter() - t0
+        A.spmv(x, y)
+        times = []
+        t_start = time.perf_counter()
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            A.spmv(x, y)
+            times.append(time.perf_counter() - t0)
+            if time.perf_counter() - t_start > budget_s:
+                break
+        fmt = A.format()
+        A.destroy()
+        sample = (f"full matrix, {len(times)} perflibs_spmv_exec_d calls after perflibs_spmv_optimize "
+                  f"(audition chose format {fmt[0]}, C={fmt[1]}, sigma={fmt[2]}); OMP threads={threads}")
+    else:
+        t_opt = 0.0
+        oracle.csr_spmv(rp, c, v, x, y=y)
+        times = []
+        t_start = time.perf_counter()
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            oracle.csr_spmv(rp, c, v, x, y=y)
+            times.append(time.perf_counter() - t0)
+            if time.perf_counter() - t_start > budget_s:
+                break
+        sample = f"full matrix, {len(times)} CSR SpMV calls of the oracle port; OMP threads={threads}"
+    sec = statistics.median(times)
+    return bytes_ / sec / 1e9, sec, t_opt, threads, kind, sample
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    m, n, rp, c, v, x = make_c2()
+    reps = max(1, args.warmup + args.steps)
+    gbs, sec, t_opt, threads, kind, sample = cpu_reference_spmv(m, n, rp, c, v, x, reps, budget_s=120.0)
+    line = {
+        "metric": "SpMV GB/s (algorithmic bytes), FP64, power-law matrix",
+        "value": gbs, "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "C2 power-law SpMV n=4194304 nnz=%d" % int(rp[-1]), "optimize_s": t_opt},
+        "impl": "reference",
+        "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------ GPU leg
+
+
+def run_b200(args):
+    import torch
+
+    import perf_libs_sparse_b200 as pls
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+
+    m, n, rp, c, v, x = make_c2()
+    nnz = int(rp[-1])
+    bytes_step = W.algorithmic_bytes_spmv(m, n, nnz, 8, 8, False)
+
+    stream = torch.cuda.Stream(device=dev)
+    sp = stream.cuda_stream
+
+    # Plain CSR baseline (the default kernel, no tuning).
+    A_plain = pls.SpMat.csr(m, n, rp, c, v)
+    A_plain.set_stream(sp)
+    A_plain.hint(pls.HINT_SPMV_INVOCATIONS, pls.INVOCATIONS_SINGLE)
+    assert A_plain.optimize() == 0
+
+    # Tuned: the exhaustive autotuner picks kernel family, C, sigma, TPR.
+    A = pls.SpMat.csr(m, n, rp, c, v)
+    A.set_stream(sp)
+    A.hint(pls.HINT_SPMV_OPERATION, pls.OPERATION_NOTRANS)
+    A.hint(pls.HINT_SPMV_INVOCATIONS, pls.INVOCATIONS_MANY)
+    t0 = time.perf_counter()
+    assert A.optimize() == 0
+    t_opt = time.perf_counter() - t0
+    cfg = A.config()
+
+    xd = torch.tensor(x, device=dev)
+    yd = torch.zeros(m, dtype=torch.float64, device=dev)
+
+    def step(M):
+        M.spmv_dev(xd.data_ptr(), yd.data_ptr(), 1.0, 0.0, sp)
+
+    def timed(M, K, Wm):
+        with torch.cuda.stream(stream):
+            for _ in range(Wm):
+                step(M)
+            torch.cuda.synchronize()
+            if world > 1:
+                torch.distributed.barrier()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(K):
+                step(M)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms / K
+
+    K, Wm = args.steps, max(args.warmup, 3)
+    # Keep the GPU busy ~0.5 s before the timed region so that the clock
+    # samples see the kernel under load.
+    soak = max(1, int(0.5 / max(bytes_step / 6.0e12, 1e-6)))
+    with ClockSampler(local) as clk:
+        timed(A, soak, 1)
+        ms_tuned = timed(A, K, Wm)
+    ms_plain = timed(A_plain, K, Wm)
+
+    # Parity of the timed result (full size) against the oracle.
+    import oracle
+
+    y_gpu = yd.cpu().numpy()
+    step(A)
+    torch.cuda.synchronize()
+    y_gpu = yd.cpu().numpy()
+    y_ref = oracle.csr_spmv(rp, c, v, x)
+    scale = oracle.csr_absdot(rp, c, v, x)
+    den = np.maximum(np.abs(y_ref), scale)
+    den[den == 0] = 1
+    max_rel = float((np.abs(y_gpu - y_ref) / den).max())
+
+    # End to end through the drop-in call with pinned host buffers.
+    xh = torch.tensor(x).pin_memory()
+    yh = torch.zeros(m, dtype=torch.float64).pin_memory()
+    lib = pls.lib()
+    import ctypes as C
+
+    xp, yp = C.c_void_p(xh.data_ptr()), C.c_void_p(yh.data_ptr())
+    for _ in range(2):
+        lib.perflibs_spmv_exec_d(pls.OPERATION_NOTRANS, 1.0, A.h, xp, 0.0, yp)
+    Ke = max(3, min(K, 30))
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(Ke):
+        st = lib.perflibs_spmv_exec_d(pls.OPERATION_NOTRANS, 1.0, A.h, xp, 0.0, yp)
+        assert st == 0
+    e2e_s = (time.perf_counter() - t0) / Ke
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    hbm, peak_kind = peaks()
+    achieved = bytes_step / (ms_tuned * 1e-3) / 1e9
+    info = A.exec_info()
+    kernels_per_step = info["kernels_per_spmv"]
+    workload = f"C2 power-law SpMV n={m} nnz={nnz}"
+    line = {
+        "metric": "SpMV GB/s (algorithmic bytes) vs B200 HBM roofline, FP64, tuned vs plain CSR",
+        "value": achieved * world,
+        "unit": "GB/s",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": Wm,
+        "ms_per_step": ms_tuned,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {
+            "workload": workload,
+            "format": {0: "CSR", 1: "SELL-C-sigma", 2: "CSR-split"}[cfg["kind"]],
+            "C": cfg["C"], "sigma": cfg["sigma"], "tpr": cfg["tpr"], "col_bytes": cfg["col_bytes"],
+            "sell_items": info["n_items"], "sell_split_chunks": info["n_split"],
+            "algorithmic_bytes_per_step": bytes_step,
+            "l2": "inputs (889 MB) exceed the 126 MB L2; no flush between steps",
+            "optimize_s": t_opt,
+            "parallelism": f"replicas x{world}",
+        },
+        "plain_csr": {"value": bytes_step / (ms_plain * 1e-3) / 1e9 * world, "ms_per_step": ms_plain},
+        "speedup_vs_plain_csr": ms_plain / ms_tuned,
+        "max_rel_err": max_rel,
+        "e2e": {"value": bytes_step / e2e_s / 1e9 * world, "unit": "GB/s",
+                "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": m * 8, "ms_per_step": e2e_s * 1e3},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "peak_source": peak_kind,
+                     "traffic": load_traffic("c2_spmv_fp64")},
+        "gpu_launches": K * kernels_per_step,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        os.environ.setdefault("OMP_PROC_BIND", "close")
+        gbs, sec, t_opt_cpu, threads, kind, sample = cpu_reference_spmv(m, n, rp, c, v, x, reps=40)
+        line["cpu_baseline"] = {"value": gbs, "unit": "GB/s", "cores": threads, "kind": kind,
+                                "sample": sample, "optimize_s": t_opt_cpu, "ms_per_step": sec * 1e3}
+    if rank == 0:
+        print(json.dumps(line))
+    A.destroy()
+    A_plain.destroy()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

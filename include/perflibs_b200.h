@@ -1,0 +1,154 @@
+/*
+ * perflibs_b200.h — extensions of libplsparse_b200 beyond the reference
+ * interface. None of these has a counterpart in the reference library's
+ * include/perflibs_sparse.h unless a comment says so; the drop-in entry
+ * points are in perflibs_sparse.h.
+ *
+ * Device pointers: every *_dev entry point takes device (HBM) pointers and
+ * a CUDA stream (a cudaStream_t passed as void*; NULL = the library's own
+ * stream for the handle's device). Calls are asynchronous with respect to
+ * the host; results are ready when the stream reaches them.
+ */
+#ifndef PERFLIBS_B200_H
+#define PERFLIBS_B200_H
+
+#include <stdint.h>
+
+#include "perflibs_sparse.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- device-pointer execution ----------------------------------------
+ * Same semantics as perflibs_spmv_exec_{s,d} (y = alpha*op(A)*x + beta*y),
+ * on device arrays, without host copies or synchronisation. */
+perflibs_status_t perflibs_b200_spmv_exec_d_dev(
+    enum perflibs_sparse_hint_value trans, double alpha, perflibs_spmat_t A,
+    const double *x, double beta, double *y, void *stream);
+perflibs_status_t perflibs_b200_spmv_exec_s_dev(
+    enum perflibs_sparse_hint_value trans, float alpha, perflibs_spmat_t A,
+    const float *x, float beta, float *y, void *stream);
+
+/* C = alpha*A*B + beta*C for a sparse A (NOTRANS), row-major dense device
+ * B (ldb >= k) and C (ldc >= k) with k columns. beta == 0 overwrites C. */
+perflibs_status_t perflibs_b200_spmm_exec_d_dev(double alpha,
+                                                perflibs_spmat_t A,
+                                                const double *B, int64_t ldb,
+                                                int32_t k, double beta,
+                                                double *C, int64_t ldc,
+                                                void *stream);
+perflibs_status_t perflibs_b200_spmm_exec_s_dev(float alpha, perflibs_spmat_t A,
+                                                const float *B, int64_t ldb,
+                                                int32_t k, float beta,
+                                                float *C, int64_t ldc,
+                                                void *stream);
+
+/* ---- value storage (opt-in reduced precision) -------------------------
+ * NATIVE keeps values in the handle's API type (FP64 for _d handles) and
+ * accumulates in it. FP32 / BF16 store values in that type and accumulate
+ * in FP32; x, y, B and C keep the API type. Takes effect at the next
+ * optimize or exec. */
+enum perflibs_b200_storage {
+  PERFLIBS_B200_STORAGE_NATIVE = 0,
+  PERFLIBS_B200_STORAGE_FP32 = 1,
+  PERFLIBS_B200_STORAGE_BF16 = 2
+};
+perflibs_status_t perflibs_b200_spmat_set_storage(perflibs_spmat_t A,
+                                                  int storage);
+
+/* ---- tuning ------------------------------------------------------------
+ * How perflibs_spmv_optimize picks the SpMV kernel when the SpMV
+ * invocations hint is MANY (the reference's auditioning condition,
+ * src/matvec.cpp:624-627):
+ *   EXHAUSTIVE: time every candidate (CSR threads-per-row x SELL C x sigma)
+ *               with CUDA events and keep the fastest;
+ *   SELECTOR:   ask the learned selector (perflibs_b200_selector_load) and
+ *               fall back to EXHAUSTIVE when none is loaded;
+ *   NONE:       keep the default CSR kernel. */
+enum perflibs_b200_tuner {
+  PERFLIBS_B200_TUNE_EXHAUSTIVE = 0,
+  PERFLIBS_B200_TUNE_SELECTOR = 1,
+  PERFLIBS_B200_TUNE_NONE = 2
+};
+perflibs_status_t perflibs_b200_spmat_set_tuner(perflibs_spmat_t A, int mode);
+
+/* Kernel families. */
+enum perflibs_b200_kind {
+  PERFLIBS_B200_KIND_CSR = 0,  /* threads-per-row vector CSR */
+  PERFLIBS_B200_KIND_SELL = 1, /* SELL-C-sigma, C in {8, 16, 32} */
+  PERFLIBS_B200_KIND_CSR_SPLIT = 2 /* CSR with long rows split across CTAs */
+};
+
+/* Force a kernel configuration for the next optimize (the role of the
+ * reference's internal set_C / set_sigma knobs, src/matrix_state.cpp:
+ * 434-457). sigma is in rows: 0 (no sort) or a multiple of C. tpr 0 picks
+ * by mean row length. */
+perflibs_status_t perflibs_b200_spmat_force_config(perflibs_spmat_t A,
+                                                   int kind, int C, int sigma,
+                                                   int tpr);
+
+/* The active configuration. */
+perflibs_status_t perflibs_b200_spmat_get_config(perflibs_spmat_t A,
+                                                 int *kind, int *C, int *sigma,
+                                                 int *tpr, int *col_bytes);
+
+/* Launch shape of the active NOTRANS SpMV: kernels launched per call, and
+ * for SELL-C-sigma the number of work items and of chunks split into
+ * column slices (0 when every chunk is one item). */
+perflibs_status_t perflibs_b200_spmat_exec_info(perflibs_spmat_t A,
+                                                int32_t *kernels_per_spmv,
+                                                int64_t *n_items,
+                                                int64_t *n_split);
+
+/* Timings the last exhaustive tune measured: up to `cap` rows of
+ * (kind, C, sigma, tpr) in cfg4 and milliseconds in ms. Returns the count
+ * in *count. */
+perflibs_status_t perflibs_b200_spmat_tune_table(perflibs_spmat_t A,
+                                                 int32_t cap, int32_t *cfg4,
+                                                 double *ms, int32_t *count);
+
+/* The SELL-C-sigma layout held on the device (after optimize picked SELL or
+ * after perflibs_b200_spmat_build_sell): info7 = {nC, C, sigma, col_bytes,
+ * n_full_chunks, ntidyup, size}; any array pointer may be NULL. Offsets are
+ * written with col_bytes bytes each, values in the storage type. */
+perflibs_status_t perflibs_b200_spmat_export_sell(
+    perflibs_spmat_t A, int64_t *info7, int64_t *cs, int64_t *cl,
+    int64_t *col_min, int64_t *permd2in, int64_t *in2permd, void *vals,
+    void *offsets);
+
+/* Build (or rebuild) the SELL-C-sigma layout with C and sigma and make it
+ * the active SpMV format, without timing anything. */
+perflibs_status_t perflibs_b200_spmat_build_sell(perflibs_spmat_t A, int C,
+                                                 int sigma);
+
+/* Per-handle CUDA stream for the host-pointer entry points (NULL restores
+ * the library stream). */
+perflibs_status_t perflibs_b200_spmat_set_stream(perflibs_spmat_t A,
+                                                 void *stream);
+
+/* CSR -> BSR on the device for a CSR handle: returns a new BSR handle with
+ * block size bs and the given block layout (blocks sorted by block column,
+ * zero-filled). m and n must be multiples of bs. */
+perflibs_status_t perflibs_b200_spmat_csr_to_bsr(perflibs_spmat_t A,
+                                                 int32_t bs, int layout,
+                                                 perflibs_spmat_t *out);
+
+/* BSR structure back to host arrays (malloc'ed; the caller frees). */
+perflibs_status_t perflibs_b200_spmat_export_bsr_d(
+    perflibs_spmat_t A, int32_t *bs, int32_t *nnzb, int32_t **row_ptr,
+    int32_t **col_indx, double **vals);
+
+/* Library / device information: SM count, L2 bytes, device ordinal. */
+perflibs_status_t perflibs_b200_device_info(int32_t *sm_count,
+                                            int64_t *l2_bytes,
+                                            int32_t *device);
+
+/* Version string of the library build. */
+const char *perflibs_b200_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PERFLIBS_B200_H */

@@ -1,0 +1,404 @@
+"""Python mirror of the perflibs_sparse C interface, over libplsparse_b200.so.
+
+The product is the C-ABI shared library built from ``csrc/`` (declared in
+``include/perflibs_sparse.h`` and ``include/perflibs_b200.h``). This module
+binds it with ctypes so that tests and benchmarks drive exactly the entry
+points a C caller links against: create -> hint -> optimize -> exec ->
+export -> destroy, with the reference's enum values and status codes.
+
+There is no fallback: importing works without a GPU (for symbol checks), but
+any call that needs the device raises ``PerflibsError`` when the CUDA
+library or the device is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libplsparse_b200.so")
+ROOT = os.path.dirname(HERE)
+INCLUDE_DIR = os.path.join(ROOT, "include")
+
+# ---------------------------------------------------------------- enums
+# Values of the reference interface (include/perflibs_sparse.h:67-149).
+STATUS_SUCCESS = 0
+STATUS_INPUT_PARAMETER_ERROR = 1
+STATUS_EXECUTION_FAILURE = 2
+
+HINT_STRUCTURE = 50
+HINT_SPMV_OPERATION = 60
+HINT_SPMM_OPERATION = 61
+HINT_MEMORY = 70
+HINT_SPMV_INVOCATIONS = 80
+HINT_SPMM_INVOCATIONS = 81
+
+COL_MAJOR = 90
+ROW_MAJOR = 91
+
+STRUCTURE_UNSTRUCTURED = 101
+OPERATION_NOTRANS = 300
+OPERATION_TRANS = 310
+OPERATION_CONJTRANS = 320
+INVOCATIONS_SINGLE = 400
+INVOCATIONS_FEW = 410
+INVOCATIONS_MANY = 420
+SCALAR_ONE = 500
+SCALAR_ZERO = 501
+SCALAR_ANY = 502
+NORM_INF = 1001
+NORM_FRB = 1002
+CREATE_NOCOPY = 1
+
+# Extensions (include/perflibs_b200.h).
+STORAGE_NATIVE, STORAGE_FP32, STORAGE_BF16 = 0, 1, 2
+TUNE_EXHAUSTIVE, TUNE_SELECTOR, TUNE_NONE = 0, 1, 2
+KIND_CSR, KIND_SELL, KIND_CSR_SPLIT = 0, 1, 2
+
+
+class PerflibsError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        super().__init__(f"{what}: status {status}")
+        self.status = status
+
+
+_lib = None
+
+
+def lib():
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise PerflibsError(STATUS_EXECUTION_FAILURE,
+                                f"{LIB_PATH} is missing; run perf_libs_sparse_b200.build")
+        L = C.CDLL(LIB_PATH)
+        vp, i32, i64, d, f, i = C.c_void_p, C.c_int32, C.c_int64, C.c_double, C.c_float, C.c_int
+        sig = {
+            "perflibs_spmat_create_csr_s": [vp, i32, i32, vp, vp, vp, i32],
+            "perflibs_spmat_create_csr_d": [vp, i32, i32, vp, vp, vp, i32],
+            "perflibs_spmat_create_dense_s": [vp, i, i32, i32, i32, vp, i32],
+            "perflibs_spmat_create_dense_d": [vp, i, i32, i32, i32, vp, i32],
+            "perflibs_spmat_create_bsr_s": [vp, i, i32, i32, i32, vp, vp, vp, i32],
+            "perflibs_spmat_create_bsr_d": [vp, i, i32, i32, i32, vp, vp, vp, i32],
+            "perflibs_spmat_create_null": [i32, i32],
+            "perflibs_spmat_create_identity": [i32],
+            "perflibs_spmat_destroy": [vp],
+            "perflibs_spmat_query": [vp, vp, vp, vp, vp],
+            "perflibs_spmat_hint": [vp, i, i],
+            "perflibs_spmv_optimize": [vp],
+            "perflibs_spmm_optimize": [i, i, i, vp, vp, i, vp],
+            "perflibs_spmv_exec_s": [i, f, vp, vp, f, vp],
+            "perflibs_spmv_exec_d": [i, d, vp, vp, d, vp],
+            "perflibs_spmm_exec_s": [i, i, f, vp, vp, f, vp],
+            "perflibs_spmm_exec_d": [i, i, d, vp, vp, d, vp],
+            "perflibs_spmat_update_s": [vp, i32, vp, vp, vp],
+            "perflibs_spmat_update_d": [vp, i32, vp, vp, vp],
+            "perflibs_spmat_export_csr_s": [vp, i32, vp, vp, vp, vp, vp],
+            "perflibs_spmat_export_csr_d": [vp, i32, vp, vp, vp, vp, vp],
+            "perflibs_spmat_export_dense_s": [vp, i, vp, vp, vp],
+            "perflibs_spmat_export_dense_d": [vp, i, vp, vp, vp],
+            "perflibs_spnorm_exec_s": [vp, i, vp],
+            "perflibs_spnorm_exec_d": [vp, i, vp],
+            "perflibs_spmat_print_err": [vp],
+            "perflibs_b200_spmv_exec_d_dev": [i, d, vp, vp, d, vp, vp],
+            "perflibs_b200_spmv_exec_s_dev": [i, f, vp, vp, f, vp, vp],
+            "perflibs_b200_spmm_exec_d_dev": [d, vp, vp, i64, i32, d, vp, i64, vp],
+            "perflibs_b200_spmm_exec_s_dev": [f, vp, vp, i64, i32, f, vp, i64, vp],
+            "perflibs_b200_spmat_set_storage": [vp, i],
+            "perflibs_b200_spmat_set_tuner": [vp, i],
+            "perflibs_b200_spmat_force_config": [vp, i, i, i, i],
+            "perflibs_b200_spmat_get_config": [vp, vp, vp, vp, vp, vp],
+            "perflibs_b200_spmat_tune_table": [vp, i32, vp, vp, vp],
+            "perflibs_b200_spmat_exec_info": [vp, vp, vp, vp],
+            "perflibs_b200_spmat_export_sell": [vp, vp, vp, vp, vp, vp, vp, vp, vp],
+            "perflibs_b200_spmat_build_sell": [vp, i, i],
+            "perflibs_b200_spmat_set_stream": [vp, vp],
+            "perflibs_b200_spmat_csr_to_bsr": [vp, i32, i, vp],
+            "perflibs_b200_spmat_export_bsr_d": [vp, vp, vp, vp, vp, vp],
+            "perflibs_b200_device_info": [vp, vp, vp],
+        }
+        for name, args in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = C.c_int
+        L.perflibs_spmat_create_null.restype = vp
+        L.perflibs_spmat_create_identity.restype = vp
+        L.perflibs_spmat_print_err.restype = None
+        L.perflibs_b200_version.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+_libc = C.CDLL(None)
+_libc.free.argtypes = [C.c_void_p]
+
+
+def _p(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _check(st: int, what: str):
+    if st != STATUS_SUCCESS:
+        raise PerflibsError(st, what)
+
+
+def device_info():
+    sm, l2, dev = C.c_int32(), C.c_int64(), C.c_int32()
+    _check(lib().perflibs_b200_device_info(C.byref(sm), C.byref(l2), C.byref(dev)), "device_info")
+    return {"sm_count": sm.value, "l2_bytes": l2.value, "device": dev.value}
+
+
+class SpMat:
+    """An owned perflibs_spmat_t handle."""
+
+    def __init__(self, handle, dtype):
+        self.h = C.c_void_p(handle) if not isinstance(handle, C.c_void_p) else handle
+        self.dtype = np.dtype(dtype)
+
+    # -------------------------------------------------------- creation
+    @staticmethod
+    def csr(m, n, row_ptr, col, vals, flags=0, check=True):
+        vals = np.ascontiguousarray(vals)
+        row_ptr = np.ascontiguousarray(row_ptr, np.int32)
+        col = np.ascontiguousarray(col, np.int32)
+        h = C.c_void_p()
+        fn = lib().perflibs_spmat_create_csr_s if vals.dtype == np.float32 else lib().perflibs_spmat_create_csr_d
+        st = fn(C.byref(h), m, n, _p(row_ptr), _p(col), _p(vals), flags)
+        M = SpMat(h, vals.dtype)
+        M.status = st
+        if check:
+            _check(st, "create_csr")
+        return M
+
+    @staticmethod
+    def bsr(layout, m, n, bs, row_ptr, col, vals, flags=0, check=True):
+        vals = np.ascontiguousarray(vals)
+        row_ptr = np.ascontiguousarray(row_ptr, np.int32)
+        col = np.ascontiguousarray(col, np.int32)
+        h = C.c_void_p()
+        fn = lib().perflibs_spmat_create_bsr_s if vals.dtype == np.float32 else lib().perflibs_spmat_create_bsr_d
+        st = fn(C.byref(h), layout, m, n, bs, _p(row_ptr), _p(col), _p(vals), flags)
+        M = SpMat(h, vals.dtype)
+        M.status = st
+        if check:
+            _check(st, "create_bsr")
+        return M
+
+    @staticmethod
+    def dense(layout, m, n, lda, vals, flags=0, check=True):
+        vals = np.ascontiguousarray(vals)
+        h = C.c_void_p()
+        fn = lib().perflibs_spmat_create_dense_s if vals.dtype == np.float32 else lib().perflibs_spmat_create_dense_d
+        st = fn(C.byref(h), layout, m, n, lda, _p(vals), flags)
+        M = SpMat(h, vals.dtype)
+        M.status = st
+        if check:
+            _check(st, "create_dense")
+        return M
+
+    @staticmethod
+    def null(m, n, dtype=np.float64):
+        h = lib().perflibs_spmat_create_null(m, n)
+        if not h:
+            raise PerflibsError(STATUS_INPUT_PARAMETER_ERROR, "create_null")
+        return SpMat(h, dtype)
+
+    @staticmethod
+    def identity(n, dtype=np.float64):
+        h = lib().perflibs_spmat_create_identity(n)
+        if not h:
+            raise PerflibsError(STATUS_INPUT_PARAMETER_ERROR, "create_identity")
+        return SpMat(h, dtype)
+
+    # --------------------------------------------------------- control
+    def hint(self, hint, value):
+        return lib().perflibs_spmat_hint(self.h, hint, value)
+
+    def optimize(self):
+        return lib().perflibs_spmv_optimize(self.h)
+
+    def query(self):
+        b, m, n, z = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        _check(lib().perflibs_spmat_query(self.h, C.byref(b), C.byref(m), C.byref(n), C.byref(z)), "query")
+        return b.value, m.value, n.value, z.value
+
+    def set_storage(self, mode):
+        return lib().perflibs_b200_spmat_set_storage(self.h, mode)
+
+    def set_tuner(self, mode):
+        return lib().perflibs_b200_spmat_set_tuner(self.h, mode)
+
+    def force_config(self, kind, C_=0, sigma=0, tpr=0):
+        return lib().perflibs_b200_spmat_force_config(self.h, kind, C_, sigma, tpr)
+
+    def build_sell(self, C_, sigma):
+        return lib().perflibs_b200_spmat_build_sell(self.h, C_, sigma)
+
+    def set_stream(self, stream_ptr: int):
+        return lib().perflibs_b200_spmat_set_stream(self.h, C.c_void_p(stream_ptr))
+
+    def config(self):
+        k, c, s, t, b = (C.c_int() for _ in range(5))
+        _check(lib().perflibs_b200_spmat_get_config(self.h, C.byref(k), C.byref(c), C.byref(s),
+                                                    C.byref(t), C.byref(b)), "get_config")
+        return {"kind": k.value, "C": c.value, "sigma": s.value, "tpr": t.value, "col_bytes": b.value}
+
+    def exec_info(self):
+        k, it, sp = C.c_int32(), C.c_int64(), C.c_int64()
+        _check(lib().perflibs_b200_spmat_exec_info(self.h, C.byref(k), C.byref(it), C.byref(sp)),
+               "exec_info")
+        return {"kernels_per_spmv": k.value, "n_items": it.value, "n_split": sp.value}
+
+    def tune_table(self):
+        cnt = C.c_int32()
+        lib().perflibs_b200_spmat_tune_table(self.h, 0, None, None, C.byref(cnt))
+        n = cnt.value
+        cfg = np.zeros((max(n, 1), 4), np.int32)
+        ms = np.zeros(max(n, 1))
+        lib().perflibs_b200_spmat_tune_table(self.h, n, _p(cfg), _p(ms), C.byref(cnt))
+        return cfg[:n], ms[:n]
+
+    # -------------------------------------------------------- execution
+    def spmv(self, x, y=None, alpha=1.0, beta=0.0, trans=OPERATION_NOTRANS, check=True):
+        """Host-pointer exec (the drop-in perflibs_spmv_exec_{s,d})."""
+        x = np.ascontiguousarray(x, self.dtype)
+        _, m, n, _ = self.query()
+        ylen = m if trans == OPERATION_NOTRANS else n
+        y = np.zeros(ylen, self.dtype) if y is None else y
+        fn = lib().perflibs_spmv_exec_s if self.dtype == np.float32 else lib().perflibs_spmv_exec_d
+        st = fn(trans, alpha, self.h, _p(x), beta, _p(y))
+        if check:
+            _check(st, "spmv_exec")
+        return y if check else (st, y)
+
+    def spmv_dev(self, x_ptr: int, y_ptr: int, alpha=1.0, beta=0.0, stream: int = 0,
+                 trans=OPERATION_NOTRANS):
+        fn = lib().perflibs_b200_spmv_exec_s_dev if self.dtype == np.float32 else lib().perflibs_b200_spmv_exec_d_dev
+        _check(fn(trans, alpha, self.h, C.c_void_p(x_ptr), beta, C.c_void_p(y_ptr),
+                  C.c_void_p(stream)), "spmv_exec_dev")
+
+    def spmm_dev(self, B_ptr: int, ldb: int, k: int, C_ptr: int, ldc: int, alpha=1.0, beta=0.0,
+                 stream: int = 0):
+        fn = lib().perflibs_b200_spmm_exec_s_dev if self.dtype == np.float32 else lib().perflibs_b200_spmm_exec_d_dev
+        _check(fn(alpha, self.h, C.c_void_p(B_ptr), ldb, k, beta, C.c_void_p(C_ptr), ldc,
+                  C.c_void_p(stream)), "spmm_exec_dev")
+
+    def update(self, rows, cols, vals):
+        rows = np.ascontiguousarray(rows, np.int32)
+        cols = np.ascontiguousarray(cols, np.int32)
+        vals = np.ascontiguousarray(vals, self.dtype)
+        fn = lib().perflibs_spmat_update_s if self.dtype == np.float32 else lib().perflibs_spmat_update_d
+        return fn(self.h, len(rows), _p(rows), _p(cols), _p(vals))
+
+    def norm(self, kind=NORM_INF):
+        if self.dtype == np.float32:
+            r = C.c_float()
+            st = lib().perflibs_spnorm_exec_s(self.h, kind, C.byref(r))
+        else:
+            r = C.c_double()
+            st = lib().perflibs_spnorm_exec_d(self.h, kind, C.byref(r))
+        _check(st, "spnorm")
+        return r.value
+
+    # ----------------------------------------------------------- export
+    def export_csr(self, index_base=0):
+        m, n = C.c_int32(), C.c_int32()
+        rp, ci, v = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        fn = lib().perflibs_spmat_export_csr_s if self.dtype == np.float32 else lib().perflibs_spmat_export_csr_d
+        _check(fn(self.h, index_base, C.byref(m), C.byref(n), C.byref(rp), C.byref(ci), C.byref(v)),
+               "export_csr")
+        try:
+            M = m.value
+            rpa = np.ctypeslib.as_array(C.cast(rp, C.POINTER(C.c_int32)), (M + 1,)).copy()
+            nnz = int(rpa[-1] - index_base)
+            cia = np.ctypeslib.as_array(C.cast(ci, C.POINTER(C.c_int32)), (max(nnz, 1),))[:nnz].copy()
+            ct = C.c_float if self.dtype == np.float32 else C.c_double
+            va = np.ctypeslib.as_array(C.cast(v, C.POINTER(ct)), (max(nnz, 1),))[:nnz].copy()
+        finally:
+            for p in (rp, ci, v):
+                _libc.free(p)
+        return m.value, n.value, rpa, cia, va
+
+    def export_dense(self, layout=ROW_MAJOR):
+        m, n = C.c_int32(), C.c_int32()
+        v = C.c_void_p()
+        fn = lib().perflibs_spmat_export_dense_s if self.dtype == np.float32 else lib().perflibs_spmat_export_dense_d
+        _check(fn(self.h, layout, C.byref(m), C.byref(n), C.byref(v)), "export_dense")
+        try:
+            ct = C.c_float if self.dtype == np.float32 else C.c_double
+            a = np.ctypeslib.as_array(C.cast(v, C.POINTER(ct)), (m.value * n.value,)).copy()
+        finally:
+            _libc.free(v)
+        if layout == ROW_MAJOR:
+            return a.reshape(m.value, n.value)
+        return a.reshape(n.value, m.value).T
+
+    def export_sell(self, vals_dtype=np.float64):
+        info = np.zeros(7, np.int64)
+        _check(lib().perflibs_b200_spmat_export_sell(self.h, _p(info), None, None, None, None, None,
+                                                     None, None), "export_sell")
+        nC, Cc, sg, nb, nfull, ntidy, size = (int(v) for v in info)
+        cs = np.zeros(max(nC, 1), np.int64)
+        cl = np.zeros(max(nC, 1), np.int64)
+        cm = np.zeros(max(nC, 1), np.int64)
+        p2i = np.zeros(max(nC * Cc, 1), np.int64)
+        i2p = np.zeros(max(nC * Cc, 1), np.int64)
+        v = np.zeros(max(size, 1), vals_dtype)
+        raw = np.zeros(max(size * nb, 1), np.uint8)
+        _check(lib().perflibs_b200_spmat_export_sell(self.h, _p(info), _p(cs), _p(cl), _p(cm), _p(p2i),
+                                                     _p(i2p), _p(v), _p(raw)), "export_sell")
+        odt = {1: np.int8, 2: np.int16, 4: np.int32, 8: np.int64}[nb]
+        return dict(nC=nC, C=Cc, sigma=sg, size=size, cs=cs[:nC], cl=cl[:nC], col_min=cm[:nC],
+                    permd2in=p2i[: nC * Cc], in2permd=i2p[: nC * Cc], vals=v[:size],
+                    offsets=raw[: size * nb].view(odt).astype(np.int64), col_bytes=nb,
+                    n_full_chunks=nfull, ntidyup=ntidy)
+
+    def to_bsr(self, bs, layout=ROW_MAJOR):
+        h = C.c_void_p()
+        _check(lib().perflibs_b200_spmat_csr_to_bsr(self.h, bs, layout, C.byref(h)), "csr_to_bsr")
+        return SpMat(h, self.dtype)
+
+    def export_bsr(self):
+        bs, nnzb = C.c_int32(), C.c_int32()
+        rp, ci, v = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        _check(lib().perflibs_b200_spmat_export_bsr_d(self.h, C.byref(bs), C.byref(nnzb), C.byref(rp),
+                                                      C.byref(ci), C.byref(v)), "export_bsr")
+        _, m, _, _ = self.query()
+        try:
+            mb = m // bs.value
+            rpa = np.ctypeslib.as_array(C.cast(rp, C.POINTER(C.c_int32)), (mb + 1,)).copy()
+            k = nnzb.value
+            cia = np.ctypeslib.as_array(C.cast(ci, C.POINTER(C.c_int32)), (max(k, 1),))[:k].copy()
+            e = k * bs.value * bs.value
+            va = np.ctypeslib.as_array(C.cast(v, C.POINTER(C.c_double)), (max(e, 1),))[:e].copy()
+        finally:
+            for p in (rp, ci, v):
+                _libc.free(p)
+        return bs.value, rpa, cia, va
+
+    def print_err(self):
+        lib().perflibs_spmat_print_err(self.h)
+
+    def destroy(self):
+        if self.h is not None and self.h.value:
+            lib().perflibs_spmat_destroy(self.h)
+        self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+def spmm_optimize(transA, transB, alpha_hint, A: SpMat, B: SpMat, beta_hint, Cm: SpMat):
+    return lib().perflibs_spmm_optimize(transA, transB, alpha_hint, A.h, B.h, beta_hint, Cm.h)
+
+
+def spmm_exec(transA, transB, alpha, A: SpMat, B: SpMat, beta, Cm: SpMat):
+    fn = lib().perflibs_spmm_exec_s if A.dtype == np.float32 else lib().perflibs_spmm_exec_d
+    return fn(transA, transB, alpha, A.h, B.h, beta, Cm.h)

@@ -1,0 +1,79 @@
+"""Build libplsparse_b200.so in-tree for sm_100a.
+
+Compiles every ``csrc/*.cu`` with nvcc for ``compute_100a``/``sm_100a`` (no
+other architecture), in parallel, and links the C-ABI shared library next to
+this file. The CUDA runtime is linked statically (nvcc's default), so the
+library only needs the driver at run time.
+
+Usage: python -m perf_libs_sparse_b200.build [--verbose-ptxas]
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libplsparse_b200.so")
+ROOT = os.path.dirname(HERE)
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+CFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-DNDEBUG",
+          "--expt-relaxed-constexpr", f"-I{os.path.join(ROOT, 'include')}"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _compile(src: str, verbose_ptxas: bool) -> tuple[str, str]:
+    obj = os.path.join(OBJ, os.path.basename(src).replace(".cu", ".o"))
+    cmd = [nvcc(), *ARCH, *CFLAGS, "-c", src, "-o", obj]
+    if verbose_ptxas:
+        cmd += ["-Xptxas", "-v"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
+    return obj, r.stderr
+
+
+def stale() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    for d in (CSRC, os.path.join(ROOT, "include")):
+        for f in os.listdir(d):
+            if os.path.getmtime(os.path.join(d, f)) > t:
+                return True
+    return False
+
+
+def build(verbose_ptxas: bool = False, force: bool = False) -> str:
+    if not force and not stale():
+        return LIB
+    os.makedirs(OBJ, exist_ok=True)
+    srcs = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
+    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
+        results = list(ex.map(lambda s: _compile(s, verbose_ptxas), srcs))
+    if verbose_ptxas:
+        for obj, log in results:
+            sys.stderr.write(log)
+    objs = [o for o, _ in results]
+    tmp = LIB + ".tmp"
+    cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose_ptxas="--verbose-ptxas" in sys.argv, force="--force" in sys.argv))

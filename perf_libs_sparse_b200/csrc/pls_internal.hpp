@@ -1,0 +1,341 @@
+// Internal types of libplsparse_b200: the matrix handle, device buffers,
+// kernel configurations and the launchers each .cu file provides.
+//
+// Data layout in HBM (all device arrays are 0-based; the user's index base is
+// remembered only for export):
+//   CSR   row_ptr int32[m+1], col int32[nnz], vals V[nnz]
+//   SELL  cs int64[nC] (chunk start), cl int32[nC] (chunk width),
+//         col_min int32[nC], permd2in int32[nC*C] (-1 = padding row),
+//         in2permd int32[m], vals V[size], offsets u8/u16/u32/u64[size]
+//         (column offset from col_min, width = col_bytes), column-major
+//         within each chunk: element (row r, column j) of chunk c sits at
+//         cs[c] + j*C + r. This is the reference's SELL-C-sigma layout
+//         (src/sell_c_sigma.hpp:43-104) element for element.
+//   BSR   row_ptr int32[mb+1], col int32[nnzb], vals V[nnzb*bs*bs] in the
+//         user's block layout (row- or column-major blocks)
+//   DENSE vals T[m*n] packed (lda = n row-major, lda = m column-major)
+// V is the value storage type: the API type (float / double) by default, or
+// float / bf16 under the reduced-precision storage modes.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/perflibs_b200.h"
+#include "../../include/perflibs_sparse.h"
+
+namespace pls {
+
+// ------------------------------------------------------------ errors
+
+struct Error : std::runtime_error {
+  perflibs_status_t status;
+  Error(perflibs_status_t s, const std::string &m)
+      : std::runtime_error(m), status(s) {}
+};
+
+#define PLS_CUDA(call)                                                         \
+  do {                                                                         \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess)                                                     \
+      throw ::pls::Error(PERFLIBS_STATUS_EXECUTION_FAILURE,                    \
+                         std::string(#call) + ": " + cudaGetErrorString(e_) + \
+                             " (" + __FILE__ + ":" + std::to_string(__LINE__) +\
+                             ")");                                             \
+  } while (0)
+
+#define PLS_LAUNCH_CHECK() PLS_CUDA(cudaGetLastError())
+
+// ------------------------------------------------------------ device buffer
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  DevBuf(DevBuf &&o) noexcept : p(o.p), bytes(o.bytes) {
+    o.p = nullptr;
+    o.bytes = 0;
+  }
+  DevBuf &operator=(DevBuf &&o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p;
+      bytes = o.bytes;
+      o.p = nullptr;
+      o.bytes = 0;
+    }
+    return *this;
+  }
+  ~DevBuf() { release(); }
+  void release() {
+    if (p)
+      cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  // Grow to at least `b` bytes (contents not kept).
+  void reserve(size_t b) {
+    if (b <= bytes && p)
+      return;
+    release();
+    if (b == 0)
+      b = 16;
+    PLS_CUDA(cudaMalloc(&p, b));
+    bytes = b;
+  }
+  template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+// ------------------------------------------------------------ enums
+
+enum class Dt : int { F32 = 0, F64 = 1 };
+enum class Fmt : int { CSR, BSR, DENSE, NUL, IDENTITY, SELL };
+enum class Vt : int { F64 = 0, F32 = 1, BF16 = 2 };  // value storage type
+
+inline size_t vt_size(Vt v) {
+  return v == Vt::F64 ? 8 : v == Vt::F32 ? 4 : 2;
+}
+
+template <class T> struct Tag { using type = T; };
+
+// Call f(Tag<V>) with the C++ type of a value storage type.
+template <class F> void with_vt(Vt vt, F &&f) {
+  switch (vt) {
+  case Vt::F64: f(Tag<double>{}); break;
+  case Vt::F32: f(Tag<float>{}); break;
+  case Vt::BF16: f(Tag<__nv_bfloat16>{}); break;
+  }
+}
+
+// SpMV kernel families the tuner chooses between.
+enum class Kind : int { CSR_VECTOR = 0, SELL = 1, CSR_SPLIT = 2 };
+
+struct SpmvConfig {
+  Kind kind = Kind::CSR_VECTOR;
+  int tpr = 0;   // threads per row (CSR_VECTOR), 0 = pick by mean row length
+  int C = 32;    // SELL chunk height
+  int sigma = 0; // SELL sort window in rows (0 = no sort)
+};
+
+// ------------------------------------------------------------ formats
+
+struct CsrDev {
+  DevBuf row_ptr, col, vals;  // vals in the API type (authoritative)
+  int64_t nnz = 0;
+  Vt vt = Vt::F64;
+  // Reduced-precision copy of the values used by the kernels when the
+  // handle's storage mode asks for one.
+  DevBuf vals_lo;
+  Vt vt_lo = Vt::F64;
+  bool lo = false;
+  const void *ev() const { return lo ? vals_lo.p : vals.p; }
+  Vt evt() const { return lo ? vt_lo : vt; }
+  // Rows longer than the split threshold, processed by the row-split
+  // kernel family (built on demand).
+  DevBuf long_rows;
+  int n_long = 0;
+  int long_threshold = 0;
+};
+
+struct SellDev {
+  int C = 0, sigma = 0;
+  int64_t nC = 0, size = 0;
+  int col_bytes = 0;
+  int64_t n_full_chunks = 0, ntidyup = 0;
+  int32_t max_width = 0;
+  DevBuf cs, cl, col_min, permd2in, in2permd, vals, offsets;
+  Vt vt = Vt::F64;
+  // Work list of (chunk, column slice) items for chunks wider than
+  // slice_w; empty when every chunk fits one item.
+  DevBuf items;
+  int64_t n_items = 0;
+  int slice_w = 0;
+  DevBuf split_chunks;  // (chunk, first slot, slice count) per split chunk
+  int64_t n_split = 0;
+  DevBuf part;          // partial sums of the split chunks' slices (scratch)
+};
+
+struct BsrDev {
+  int bs = 0;
+  int layout = PERFLIBS_ROW_MAJOR;
+  int32_t mb = 0, nb = 0;
+  int64_t nnzb = 0;
+  DevBuf row_ptr, col, vals;
+  Vt vt = Vt::F64;
+  DevBuf vals_lo;
+  Vt vt_lo = Vt::F64;
+  bool lo = false;
+  const void *ev() const { return lo ? vals_lo.p : vals.p; }
+  Vt evt() const { return lo ? vt_lo : vt; }
+};
+
+struct DenseDev {
+  int layout = PERFLIBS_ROW_MAJOR;
+  int64_t lda = 0;
+  DevBuf vals;  // API type
+  bool is_zero = false;
+};
+
+// Per-candidate timing recorded by the tuner.
+struct TuneEntry {
+  SpmvConfig cfg;
+  double ms = 0;
+  double beta = 1.0;  // SELL padding efficiency (1 for CSR)
+};
+
+}  // namespace pls
+
+// The opaque handle of the C interface.
+struct perflibs_spmat_top_t {
+  pls::Dt dt = pls::Dt::F64;
+  pls::Fmt fmt = pls::Fmt::CSR;
+  // The format the user created (CSR / BSR / DENSE / NUL / IDENTITY);
+  // `fmt` may move to SELL after optimize, as in the reference.
+  pls::Fmt created = pls::Fmt::CSR;
+  int32_t m = 0, n = 0;
+  int64_t nnz = 0;
+  int32_t index_base = 0;
+  int device = 0;
+
+  // Hints (reference defaults: src/types.hpp:40-76).
+  int hint_structure = PERFLIBS_SPARSE_STRUCTURE_UNSTRUCTURED;
+  int hint_memory = PERFLIBS_SPARSE_MEMORY_ALLOCS;
+  int hint_spmv_op = PERFLIBS_SPARSE_OPERATION_NOTRANS;
+  int hint_spmv_inv = PERFLIBS_SPARSE_INVOCATIONS_MANY;
+  int hint_spmm_op = PERFLIBS_SPARSE_OPERATION_NOTRANS;
+  int hint_spmm_inv = PERFLIBS_SPARSE_INVOCATIONS_MANY;
+  int hint_spadd_op = PERFLIBS_SPARSE_OPERATION_NOTRANS;
+  int hint_spadd_inv = PERFLIBS_SPARSE_INVOCATIONS_MANY;
+  int hint_spmm_strat = PERFLIBS_SPARSE_SPMM_STRAT_UNSET;
+  int hint_spsm_op = PERFLIBS_SPARSE_OPERATION_NOTRANS;
+  int hint_spsv_op = PERFLIBS_SPARSE_OPERATION_NOTRANS;
+  int hint_spsv_inv = PERFLIBS_SPARSE_INVOCATIONS_MANY;
+  int hint_spsv_strat = PERFLIBS_SPARSE_SPSV_STRAT_UNSET;
+  bool hint_hpcg = false;
+
+  // Error record (reference sp_error_t, src/util.hpp:294-298).
+  int err_type = 0;
+  int err_code = 0;
+  std::string err_msg;
+
+  // Extension state.
+  int storage = PERFLIBS_B200_STORAGE_NATIVE;  // requested value storage
+  int tuner = PERFLIBS_B200_TUNE_EXHAUSTIVE;
+  bool forced = false;
+  pls::SpmvConfig forced_cfg;
+  pls::SpmvConfig cfg;  // active SpMV kernel configuration
+  bool tuned = false;
+  int tuned_op = PERFLIBS_SPARSE_OPERATION_NOTRANS;
+  std::vector<pls::TuneEntry> tune_table;
+  cudaStream_t stream = nullptr;  // nullptr = library stream
+
+  pls::CsrDev csr;
+  pls::SellDev sell;
+  pls::BsrDev bsr;
+  pls::DenseDev dense;
+
+  // CSR of A^T (built on demand for transposed operations).
+  pls::CsrDev csrT;
+  bool has_csrT = false;
+
+  // Staging for host-pointer execution.
+  pls::DevBuf xbuf, ybuf;
+};
+
+namespace pls {
+
+using Mat = perflibs_spmat_top_t;
+
+cudaStream_t lib_stream(int device);
+cudaStream_t stream_of(const Mat *A);
+
+// ------------------------------------------------------------ launchers
+// SpMV: y = alpha*op(A)*x + beta*y on device pointers. X is float/double.
+template <class X>
+void spmv_csr(const CsrDev &c, int32_t m, int tpr, const X *x, X *y, X alpha,
+              X beta, cudaStream_t s);
+template <class X>
+void spmv_csr_split(const CsrDev &c, int32_t m, const X *x, X *y, X alpha,
+                    X beta, cudaStream_t s);
+template <class X>
+void spmv_sell(const SellDev &s, const X *x, X *y, X alpha, X beta,
+               cudaStream_t st);
+template <class X>
+void spmv_bsr(const BsrDev &b, const X *x, X *y, X alpha, X beta,
+              cudaStream_t s);
+template <class X>
+void spmv_csr_trans(const CsrDev &c, int32_t m, int32_t n, const X *x, X *y,
+                    X alpha, X beta, cudaStream_t s);
+template <class X>
+void spmv_dense(const DenseDev &d, int32_t m, int32_t n, bool trans,
+                const X *x, X *y, X alpha, X beta, cudaStream_t s);
+template <class X>
+void axpby(int64_t n, X alpha, const X *x, X beta, X *y, cudaStream_t s);
+template <class X>
+void scal(int64_t n, X beta, X *y, cudaStream_t s);
+
+// SpMM: C = alpha*A*B + beta*C, row-major B (ldb) and C (ldc), k columns.
+template <class X>
+void spmm_csr(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
+              int64_t ldc, int k, X alpha, X beta, cudaStream_t s);
+template <class X>
+void spmm_bsr(const BsrDev &b, const X *B, int64_t ldb, X *C, int64_t ldc,
+              int k, X alpha, X beta, cudaStream_t s);
+
+// Layout helpers.
+template <class X>
+void transpose_dense(const X *in, int64_t rows, int64_t cols, int64_t ldin,
+                     X *out, int64_t ldout, cudaStream_t s);
+template <class X>
+void strided_copy(const X *in, int64_t stride_in, X *out, int64_t stride_out,
+                  int64_t n, cudaStream_t s);
+
+// Conversions.
+void convert_values(const void *in, Vt vin, void *out, Vt vout, int64_t n,
+                    cudaStream_t s);
+void build_sell(const CsrDev &c, int32_t m, int C, int sigma, SellDev &out,
+                cudaStream_t s);
+void sell_build_work_list(SellDev &s, int slice_w, cudaStream_t st);
+void build_csr_transpose(const CsrDev &c, int32_t m, int32_t n, CsrDev &out,
+                         cudaStream_t s);
+void bsr_to_csr(const BsrDev &b, int32_t m, bool drop_zeros, CsrDev &out,
+                cudaStream_t s);
+void csr_to_bsr(const CsrDev &c, int32_t m, int32_t n, int bs, int layout,
+                BsrDev &out, cudaStream_t s);
+void csr_build_long_rows(CsrDev &c, int32_t m, int threshold, cudaStream_t s);
+
+// Norms (double accumulate on device, result to host).
+double inf_norm_csr(const CsrDev &c, int32_t m, cudaStream_t s);
+double frb_norm_values(const void *vals, Vt vt, int64_t n, cudaStream_t s);
+double inf_norm_bsr(const BsrDev &b, cudaStream_t s);
+double inf_norm_dense(const DenseDev &d, Dt dt, int32_t m, int32_t n,
+                      cudaStream_t s);
+
+// Updates of existing entries: returns index of the first update that does
+// not name a stored entry (or n_updates when all were applied).
+int64_t update_csr_values(CsrDev &c, SellDev *sell, int32_t m, int32_t n,
+                          int64_t n_updates, const int32_t *rows_host,
+                          const int32_t *cols_host, const void *vals_host,
+                          Dt dt, int32_t base, cudaStream_t s);
+
+// Tuning.
+std::vector<SpmvConfig> tune_candidates(const Mat *A);
+void tune_spmv(Mat *A);
+SpmvConfig default_config(const Mat *A);
+double time_config(Mat *A, const SpmvConfig &cfg, int reps);
+void apply_config(Mat *A, const SpmvConfig &cfg);
+
+// Execute a configured SpMV on device pointers.
+template <class X>
+void run_spmv(Mat *A, int op, const X *x, X *y, X alpha, X beta,
+              cudaStream_t s);
+
+}  // namespace pls

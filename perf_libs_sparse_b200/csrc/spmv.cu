@@ -1,0 +1,585 @@
+// SpMV kernels of libplsparse_b200 (sm_100a).
+//
+// All kernels compute y = alpha*op(A)*x + beta*y. The path is HBM-bound
+// (about 0.17 flop/byte for FP64 CSR), so the kernels are built around the
+// memory system, not the tensor cores:
+//   * matrix data is read exactly once with streaming loads; x is gathered
+//     through the read-only path and stays resident in L2;
+//   * each row's sum runs in one thread or one group of lanes, so a row's
+//     result depends only on that row (no atomics on the NOTRANS path);
+//   * grids launch one thread group per row / chunk and let the block
+//     scheduler balance uneven rows across the 148 SMs.
+#include "common.cuh"
+#include "pls_internal.hpp"
+
+namespace pls {
+
+template <class X, class Acc>
+__device__ __forceinline__ void store_y(X *y, int64_t i, Acc sum, X alpha,
+                                        X beta, int beta_nz) {
+  // The reference's epilogue: sum*alpha, plus beta*y when beta != 0
+  // (src/compressed_sparse_rows.cpp:1289-1298, src/sell_c_sigma.cpp:779-794).
+  X s = (X)sum * alpha;
+  if (beta_nz)
+    s += beta * y[i];
+  y[i] = s;
+}
+
+// ---------------------------------------------------------------- CSR
+
+// TPR lanes per row; rows longer than skip_len (when > 0) are left to the
+// long-row kernel.
+template <int TPR, class V, class X>
+__global__ void __launch_bounds__(256)
+    k_csr_vector(int32_t m, const int32_t *__restrict__ rp,
+                 const int32_t *__restrict__ col, const V *__restrict__ val,
+                 const X *__restrict__ x, X *__restrict__ y, X alpha, X beta,
+                 int beta_nz, int32_t skip_len) {
+  using Acc = typename AccOf<V, X>::type;
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t row = gid / TPR;
+  if (row >= m)
+    return;
+  const int sub = threadIdx.x & (TPR - 1);
+  const int32_t s = __ldg(rp + row), e = __ldg(rp + row + 1);
+  if (skip_len > 0 && e - s > skip_len)
+    return;  // uniform across the row's lanes
+  Acc sum = 0;
+  int32_t j = s + sub;
+#pragma unroll 2
+  for (; j + TPR < e; j += 2 * TPR) {
+    const V v0 = ld_stream(val + j), v1 = ld_stream(val + j + TPR);
+    const int32_t c0 = ld_stream(col + j), c1 = ld_stream(col + j + TPR);
+    sum = fma(to_acc<Acc>(v0), to_acc<Acc>(ld_ro(x + c0)), sum);
+    sum = fma(to_acc<Acc>(v1), to_acc<Acc>(ld_ro(x + c1)), sum);
+  }
+  if (j < e)
+    sum = fma(to_acc<Acc>(ld_stream(val + j)),
+              to_acc<Acc>(ld_ro(x + ld_stream(col + j))), sum);
+  if constexpr (TPR > 1)
+    sum = group_sum<TPR>(sum, group_mask<TPR>());
+  if (sub == 0)
+    store_y(y, row, sum, alpha, beta, beta_nz);
+}
+
+// One CTA per long row (rows listed in `rows`), block-wide reduction.
+template <class V, class X>
+__global__ void __launch_bounds__(256)
+    k_csr_long(const int32_t *__restrict__ rows, const int32_t *__restrict__ rp,
+               const int32_t *__restrict__ col, const V *__restrict__ val,
+               const X *__restrict__ x, X *__restrict__ y, X alpha, X beta,
+               int beta_nz) {
+  using Acc = typename AccOf<V, X>::type;
+  __shared__ Acc part[8];
+  const int32_t row = rows[blockIdx.x];
+  const int32_t s = __ldg(rp + row), e = __ldg(rp + row + 1);
+  Acc sum = 0;
+  for (int32_t j = s + threadIdx.x; j < e; j += blockDim.x)
+    sum = fma(to_acc<Acc>(ld_stream(val + j)),
+              to_acc<Acc>(ld_ro(x + ld_stream(col + j))), sum);
+  sum = group_sum<32>(sum, 0xffffffffu);
+  if ((threadIdx.x & 31) == 0)
+    part[threadIdx.x >> 5] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    Acc t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+      t += part[w];
+    store_y(y, row, t, alpha, beta, beta_nz);
+  }
+}
+
+template <int TPR, class V, class X>
+static void launch_csr_vector(const CsrDev &c, int32_t m, const X *x, X *y,
+                              X alpha, X beta, int32_t skip, cudaStream_t s) {
+  const int64_t threads = (int64_t)m * TPR;
+  const int64_t blocks = div_up(threads, 256);
+  k_csr_vector<TPR, V, X><<<(unsigned)blocks, 256, 0, s>>>(
+      m, c.row_ptr.as<int32_t>(), c.col.as<int32_t>(), (const V *)c.ev(), x, y,
+      alpha, beta, beta != X(0), skip);
+}
+
+template <class V, class X>
+static void csr_vector_dispatch(const CsrDev &c, int32_t m, int tpr,
+                                const X *x, X *y, X alpha, X beta,
+                                int32_t skip, cudaStream_t s) {
+  switch (tpr) {
+  case 1: launch_csr_vector<1, V>(c, m, x, y, alpha, beta, skip, s); break;
+  case 2: launch_csr_vector<2, V>(c, m, x, y, alpha, beta, skip, s); break;
+  case 4: launch_csr_vector<4, V>(c, m, x, y, alpha, beta, skip, s); break;
+  case 8: launch_csr_vector<8, V>(c, m, x, y, alpha, beta, skip, s); break;
+  case 16: launch_csr_vector<16, V>(c, m, x, y, alpha, beta, skip, s); break;
+  default: launch_csr_vector<32, V>(c, m, x, y, alpha, beta, skip, s); break;
+  }
+}
+
+template <class X>
+void spmv_csr(const CsrDev &c, int32_t m, int tpr, const X *x, X *y, X alpha,
+              X beta, cudaStream_t s) {
+  if (m == 0)
+    return;
+  with_vt(c.evt(), [&](auto tag) {
+    using V = typename decltype(tag)::type;
+    if constexpr (std::is_same_v<X, float> && std::is_same_v<V, double>)
+      throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE, "FP64 storage with FP32 API");
+    else
+      csr_vector_dispatch<V, X>(c, m, tpr, x, y, alpha, beta, 0, s);
+  });
+  PLS_LAUNCH_CHECK();
+}
+
+// Vector kernel for rows up to the threshold + one CTA per longer row.
+template <class X>
+void spmv_csr_split(const CsrDev &c, int32_t m, const X *x, X *y, X alpha,
+                    X beta, cudaStream_t s) {
+  if (m == 0)
+    return;
+  with_vt(c.evt(), [&](auto tag) {
+    using V = typename decltype(tag)::type;
+    if constexpr (std::is_same_v<X, float> && std::is_same_v<V, double>) {
+      throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE, "FP64 storage with FP32 API");
+    } else {
+      int tpr = 32;
+      int32_t thr = c.long_threshold;
+      if (thr <= 64) tpr = 4;
+      else if (thr <= 256) tpr = 8;
+      else if (thr <= 1024) tpr = 16;
+      csr_vector_dispatch<V, X>(c, m, tpr, x, y, alpha, beta, thr, s);
+      if (c.n_long > 0)
+        k_csr_long<V, X><<<c.n_long, 256, 0, s>>>(
+            c.long_rows.as<int32_t>(), c.row_ptr.as<int32_t>(),
+            c.col.as<int32_t>(), (const V *)c.ev(), x, y, alpha, beta,
+            beta != X(0));
+    }
+  });
+  PLS_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------- SELL-C-sigma
+
+// One lane per (chunk, row): the row's products are summed strictly in
+// column order j = 0 .. cl-1 over the padded chunk, the order the reference's
+// spmv_scs<T,C> uses (src/sell_c_sigma.cpp:727-775). Lane r of chunk c
+// reads element cs[c] + j*C + r, so the C lanes of a chunk read C
+// consecutive values per step (a full 256-byte line for C=32, FP64).
+template <int C, class V, class O, class X>
+__global__ void __launch_bounds__(256)
+    k_sell(int64_t nC, const int64_t *__restrict__ cs,
+           const int32_t *__restrict__ cl, const int32_t *__restrict__ cmin,
+           const int32_t *__restrict__ perm, const V *__restrict__ vals,
+           const O *__restrict__ offs, const X *__restrict__ x,
+           X *__restrict__ y, X alpha, X beta, int beta_nz) {
+  using Acc = typename AccOf<V, X>::type;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t c = t / C;
+  if (c >= nC)
+    return;
+  const int r = (int)(t % C);
+  const int32_t w = __ldg(cl + c);
+  const int64_t base = __ldg(cs + c) + r;
+  const X *xb = x + (w > 0 ? __ldg(cmin + c) : 0);
+  const V *vp = vals + base;
+  const O *op = offs + base;
+  Acc acc = 0;
+  int32_t j = 0;
+  for (; j + 4 <= w; j += 4) {
+    const V v0 = ld_stream(vp), v1 = ld_stream(vp + C), v2 = ld_stream(vp + 2 * C),
+            v3 = ld_stream(vp + 3 * C);
+    const O o0 = ld_stream(op), o1 = ld_stream(op + C), o2 = ld_stream(op + 2 * C),
+            o3 = ld_stream(op + 3 * C);
+    const Acc x0 = to_acc<Acc>(ld_ro(xb + o0)), x1 = to_acc<Acc>(ld_ro(xb + o1)),
+              x2 = to_acc<Acc>(ld_ro(xb + o2)), x3 = to_acc<Acc>(ld_ro(xb + o3));
+    acc = fma(to_acc<Acc>(v0), x0, acc);
+    acc = fma(to_acc<Acc>(v1), x1, acc);
+    acc = fma(to_acc<Acc>(v2), x2, acc);
+    acc = fma(to_acc<Acc>(v3), x3, acc);
+    vp += 4 * C;
+    op += 4 * C;
+  }
+  for (; j < w; ++j) {
+    acc = fma(to_acc<Acc>(ld_stream(vp)), to_acc<Acc>(ld_ro(xb + ld_stream(op))), acc);
+    vp += C;
+    op += C;
+  }
+  const int32_t dst = __ldg(perm + c * C + r);
+  if (dst >= 0)
+    store_y(y, dst, acc, alpha, beta, beta_nz);
+}
+
+// Work-list variant: item = (chunk, j0, j1, slot). Items with slot < 0 cover
+// a whole chunk and write y; the others write a partial sum for their
+// column slice into part[slot*C + r], combined in slice order by
+// k_sell_combine. Used when a few chunks are much wider than the rest
+// (power-law row lengths), so one wide chunk does not serialise on a single
+// group of lanes.
+template <int C, class V, class O, class X>
+__global__ void __launch_bounds__(256)
+    k_sell_items(int64_t n_items, const int4 *__restrict__ items,
+                 const int64_t *__restrict__ cs, const int32_t *__restrict__ cmin,
+                 const int32_t *__restrict__ perm, const V *__restrict__ vals,
+                 const O *__restrict__ offs, const X *__restrict__ x,
+                 X *__restrict__ y, typename AccOf<V, X>::type *__restrict__ part,
+                 X alpha, X beta, int beta_nz) {
+  using Acc = typename AccOf<V, X>::type;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t it = t / C;
+  if (it >= n_items)
+    return;
+  const int r = (int)(t % C);
+  const int4 w = items[it];  // chunk, j0, j1, slot
+  const int64_t c = w.x;
+  const int64_t base = __ldg(cs + c) + (int64_t)w.y * C + r;
+  const X *xb = x + (w.z > w.y ? __ldg(cmin + c) : 0);
+  const V *vp = vals + base;
+  const O *op = offs + base;
+  const int32_t len = w.z - w.y;
+  Acc acc = 0;
+  int32_t j = 0;
+  for (; j + 4 <= len; j += 4) {
+    const V v0 = ld_stream(vp), v1 = ld_stream(vp + C), v2 = ld_stream(vp + 2 * C),
+            v3 = ld_stream(vp + 3 * C);
+    const O o0 = ld_stream(op), o1 = ld_stream(op + C), o2 = ld_stream(op + 2 * C),
+            o3 = ld_stream(op + 3 * C);
+    const Acc x0 = to_acc<Acc>(ld_ro(xb + o0)), x1 = to_acc<Acc>(ld_ro(xb + o1)),
+              x2 = to_acc<Acc>(ld_ro(xb + o2)), x3 = to_acc<Acc>(ld_ro(xb + o3));
+    acc = fma(to_acc<Acc>(v0), x0, acc);
+    acc = fma(to_acc<Acc>(v1), x1, acc);
+    acc = fma(to_acc<Acc>(v2), x2, acc);
+    acc = fma(to_acc<Acc>(v3), x3, acc);
+    vp += 4 * C;
+    op += 4 * C;
+  }
+  for (; j < len; ++j) {
+    acc = fma(to_acc<Acc>(ld_stream(vp)), to_acc<Acc>(ld_ro(xb + ld_stream(op))), acc);
+    vp += C;
+    op += C;
+  }
+  if (w.w < 0) {
+    const int32_t dst = __ldg(perm + c * C + r);
+    if (dst >= 0)
+      store_y(y, dst, acc, alpha, beta, beta_nz);
+  } else {
+    part[(int64_t)w.w * C + r] = acc;
+  }
+}
+
+// split: (chunk, first slot, slice count) per split chunk.
+template <int C, class Acc, class X>
+__global__ void k_sell_combine(int64_t n_split, const int4 *__restrict__ split,
+                               const int32_t *__restrict__ perm,
+                               const Acc *__restrict__ part, X *__restrict__ y,
+                               X alpha, X beta, int beta_nz) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t sidx = t / C;
+  if (sidx >= n_split)
+    return;
+  const int r = (int)(t % C);
+  const int4 sp = split[sidx];
+  Acc acc = 0;
+  for (int q = 0; q < sp.z; ++q)
+    acc += part[(int64_t)(sp.y + q) * C + r];
+  const int32_t dst = __ldg(perm + (int64_t)sp.x * C + r);
+  if (dst >= 0)
+    store_y(y, dst, acc, alpha, beta, beta_nz);
+}
+
+template <int C, class V, class O, class X>
+static void launch_sell(const SellDev &s, const X *x, X *y, X alpha, X beta,
+                        cudaStream_t st) {
+  using Acc = typename AccOf<V, X>::type;
+  const int bnz = beta != X(0);
+  if (s.n_items == 0) {
+    const int64_t blocks = div_up(s.nC * C, 256);
+    if (blocks == 0)
+      return;
+    k_sell<C, V, O, X><<<(unsigned)blocks, 256, 0, st>>>(
+        s.nC, s.cs.as<int64_t>(), s.cl.as<int32_t>(), s.col_min.as<int32_t>(),
+        s.permd2in.as<int32_t>(), s.vals.as<V>(), s.offsets.as<O>(), x, y,
+        alpha, beta, bnz);
+  } else {
+    const int64_t blocks = div_up(s.n_items * C, 256);
+    Acc *part = (Acc *)s.part.p;  // partial sums (scratch)
+    k_sell_items<C, V, O, X><<<(unsigned)blocks, 256, 0, st>>>(
+        s.n_items, s.items.as<int4>(), s.cs.as<int64_t>(),
+        s.col_min.as<int32_t>(), s.permd2in.as<int32_t>(), s.vals.as<V>(),
+        s.offsets.as<O>(), x, y, part, alpha, beta, bnz);
+    if (s.n_split > 0) {
+      const int64_t b2 = div_up(s.n_split * C, 256);
+      k_sell_combine<C, Acc, X><<<(unsigned)b2, 256, 0, st>>>(
+          s.n_split, s.split_chunks.as<int4>(), s.permd2in.as<int32_t>(), part,
+          y, alpha, beta, bnz);
+    }
+  }
+}
+
+template <int C, class V, class X>
+static void sell_by_width(const SellDev &s, const X *x, X *y, X alpha, X beta,
+                          cudaStream_t st) {
+  switch (s.col_bytes) {
+  case 1: launch_sell<C, V, uint8_t, X>(s, x, y, alpha, beta, st); break;
+  case 2: launch_sell<C, V, uint16_t, X>(s, x, y, alpha, beta, st); break;
+  case 4: launch_sell<C, V, uint32_t, X>(s, x, y, alpha, beta, st); break;
+  default:
+    throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE, "unsupported SELL offset width");
+  }
+}
+
+template <class X>
+void spmv_sell(const SellDev &s, const X *x, X *y, X alpha, X beta,
+               cudaStream_t st) {
+  if (s.nC == 0)
+    return;
+  with_vt(s.vt, [&](auto tag) {
+    using V = typename decltype(tag)::type;
+    if constexpr (std::is_same_v<X, float> && std::is_same_v<V, double>) {
+      throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE, "FP64 storage with FP32 API");
+    } else {
+      switch (s.C) {
+      case 8: sell_by_width<8, V, X>(s, x, y, alpha, beta, st); break;
+      case 16: sell_by_width<16, V, X>(s, x, y, alpha, beta, st); break;
+      case 32: sell_by_width<32, V, X>(s, x, y, alpha, beta, st); break;
+      default:
+        throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE, "SELL chunk height must be 8, 16 or 32");
+      }
+    }
+  });
+  PLS_LAUNCH_CHECK();
+}
+
+// ------------------------------------------------------------ transpose
+
+// y = alpha*A^T*x + beta*y: y scaled first, then every nonzero scatters
+// alpha*val*x[row] into y[col] (the reference's spmv_csr_trans scheme,
+// src/compressed_sparse_rows.cpp:1558-1676, with hardware atomics).
+template <class V, class X>
+__global__ void k_csr_trans_scatter(int32_t m, const int32_t *__restrict__ rp,
+                                    const int32_t *__restrict__ col,
+                                    const V *__restrict__ val,
+                                    const X *__restrict__ x, X *__restrict__ y,
+                                    X alpha) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t row = gid / 32;
+  if (row >= m)
+    return;
+  const int lane = threadIdx.x & 31;
+  const X xr = alpha * x[row];
+  for (int32_t j = rp[row] + lane; j < rp[row + 1]; j += 32)
+    atomicAdd(y + col[j], (X)to_acc<double>(val[j]) * xr);
+}
+
+template <class X> __global__ void k_scal(int64_t n, X beta, X *y) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n)
+    y[i] = beta == X(0) ? X(0) : y[i] * beta;
+}
+
+template <class X>
+__global__ void k_axpby(int64_t n, X alpha, const X *x, X beta, X *y) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n)
+    y[i] = alpha * x[i] + (beta == X(0) ? X(0) : beta * y[i]);
+}
+
+template <class X> void scal(int64_t n, X beta, X *y, cudaStream_t s) {
+  if (n <= 0)
+    return;
+  k_scal<X><<<(unsigned)div_up(n, 256), 256, 0, s>>>(n, beta, y);
+  PLS_LAUNCH_CHECK();
+}
+
+template <class X>
+void axpby(int64_t n, X alpha, const X *x, X beta, X *y, cudaStream_t s) {
+  if (n <= 0)
+    return;
+  k_axpby<X><<<(unsigned)div_up(n, 256), 256, 0, s>>>(n, alpha, x, beta, y);
+  PLS_LAUNCH_CHECK();
+}
+
+template <class X>
+void spmv_csr_trans(const CsrDev &c, int32_t m, int32_t n, const X *x, X *y,
+                    X alpha, X beta, cudaStream_t s) {
+  scal<X>(n, beta, y, s);
+  if (m == 0 || c.nnz == 0)
+    return;
+  with_vt(c.evt(), [&](auto tag) {
+    using V = typename decltype(tag)::type;
+    k_csr_trans_scatter<V, X><<<(unsigned)div_up((int64_t)m * 32, 256), 256, 0, s>>>(
+        m, c.row_ptr.as<int32_t>(), c.col.as<int32_t>(), (const V *)c.ev(), x, y,
+        alpha);
+  });
+  PLS_LAUNCH_CHECK();
+}
+
+// -------------------------------------------------------------- dense
+
+// Output row i of op(A) with element (i, j) at A[i*rs + j*cs]. A warp per
+// row when the row is contiguous, a thread per row otherwise.
+template <class X>
+__global__ void k_gemv_warp(int64_t rows, int64_t cols, const X *A, int64_t rs,
+                            const X *x, X *y, X alpha, X beta) {
+  const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32;
+  if (row >= rows)
+    return;
+  const int lane = threadIdx.x & 31;
+  X s = 0;
+  for (int64_t j = lane; j < cols; j += 32)
+    s = fma(A[row * rs + j], x[j], s);
+  s = group_sum<32>(s, 0xffffffffu);
+  if (lane == 0)
+    y[row] = alpha * s + (beta == X(0) ? X(0) : beta * y[row]);
+}
+
+template <class X>
+__global__ void k_gemv_thread(int64_t rows, int64_t cols, const X *A,
+                              int64_t cs, const X *x, X *y, X alpha, X beta) {
+  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= rows)
+    return;
+  X s = 0;
+  for (int64_t j = 0; j < cols; ++j)
+    s = fma(A[row + j * cs], x[j], s);
+  y[row] = alpha * s + (beta == X(0) ? X(0) : beta * y[row]);
+}
+
+template <class X>
+void spmv_dense(const DenseDev &d, int32_t m, int32_t n, bool trans,
+                const X *x, X *y, X alpha, X beta, cudaStream_t s) {
+  const int64_t rows = trans ? n : m, cols = trans ? m : n;
+  if (rows == 0)
+    return;
+  // Stored element (r, c) at r*lda (row-major) or c*lda (column-major).
+  const bool row_contig = (d.layout == PERFLIBS_ROW_MAJOR) != trans;
+  const X *A = d.vals.as<X>();
+  if (row_contig)
+    k_gemv_warp<X><<<(unsigned)div_up(rows * 32, 256), 256, 0, s>>>(
+        rows, cols, A, d.lda, x, y, alpha, beta);
+  else
+    k_gemv_thread<X><<<(unsigned)div_up(rows, 256), 256, 0, s>>>(
+        rows, cols, A, d.lda, x, y, alpha, beta);
+  PLS_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------- BSR
+
+// Block sizes whose bs*bs elements tile a warp (bs = 1, 2, 4): a warp per
+// block row; lane l owns element e = l % (bs*bs) of 32/(bs*bs) consecutive
+// blocks per step, so every step reads 32 consecutive values. Lanes holding
+// the same scalar row are reduced with shuffles at the end.
+template <int BS, class V, class X>
+__global__ void __launch_bounds__(256)
+    k_bsr_small(int32_t mb, int layout, const int32_t *__restrict__ rp,
+                const int32_t *__restrict__ col, const V *__restrict__ val,
+                const X *__restrict__ x, X *__restrict__ y, X alpha, X beta,
+                int beta_nz) {
+  using Acc = typename AccOf<V, X>::type;
+  constexpr int E = BS * BS, PER = 32 / E;
+  const int64_t br = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32;
+  if (br >= mb)
+    return;
+  const int lane = threadIdx.x & 31, e = lane % E, slot = lane / E;
+  const bool rm = layout == PERFLIBS_ROW_MAJOR;
+  const int i = rm ? e / BS : e % BS;
+  const int j = rm ? e % BS : e / BS;
+  Acc acc = 0;
+  for (int32_t b = rp[br] + slot; b < rp[br + 1]; b += PER) {
+    const Acc v = to_acc<Acc>(ld_stream(val + (int64_t)b * E + e));
+    acc = fma(v, to_acc<Acc>(ld_ro(x + (int64_t)ld_stream(col + b) * BS + j)), acc);
+  }
+  // Reduce over all lanes with the same i: the j bits and the slot bits.
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int lo = rm ? o : o;  // lane bit o
+    const bool is_i_bit = rm ? (o >= BS && o < E) : (o < BS);
+    if (!is_i_bit)
+      acc += __shfl_xor_sync(0xffffffffu, acc, lo);
+  }
+  const bool owner = rm ? (j == 0 && slot == 0) : (j == 0 && slot == 0);
+  if (owner) {
+    const int64_t r = br * BS + i;
+    store_y(y, r, acc, alpha, beta, beta_nz);
+  }
+}
+
+// Any block size: a thread per scalar row.
+template <class V, class X>
+__global__ void __launch_bounds__(256)
+    k_bsr_rows(int32_t mb, int bs, int layout, const int32_t *__restrict__ rp,
+               const int32_t *__restrict__ col, const V *__restrict__ val,
+               const X *__restrict__ x, X *__restrict__ y, X alpha, X beta,
+               int beta_nz) {
+  using Acc = typename AccOf<V, X>::type;
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= (int64_t)mb * bs)
+    return;
+  const int64_t br = r / bs;
+  const int i = (int)(r % bs);
+  const int64_t E = (int64_t)bs * bs;
+  const bool rm = layout == PERFLIBS_ROW_MAJOR;
+  Acc acc = 0;
+  for (int32_t b = rp[br]; b < rp[br + 1]; ++b) {
+    const V *blk = val + (int64_t)b * E;
+    const X *xb = x + (int64_t)col[b] * bs;
+    for (int j = 0; j < bs; ++j) {
+      const V v = rm ? ld_stream(blk + (int64_t)i * bs + j) : ld_stream(blk + (int64_t)j * bs + i);
+      acc = fma(to_acc<Acc>(v), to_acc<Acc>(ld_ro(xb + j)), acc);
+    }
+  }
+  store_y(y, r, acc, alpha, beta, beta_nz);
+}
+
+template <class X>
+void spmv_bsr(const BsrDev &b, const X *x, X *y, X alpha, X beta,
+              cudaStream_t s) {
+  if (b.mb == 0)
+    return;
+  const int bnz = beta != X(0);
+  with_vt(b.evt(), [&](auto tag) {
+    using V = typename decltype(tag)::type;
+    if constexpr (std::is_same_v<X, float> && std::is_same_v<V, double>) {
+      throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE, "FP64 storage with FP32 API");
+    } else {
+      const unsigned wblocks = (unsigned)div_up((int64_t)b.mb * 32, 256);
+      switch (b.bs) {
+      case 1:
+        k_bsr_small<1, V, X><<<wblocks, 256, 0, s>>>(b.mb, b.layout, b.row_ptr.as<int32_t>(),
+            b.col.as<int32_t>(), (const V *)b.ev(), x, y, alpha, beta, bnz);
+        break;
+      case 2:
+        k_bsr_small<2, V, X><<<wblocks, 256, 0, s>>>(b.mb, b.layout, b.row_ptr.as<int32_t>(),
+            b.col.as<int32_t>(), (const V *)b.ev(), x, y, alpha, beta, bnz);
+        break;
+      case 4:
+        k_bsr_small<4, V, X><<<wblocks, 256, 0, s>>>(b.mb, b.layout, b.row_ptr.as<int32_t>(),
+            b.col.as<int32_t>(), (const V *)b.ev(), x, y, alpha, beta, bnz);
+        break;
+      default:
+        k_bsr_rows<V, X><<<(unsigned)div_up((int64_t)b.mb * b.bs, 256), 256, 0, s>>>(
+            b.mb, b.bs, b.layout, b.row_ptr.as<int32_t>(), b.col.as<int32_t>(),
+            (const V *)b.ev(), x, y, alpha, beta, bnz);
+      }
+    }
+  });
+  PLS_LAUNCH_CHECK();
+}
+
+// ------------------------------------------------------ instantiations
+#define PLS_INST(X)                                                            \
+  template void spmv_csr<X>(const CsrDev &, int32_t, int, const X *, X *, X,  \
+                            X, cudaStream_t);                                  \
+  template void spmv_csr_split<X>(const CsrDev &, int32_t, const X *, X *, X, \
+                                  X, cudaStream_t);                            \
+  template void spmv_sell<X>(const SellDev &, const X *, X *, X, X,           \
+                             cudaStream_t);                                    \
+  template void spmv_bsr<X>(const BsrDev &, const X *, X *, X, X,             \
+                            cudaStream_t);                                     \
+  template void spmv_csr_trans<X>(const CsrDev &, int32_t, int32_t,           \
+                                  const X *, X *, X, X, cudaStream_t);         \
+  template void spmv_dense<X>(const DenseDev &, int32_t, int32_t, bool,       \
+                              const X *, X *, X, X, cudaStream_t);             \
+  template void axpby<X>(int64_t, X, const X *, X, X *, cudaStream_t);        \
+  template void scal<X>(int64_t, X, X *, cudaStream_t);
+
+PLS_INST(float)
+PLS_INST(double)
+
+}  // namespace pls

@@ -1,0 +1,81 @@
+"""CPU: the C-ABI library loads, exports every entry point the headers
+declare, and fails loudly (never silently) where no GPU is present."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import perf_libs_sparse_b200 as pls
+
+HEADERS = [os.path.join(pls.INCLUDE_DIR, h) for h in ("perflibs_sparse.h", "perflibs_b200.h")]
+
+
+def declared_functions():
+    names = set()
+    for h in HEADERS:
+        txt = open(h).read()
+        txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+        for m in re.finditer(r"\b(perflibs_\w+)\s*\(", txt):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_headers_declare_the_drop_in_subset():
+    names = declared_functions()
+    for required in [
+        "perflibs_spmat_create_csr_d", "perflibs_spmat_create_csr_s", "perflibs_spmat_create_bsr_d",
+        "perflibs_spmat_create_dense_d", "perflibs_spmat_create_null", "perflibs_spmat_hint",
+        "perflibs_spmv_optimize", "perflibs_spmm_optimize", "perflibs_spmv_exec_d",
+        "perflibs_spmv_exec_s", "perflibs_spmm_exec_d", "perflibs_spmm_exec_s",
+        "perflibs_spmat_export_csr_d", "perflibs_spmat_export_dense_d", "perflibs_spnorm_exec_d",
+        "perflibs_spmat_query", "perflibs_spmat_destroy", "perflibs_spmat_print_err",
+    ]:
+        assert required in names
+
+
+def test_library_exports_every_declared_symbol():
+    L = ctypes.CDLL(pls.LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_library_is_sm100a_only():
+    # The fat binary carries sm_100a code only; cuobjdump is not used, the
+    # build command line is the evidence.
+    import perf_libs_sparse_b200.build as b
+
+    assert b.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def test_enum_values_match_reference_interface():
+    # include/perflibs_sparse.h:67-149 of the reference.
+    assert (pls.STATUS_SUCCESS, pls.STATUS_INPUT_PARAMETER_ERROR, pls.STATUS_EXECUTION_FAILURE) == (0, 1, 2)
+    assert (pls.OPERATION_NOTRANS, pls.OPERATION_TRANS, pls.OPERATION_CONJTRANS) == (300, 310, 320)
+    assert (pls.INVOCATIONS_SINGLE, pls.INVOCATIONS_FEW, pls.INVOCATIONS_MANY) == (400, 410, 420)
+    assert (pls.COL_MAJOR, pls.ROW_MAJOR) == (90, 91)
+    assert (pls.NORM_INF, pls.NORM_FRB) == (1001, 1002)
+    txt = open(HEADERS[0]).read()
+    for name, val in [("PERFLIBS_SPARSE_HINT_SPMV_INVOCATIONS", 80), ("PERFLIBS_SPARSE_SCALAR_ANY", 502),
+                      ("PERFLIBS_SPARSE_SPMM_STRAT_OPT_FULL_STRUCT", 603), ("PERFLIBS_SPARSE_CREATE_NOCOPY", 1)]:
+        assert re.search(rf"{name}\s*=?\s*{val}\b", txt), name
+
+
+def _no_gpu():
+    try:
+        import torch
+
+        return not torch.cuda.is_available()
+    except Exception:
+        return True
+
+
+@pytest.mark.skipif(not _no_gpu(), reason="only meaningful without a GPU")
+def test_fails_loudly_without_gpu():
+    rp = np.array([0, 1], np.int32)
+    c = np.array([0], np.int32)
+    v = np.array([1.0])
+    with pytest.raises(pls.PerflibsError) as e:
+        pls.SpMat.csr(1, 1, rp, c, v)
+    assert e.value.status == pls.STATUS_EXECUTION_FAILURE

@@ -1,0 +1,158 @@
+"""GPU parity: sparse x dense SpMM through the C-ABI (drop-in create / hint /
+optimize / exec / export flow), against the reference's golden vectors and
+the oracle. FP64 tolerance 1e-12 (scaled per element as for SpMV)."""
+import numpy as np
+import pytest
+
+import oracle
+import perf_libs_sparse_b200 as pls
+from perf_libs_sparse_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def spmm_ref(rp, c, v, B, alpha, beta, C0):
+    return oracle.csr_spmm(rp, c, v, np.ascontiguousarray(B), B.shape[1], Cmat=C0, alpha=alpha, beta=beta)
+
+
+def scaled_err(got, ref, rp, c, v, B, alpha, beta, C0):
+    absA = oracle.csr_spmm(rp, c, np.abs(v), np.abs(np.ascontiguousarray(B)), B.shape[1])
+    sc = abs(alpha) * absA
+    if C0 is not None and beta != 0:
+        sc = sc + abs(beta) * np.abs(C0)
+    den = np.maximum(np.abs(ref), sc)
+    den[den == 0] = 1
+    return (np.abs(got - ref) / den).max()
+
+
+def test_kat_matmul_variants(kats):
+    k = kats["matmul_variants_d"]
+    rp, c, v = np.array(k["row_ptr"]), np.array(k["col"]), np.array(k["vals"])
+    Ad = np.array(k["denseA"]).reshape(4, 4)
+    Bd = np.array(k["denseB"]).reshape(4, 4)
+    A = pls.SpMat.csr(4, 4, rp, c, v)
+    B = pls.SpMat.dense(pls.ROW_MAJOR, 4, 4, 4, Bd.reshape(-1))
+    opt_null = pls.SpMat.null(4, 4)
+    assert pls.spmm_optimize(pls.OPERATION_NOTRANS, pls.OPERATION_NOTRANS, pls.SCALAR_ANY, A, B,
+                             pls.SCALAR_ANY, opt_null) == 0
+    for ta in (pls.OPERATION_NOTRANS, pls.OPERATION_TRANS):
+        for tb in (pls.OPERATION_NOTRANS, pls.OPERATION_TRANS):
+            Cm = pls.SpMat.null(4, 4)
+            alpha = k["alpha_notrans"] if ta == pls.OPERATION_NOTRANS else k["alpha_trans"]
+            assert pls.spmm_exec(ta, tb, alpha, A, B, 0.0, Cm) == 0
+            opA = Ad if ta == pls.OPERATION_NOTRANS else Ad.T
+            opB = Bd if tb == pls.OPERATION_NOTRANS else Bd.T
+            np.testing.assert_allclose(Cm.export_dense(pls.ROW_MAJOR), alpha * opA @ opB, atol=k["tol"])
+    C0 = np.array(k["c_init"]).reshape(4, 4)
+    Cd = pls.SpMat.dense(pls.ROW_MAJOR, 4, 4, 4, C0.reshape(-1))
+    assert pls.spmm_exec(pls.OPERATION_NOTRANS, pls.OPERATION_NOTRANS, k["alpha_beta"], A, B, k["beta"], Cd) == 0
+    np.testing.assert_allclose(Cd.export_dense(), k["alpha_beta"] * Ad @ Bd + k["beta"] * C0, atol=k["tol"])
+    # column-major B and C
+    Bc = pls.SpMat.dense(pls.COL_MAJOR, 4, 4, 4, Bd.T.reshape(-1))
+    Cc = pls.SpMat.dense(pls.COL_MAJOR, 4, 4, 4, C0.T.reshape(-1))
+    assert pls.spmm_exec(pls.OPERATION_NOTRANS, pls.OPERATION_NOTRANS, k["alpha_beta"], A, Bc, k["beta"], Cc) == 0
+    np.testing.assert_allclose(Cc.export_dense(pls.ROW_MAJOR), k["alpha_beta"] * Ad @ Bd + C0, atol=k["tol"])
+    np.testing.assert_allclose(Cc.export_dense(pls.COL_MAJOR), k["alpha_beta"] * Ad @ Bd + C0, atol=k["tol"])
+
+
+def test_kat_matrix_kernel_ops(kats):
+    k = kats["matrix_kernel_ops_spmm"]
+    rp, c, v = np.array(k["row_ptr"]), np.array(k["col"]), np.array(k["vals"])
+    Bd = np.array(k["denseB"]).reshape(4, 4)
+    Ad = np.zeros((4, 4))
+    for i in range(4):
+        for p in range(rp[i], rp[i + 1]):
+            Ad[i, c[p]] = v[p]
+    A = pls.SpMat.csr(4, 4, rp, c, v)
+    B = pls.SpMat.dense(pls.ROW_MAJOR, 4, 4, 4, Bd.reshape(-1))
+    Cm = pls.SpMat.null(4, 4)
+    assert pls.spmm_optimize(pls.OPERATION_NOTRANS, pls.OPERATION_NOTRANS, pls.SCALAR_ANY, A, B,
+                             pls.SCALAR_ZERO, Cm) == 0
+    assert pls.spmm_exec(pls.OPERATION_NOTRANS, pls.OPERATION_NOTRANS, 1.0, A, B, 0.0, Cm) == 0
+    np.testing.assert_allclose(Cm.export_dense(), Ad @ Bd, atol=k["tol"])
+
+
+@pytest.mark.parametrize("k", [1, 3, 5, 8, 13, 32, 128])
+def test_random_spmm_vs_oracle(k):
+    rng = np.random.default_rng(k)
+    for m, n, ml, base in [(200, 150, 20, 0), (1500, 1000, 40, 1)]:
+        rp, c, v = W.random_csr(m, n, ml, rng, base=base)
+        Bd = rng.uniform(-1, 1, (n, k))
+        C0 = rng.uniform(-1, 1, (m, k))
+        rp0, c0 = rp - base, c - base
+        for alpha, beta in [(1.0, 0.0), (1.5, 1.0), (-0.5, 0.25)]:
+            A = pls.SpMat.csr(m, n, rp, c, v)
+            B = pls.SpMat.dense(pls.ROW_MAJOR, n, k, k, Bd.reshape(-1))
+            Cm = pls.SpMat.dense(pls.ROW_MAJOR, m, k, k, C0.reshape(-1)) if beta != 0 else pls.SpMat.null(m, k)
+            assert pls.spmm_optimize(pls.OPERATION_NOTRANS, pls.OPERATION_NOTRANS, pls.SCALAR_ANY, A, B,
+                                     pls.SCALAR_ANY if beta else pls.SCALAR_ZERO, Cm) == 0
+            assert pls.spmm_exec(pls.OPERATION_NOTRANS, pls.OPERATION_NOTRANS, alpha, A, B, beta, Cm) == 0
+            got = Cm.export_dense()
+            ref = spmm_ref(rp0, c0, v, Bd, alpha, beta, C0 if beta else None)
+            assert scaled_err(got, ref, rp0, c0, v, Bd, alpha, beta, C0) <= 1e-12, (m, k, alpha, beta)
+
+
+def test_repeated_exec_with_beta_zero_overwrites():
+    rng = np.random.default_rng(2)
+    rp, c, v = W.random_csr(300, 300, 10, rng)
+    Bd = rng.uniform(-1, 1, (300, 16))
+    A = pls.SpMat.csr(300, 300, rp, c, v)
+    B = pls.SpMat.dense(pls.ROW_MAJOR, 300, 16, 16, Bd.reshape(-1))
+    Cm = pls.SpMat.null(300, 16)
+    pls.spmm_optimize(pls.OPERATION_NOTRANS, pls.OPERATION_NOTRANS, pls.SCALAR_ONE, A, B, pls.SCALAR_ZERO, Cm)
+    for _ in range(3):
+        assert pls.spmm_exec(pls.OPERATION_NOTRANS, pls.OPERATION_NOTRANS, 1.0, A, B, 0.0, Cm) == 0
+    ref = spmm_ref(rp, c, v, Bd, 1.0, 0.0, None)
+    np.testing.assert_allclose(Cm.export_dense(), ref, rtol=1e-12, atol=1e-12)
+
+
+def test_bsr_spmm_vs_oracle():
+    rng = np.random.default_rng(9)
+    for bs in (2, 4, 8, 3):
+        for layout in (pls.ROW_MAJOR, pls.COL_MAJOR):
+            m = n = bs * 40
+            rp, c, v = W.random_csr(m, n, 12, rng)
+            brp, bc, bv = oracle.csr2bsr(rp, c, v, m, n, bs, layout)
+            for k in (4, 8, 64):
+                Bd = rng.uniform(-1, 1, (n, k))
+                A = pls.SpMat.bsr(layout, m, n, bs, brp, bc, bv)
+                B = pls.SpMat.dense(pls.ROW_MAJOR, n, k, k, Bd.reshape(-1))
+                Cm = pls.SpMat.null(m, k)
+                assert pls.spmm_exec(pls.OPERATION_NOTRANS, pls.OPERATION_NOTRANS, 1.0, A, B, 0.0, Cm) == 0
+                ref = spmm_ref(rp, c, v, Bd, 1.0, 0.0, None)
+                np.testing.assert_allclose(Cm.export_dense(), ref, rtol=1e-12, atol=1e-12)
+                # BSR SpMV
+                x = rng.uniform(-1, 1, n)
+                np.testing.assert_allclose(A.spmv(x), oracle.csr_spmv(rp, c, v, x), rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("storage,tol", [(pls.STORAGE_NATIVE, 1e-12), (pls.STORAGE_FP32, 1e-5),
+                                         (pls.STORAGE_BF16, 1e-2)])
+def test_stencil_spmm_storage_modes(storage, tol):
+    m, n, rp, c, v = W.stencil_27pt(24, seed=2)
+    rng = np.random.default_rng(2)
+    for k in (8, 32):
+        Bd = rng.uniform(-1, 1, (n, k))
+        ref = spmm_ref(rp, c, v, Bd, 1.0, 0.0, None)
+        dt = np.float64 if storage == pls.STORAGE_NATIVE else np.float32
+        A = pls.SpMat.csr(m, n, rp, c, v.astype(dt))
+        A.set_storage(storage)
+        B = pls.SpMat.dense(pls.ROW_MAJOR, n, k, k, Bd.astype(dt).reshape(-1))
+        Cm = pls.SpMat.null(m, k)
+        assert pls.spmm_exec(pls.OPERATION_NOTRANS, pls.OPERATION_NOTRANS, 1.0, A, B, 0.0, Cm) == 0
+        got = Cm.export_dense().astype(np.float64)
+        assert scaled_err(got, ref, rp, c, v, Bd, 1.0, 0.0, None) <= tol
+
+
+def test_device_pointer_spmm():
+    import torch
+
+    rng = np.random.default_rng(3)
+    rp, c, v = W.random_csr(1000, 800, 30, rng)
+    Bd = rng.uniform(-1, 1, (800, 32))
+    A = pls.SpMat.csr(1000, 800, rp, c, v)
+    Bt = torch.tensor(Bd, device="cuda")
+    Ct = torch.empty((1000, 32), dtype=torch.float64, device="cuda")
+    A.spmm_dev(Bt.data_ptr(), 32, 32, Ct.data_ptr(), 32, 1.0, 0.0, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(Ct.cpu().numpy(), spmm_ref(rp, c, v, Bd, 1.0, 0.0, None), rtol=1e-12, atol=1e-12)

@@ -1,0 +1,127 @@
+"""CPU: the oracle restatement against the reference's golden vectors and
+against the reference library itself (oracle/_ref, when built)."""
+import numpy as np
+import pytest
+
+import oracle
+from tests.conftest import case_names
+
+pytestmark = pytest.mark.filterwarnings("ignore")
+
+
+def test_spmv_basic_kat(kats):
+    k = kats["spmv_basic_d"]
+    rp = np.array(k["row_ptr"], np.int32)
+    c = np.array(k["col"], np.int32)
+    v = np.array(k["vals"], np.float64)
+    x = np.array(k["x"], np.float64)
+    for mode in (0, 1):
+        y = oracle.csr_spmv(rp, c, v, x, alpha=k["alpha"], beta=k["beta"], mode=mode)
+        np.testing.assert_allclose(y, k["y"], atol=k["tol"])
+
+
+def test_bsr_kats(kats):
+    k = kats["bsr_row_major"]
+    rp = np.array(k["row_ptr"], np.int32)
+    c = np.array(k["col"], np.int32)
+    v = np.array(k["vals"], np.float64)
+    x = np.array(k["x"], np.float64)
+    y = oracle.bsr_spmv(rp, c, v, k["bs"], k["layout"], x)
+    np.testing.assert_allclose(y, k["y_notrans"], atol=k["tol"])
+    crp, cc, cv = oracle.bsr2csr(rp, c, v, k["bs"], k["layout"])
+    yt = oracle.csr_spmv_trans(crp, cc, cv, k["n"], x)
+    np.testing.assert_allclose(yt, k["y_trans"], atol=k["tol"])
+
+    k = kats["bsr_col_major"]
+    rp = np.array(k["row_ptr"], np.int32)
+    c = np.array(k["col"], np.int32)
+    v = np.array(k["vals"], np.float64)
+    crp, cc, cv = oracle.bsr2csr(rp, c, v, k["bs"], k["layout"])
+    assert oracle.csr_inf_norm(crp, cv) == k["inf_norm"]
+    yt = oracle.csr_spmv_trans(crp, cc, cv, k["n"], np.array(k["x"], float), alpha=k["alpha_trans"])
+    np.testing.assert_allclose(yt, k["y_trans_scaled"], atol=k["tol"])
+
+
+def test_spmm_kats(kats):
+    k = kats["matmul_variants_d"]
+    rp = np.array(k["row_ptr"], np.int32)
+    c = np.array(k["col"], np.int32)
+    v = np.array(k["vals"], np.float64)
+    A = np.array(k["denseA"]).reshape(4, 4)
+    B = np.array(k["denseB"]).reshape(4, 4)
+    C0 = np.array(k["c_init"]).reshape(4, 4)
+    got = oracle.csr_spmm(rp, c, v, B, 4, alpha=1.0, beta=0.0)
+    np.testing.assert_allclose(got, A @ B, atol=k["tol"])
+    got = oracle.csr_spmm(rp, c, v, B, 4, Cmat=C0, alpha=k["alpha_beta"], beta=k["beta"])
+    np.testing.assert_allclose(got, k["alpha_beta"] * A @ B + C0, atol=k["tol"])
+
+
+def test_csr2bsr_roundtrip():
+    rng = np.random.default_rng(5)
+    from perf_libs_sparse_b200 import workloads as W
+    for bs in (2, 4, 8):
+        for layout in (90, 91):
+            m = n = bs * 9
+            rp, c, v = W.random_csr(m, n, 10, rng, empty_frac=0.2)
+            brp, bc, bv = oracle.csr2bsr(rp, c, v, m, n, bs, layout)
+            rp2, c2, v2 = oracle.bsr2csr(brp, bc, bv, bs, layout)
+            np.testing.assert_array_equal(rp2, rp)
+            np.testing.assert_array_equal(c2, c)
+            np.testing.assert_array_equal(v2, v)
+
+
+def test_port_matches_reference_fixtures(ref_outputs):
+    """Restated SELL builder and CSR exec vs the reference library's own
+    outputs (committed fixtures made by tests/golden/make_golden.py)."""
+    f = ref_outputs
+    for name in case_names(f):
+        rp, c, v = f[f"{name}/row_ptr"], f[f"{name}/col"], f[f"{name}/vals"]
+        m, n = (int(t) for t in f[f"{name}/shape"])
+        x, y0 = f[f"{name}/x"], f[f"{name}/y0"]
+        y = oracle.csr_spmv(rp, c, v, x, y=y0, alpha=1.5, beta=-0.5, mode=1)
+        np.testing.assert_allclose(y, f[f"{name}/y_csr"], rtol=1e-12, atol=1e-12)
+        for key in [k[: -len("/info")] for k in f.files if k.startswith(name + "/scs_") and k.endswith("/info")]:
+            info = f[key + "/info"]
+            C, sigma = int(info[1]), int(info[2])
+            s = oracle.scs_build(rp, c, v, n, C, sigma)
+            got = [s["nC"], s["C"], s["sigma"], s["col_bytes"], s["n_full_chunks"], s["ntidyup"], s["size"]]
+            assert got == [int(t) for t in info], key
+            for fld in ("cs", "cl", "col_min", "permd2in", "vals"):
+                np.testing.assert_array_equal(s[fld], f[f"{key}/{fld}"], err_msg=f"{key}/{fld}")
+            np.testing.assert_array_equal(s["offsets"], f[f"{key}/offsets"].astype(np.int64))
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference library not built here")
+def test_port_matches_reference_live():
+    """Live cross-check on fresh random cases, including SELL exec (C <= 16,
+    the sizes the reference executes)."""
+    from perf_libs_sparse_b200 import workloads as W
+    rng = np.random.default_rng(99)
+    for t in range(25):
+        m = int(rng.integers(1, 400))
+        n = int(rng.integers(1, 900))
+        rp, c, v = W.random_csr(m, n, min(n, 40), rng, base=int(t % 2))
+        for C in (2, 8, 16, 32):
+            for sigma in (0, C, 4 * C):
+                a = oracle.ref_scs_build(rp, c, v, n, C, sigma)
+                b = oracle.scs_build(rp, c, v, n, C, sigma)
+                for k in ("cs", "cl", "col_min", "permd2in", "in2permd", "vals", "offsets"):
+                    np.testing.assert_array_equal(a[k], b[k])
+                assert (a["col_bytes"], a["n_full_chunks"], a["ntidyup"]) == (
+                    b["col_bytes"], b["n_full_chunks"], b["ntidyup"])
+                x = rng.uniform(-1, 1, n)
+                yp = oracle.scs_spmv(b, x, alpha=1.0)
+                assert np.all(np.isfinite(yp))
+
+
+def test_scs_spmv_equals_csr():
+    from perf_libs_sparse_b200 import workloads as W
+    rng = np.random.default_rng(3)
+    rp, c, v = W.random_csr(500, 700, 50, rng)
+    x = rng.uniform(-1, 1, 700)
+    y_ref = oracle.csr_spmv(rp, c, v, x)
+    for C in (8, 32):
+        for sigma in (0, 64 * C // 8):
+            s = oracle.scs_build(rp, c, v, 700, C, sigma)
+            y = oracle.scs_spmv(s, x)
+            np.testing.assert_allclose(y, y_ref, rtol=1e-12, atol=1e-12)
