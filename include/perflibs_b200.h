@@ -139,6 +139,76 @@ perflibs_status_t perflibs_b200_spmat_export_bsr_d(
     perflibs_spmat_t A, int32_t *bs, int32_t *nnzb, int32_t **row_ptr,
     int32_t **col_indx, double **vals);
 
+/* ---- creation from device arrays ---------------------------------------
+ * A CSR handle whose arrays already live in HBM (0- or 1-based, as
+ * row_ptr[0] says; the arrays are copied, the caller keeps ownership). */
+perflibs_status_t perflibs_b200_spmat_create_csr_d_dev(
+    perflibs_spmat_t *A, int32_t m, int32_t n, const int32_t *row_ptr,
+    const int32_t *col_indx, const double *vals, void *stream);
+
+/* ---- structure statistics -----------------------------------------------
+ * PERFLIBS_B200_NFEATURES statistics of a CSR handle, computed on the
+ * device, in this order:
+ *   0 log2(m+1)        1 log2(n+1)        2 log2(nnz+1)
+ *   3 mean row length  4 row length std   5 skew    6 excess kurtosis
+ *   7 log2(1+min len)  8 log2(1+max len)  9 empty-row fraction
+ *  10 log2(1+p50 len) 11 log2(1+p90 len) 12 log2(1+p99 len)
+ *  13 log2(max/mean)  14 mean |i-j|/n      15 max |i-j|/n (bandwidth)
+ *  16 fraction of nonzeros with |i-j| <= 32
+ *  17 block fill at bs 2   18 at bs 4   19 at bs 8   (nnz / (bs^2 * blocks))
+ *  20 SELL beta C=8 sigma=0   21 C=32 sigma=0   22 C=32 sigma=1024
+ *  23 log2(1+mgmd), mgmd the reference's mean geometric distance between
+ *     consecutive nonzeros of a row (src/matrix_statistics.cpp:23-93). */
+#define PERFLIBS_B200_NFEATURES 24
+perflibs_status_t perflibs_b200_spmat_features(perflibs_spmat_t A,
+                                               float *features);
+
+/* ---- learned format / parameter selector ---------------------------------
+ * An MLP NFEATURES -> 64 -> 64 -> n_classes (ReLU, softmax), FP32, trained
+ * and run by the library's own CUDA kernels. Class c is candidate c of the
+ * exhaustive tuner (perflibs_b200_tune_candidates). */
+typedef struct perflibs_b200_selector_s *perflibs_b200_selector_t;
+
+/* The tuner's candidate list: cfg4 rows of (kind, C, sigma, tpr). */
+perflibs_status_t perflibs_b200_tune_candidates(int32_t cap, int32_t *cfg4,
+                                                int32_t *count);
+
+perflibs_status_t perflibs_b200_selector_create(perflibs_b200_selector_t *S,
+                                                int32_t n_classes,
+                                                uint64_t seed);
+perflibs_status_t perflibs_b200_selector_destroy(perflibs_b200_selector_t S);
+/* Parameter vector (W1, b1, W2, b2, W3, b3, then the 2*NFEATURES feature
+ * normalisation mean / inverse std): count, read, write. */
+int64_t perflibs_b200_selector_param_count(perflibs_b200_selector_t S);
+perflibs_status_t perflibs_b200_selector_get_params(perflibs_b200_selector_t S,
+                                                    float *params);
+perflibs_status_t perflibs_b200_selector_set_params(perflibs_b200_selector_t S,
+                                                    const float *params);
+/* Mean soft-target cross-entropy over n samples (host arrays X[n][NF],
+ * T[n][n_classes]) and its gradient w.r.t. the trainable parameters
+ * (grad has the trainable-parameter count = param_count - 2*NFEATURES). */
+perflibs_status_t perflibs_b200_selector_loss_grad(perflibs_b200_selector_t S,
+                                                   const float *X,
+                                                   const float *T, int32_t n,
+                                                   float *loss, float *grad);
+/* Adam training on the device: the feature normalisation is fitted to X
+ * first; one epoch = all samples in shuffled mini-batches; each step is a
+ * CUDA graph replay. */
+perflibs_status_t perflibs_b200_selector_train(perflibs_b200_selector_t S,
+                                               const float *X, const float *T,
+                                               int32_t n, int32_t epochs,
+                                               int32_t batch, float lr,
+                                               uint64_t seed,
+                                               float *final_loss);
+/* Class probabilities (n x n_classes) and argmax classes. */
+perflibs_status_t perflibs_b200_selector_predict(perflibs_b200_selector_t S,
+                                                 const float *X, int32_t n,
+                                                 float *probs, int32_t *cls);
+/* Use S when the handle's tuner is PERFLIBS_B200_TUNE_SELECTOR. The selector
+ * must outlive the handle's optimize calls. */
+perflibs_status_t perflibs_b200_spmat_set_selector(perflibs_spmat_t A,
+                                                   perflibs_b200_selector_t S);
+
 /* Library / device information: SM count, L2 bytes, device ordinal. */
 perflibs_status_t perflibs_b200_device_info(int32_t *sm_count,
                                             int64_t *l2_bytes,

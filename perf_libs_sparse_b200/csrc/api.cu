@@ -1193,6 +1193,23 @@ perflibs_status_t perflibs_spmv_optimize(perflibs_spmat_t A) {
       return PERFLIBS_STATUS_SUCCESS;
     if (A->fmt == Fmt::BSR)
       return PERFLIBS_STATUS_SUCCESS;  // the BSR kernel is kept, as the reference keeps BSR
+    if (A->tuner == PERFLIBS_B200_TUNE_SELECTOR && A->selector) {
+      // Learned selector: features on the device, one MLP forward pass,
+      // the predicted candidate applied without timing anything.
+      float f[PERFLIBS_B200_NFEATURES];
+      compute_features(A, f);
+      int32_t cls = -1;
+      const auto cands = tune_candidates(A);
+      if (perflibs_b200_selector_predict(A->selector, f, 1, nullptr, &cls) ==
+              PERFLIBS_STATUS_SUCCESS &&
+          cls >= 0 && cls < (int32_t)cands.size()) {
+        apply_config(A, cands[cls]);
+        A->selector_class = cls;
+        A->tuned = true;
+        A->tuned_op = op;
+        return PERFLIBS_STATUS_SUCCESS;
+      }
+    }
     tune_spmv(A);
     A->tuned = true;
     A->tuned_op = op;
@@ -1598,6 +1615,101 @@ perflibs_status_t perflibs_b200_spmat_export_bsr_d(perflibs_spmat_t A, int32_t *
     *vals = v;
     return PERFLIBS_STATUS_SUCCESS;
   });
+}
+
+perflibs_status_t perflibs_b200_spmat_create_csr_d_dev(perflibs_spmat_t *out, int32_t m,
+                                                      int32_t n, const int32_t *row_ptr,
+                                                      const int32_t *col_indx, const double *vals,
+                                                      void *stream) {
+  if (!out)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  Mat *A = nullptr;
+  try {
+    A = new_mat(Dt::F64, Fmt::CSR);
+  } catch (const Error &e) {
+    *out = nullptr;
+    return e.status;
+  }
+  *out = A;
+  return guarded(A, [&]() -> perflibs_status_t {
+    if (m < 0)
+      return param_error(A, 2);
+    if (n < 0)
+      return param_error(A, 3);
+    if (!row_ptr)
+      return param_error(A, 4);
+    cudaStream_t s = stream ? (cudaStream_t)stream : stream_of(A);
+    int32_t ends[2] = {0, 0};
+    PLS_CUDA(cudaMemcpyAsync(&ends[0], row_ptr, 4, cudaMemcpyDeviceToHost, s));
+    PLS_CUDA(cudaMemcpyAsync(&ends[1], row_ptr + m, 4, cudaMemcpyDeviceToHost, s));
+    PLS_CUDA(cudaStreamSynchronize(s));
+    if (ends[0] != 0 && ends[0] != 1)
+      return param_error(A, 4);
+    A->m = m;
+    A->n = n;
+    A->index_base = ends[0];
+    A->nnz = (int64_t)ends[1] - ends[0];
+    if (A->nnz < 0)
+      return param_error(A, 4, "row_ptr[m] is below row_ptr[0]");
+    CsrDev &c = A->csr;
+    c.nnz = A->nnz;
+    c.vt = Vt::F64;
+    c.row_ptr.reserve(4 * ((size_t)m + 1));
+    c.col.reserve(std::max<size_t>(4 * A->nnz, 16));
+    c.vals.reserve(std::max<size_t>(8 * A->nnz, 16));
+    PLS_CUDA(cudaMemcpyAsync(c.row_ptr.p, row_ptr, 4 * ((size_t)m + 1), cudaMemcpyDeviceToDevice, s));
+    if (A->nnz) {
+      PLS_CUDA(cudaMemcpyAsync(c.col.p, col_indx, 4 * A->nnz, cudaMemcpyDeviceToDevice, s));
+      PLS_CUDA(cudaMemcpyAsync(c.vals.p, vals, 8 * A->nnz, cudaMemcpyDeviceToDevice, s));
+    }
+    if (A->index_base) {
+      k_sub_base<<<(unsigned)div_up((int64_t)m + 1, 256), 256, 0, s>>>((int64_t)m + 1, 1,
+                                                                        c.row_ptr.as<int32_t>());
+      if (A->nnz)
+        k_sub_base<<<(unsigned)div_up(A->nnz, 256), 256, 0, s>>>(A->nnz, 1, c.col.as<int32_t>());
+      PLS_LAUNCH_CHECK();
+    }
+    PLS_CUDA(cudaStreamSynchronize(s));
+    A->cfg = default_config(A);
+    return PERFLIBS_STATUS_SUCCESS;
+  });
+}
+
+perflibs_status_t perflibs_b200_spmat_features(perflibs_spmat_t A, float *features) {
+  if (!A || !features)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  return guarded(A, [&]() -> perflibs_status_t {
+    DeviceGuard g(A->device);
+    bsr_become_csr(A);
+    if (A->fmt != Fmt::CSR && A->fmt != Fmt::SELL)
+      return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+    compute_features(A, features);
+    return PERFLIBS_STATUS_SUCCESS;
+  });
+}
+
+perflibs_status_t perflibs_b200_tune_candidates(int32_t cap, int32_t *cfg4, int32_t *count) {
+  if (!count)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  const auto c = tune_candidates(nullptr);
+  for (int32_t i = 0; i < std::min<int32_t>(cap, (int32_t)c.size()); ++i) {
+    if (cfg4) {
+      cfg4[4 * i + 0] = (int)c[i].kind;
+      cfg4[4 * i + 1] = c[i].C;
+      cfg4[4 * i + 2] = c[i].sigma;
+      cfg4[4 * i + 3] = c[i].tpr;
+    }
+  }
+  *count = (int32_t)c.size();
+  return PERFLIBS_STATUS_SUCCESS;
+}
+
+perflibs_status_t perflibs_b200_spmat_set_selector(perflibs_spmat_t A, perflibs_b200_selector_t S) {
+  if (!A)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  A->selector = S;
+  A->tuned = false;
+  return PERFLIBS_STATUS_SUCCESS;
 }
 
 perflibs_status_t perflibs_b200_device_info(int32_t *sm_count, int64_t *l2_bytes,

@@ -546,6 +546,56 @@ void csr_to_bsr(const CsrDev &c, int32_t m, int32_t n, int bs, int layout,
   out = std::move(B);
 }
 
+// Number of distinct bs x bs blocks holding at least one stored entry
+// (m and n need not be multiples of bs here).
+int64_t count_blocks(const CsrDev &c, int32_t m, int32_t n, int bs, cudaStream_t s) {
+  const int64_t nnz = c.nnz;
+  if (nnz == 0)
+    return 0;
+  const int64_t nbc = std::max<int64_t>(div_up(n, bs), 1);
+  const int64_t nbr = std::max<int64_t>(div_up(m, bs), 1);
+  DevBuf row_of, key, idx, key2, idx2, flag, bid;
+  row_of.reserve(4 * nnz);
+  key.reserve(8 * nnz);
+  idx.reserve(4 * nnz);
+  key2.reserve(8 * nnz);
+  idx2.reserve(4 * nnz);
+  flag.reserve(4 * nnz);
+  bid.reserve(4 * nnz);
+  k_row_of_nnz<<<(unsigned)div_up(m, 256), 256, 0, s>>>(m, c.row_ptr.as<int32_t>(),
+                                                         row_of.as<int32_t>());
+  k_block_keys<<<(unsigned)div_up(nnz, 256), 256, 0, s>>>(
+      nnz, bs, nbc, row_of.as<int32_t>(), c.col.as<int32_t>(), key.as<unsigned long long>(),
+      idx.as<int32_t>());
+  int end_bit = 1;
+  while (end_bit < 64 && ((unsigned long long)nbr * nbc >> end_bit) != 0)
+    end_bit++;
+  {
+    size_t tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, key.as<unsigned long long>(),
+                                    key2.as<unsigned long long>(), idx.as<int32_t>(),
+                                    idx2.as<int32_t>(), (int)nnz, 0, end_bit, s);
+    CubTemp tmp;
+    PLS_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(tb), tb, key.as<unsigned long long>(),
+                                             key2.as<unsigned long long>(), idx.as<int32_t>(),
+                                             idx2.as<int32_t>(), (int)nnz, 0, end_bit, s));
+  }
+  k_head_flags<<<(unsigned)div_up(nnz, 256), 256, 0, s>>>(nnz, key2.as<unsigned long long>(),
+                                                           flag.as<int32_t>());
+  {
+    size_t tb = 0;
+    cub::DeviceScan::InclusiveSum(nullptr, tb, flag.as<int32_t>(), bid.as<int32_t>(), (int)nnz, s);
+    CubTemp tmp;
+    PLS_CUDA(cub::DeviceScan::InclusiveSum(tmp.get(tb), tb, flag.as<int32_t>(), bid.as<int32_t>(),
+                                           (int)nnz, s));
+  }
+  PLS_LAUNCH_CHECK();
+  int32_t last = 0;
+  PLS_CUDA(cudaMemcpyAsync(&last, bid.as<int32_t>() + nnz - 1, 4, cudaMemcpyDeviceToHost, s));
+  PLS_CUDA(cudaStreamSynchronize(s));
+  return last;
+}
+
 void csr_build_long_rows(CsrDev &c, int32_t m, int threshold, cudaStream_t s) {
   c.long_threshold = threshold;
   c.n_long = 0;

@@ -229,6 +229,8 @@ struct perflibs_spmat_top_t {
   // Extension state.
   int storage = PERFLIBS_B200_STORAGE_NATIVE;  // requested value storage
   int tuner = PERFLIBS_B200_TUNE_EXHAUSTIVE;
+  perflibs_b200_selector_t selector = nullptr;  // not owned
+  int selector_class = -1;                      // last prediction
   bool forced = false;
   pls::SpmvConfig forced_cfg;
   pls::SpmvConfig cfg;  // active SpMV kernel configuration
@@ -325,6 +327,11 @@ int64_t update_csr_values(CsrDev &c, SellDev *sell, int32_t m, int32_t n,
                           int64_t n_updates, const int32_t *rows_host,
                           const int32_t *cols_host, const void *vals_host,
                           Dt dt, int32_t base, cudaStream_t s);
+
+// Statistics for the learned selector (PERFLIBS_B200_NFEATURES floats).
+void compute_features(const Mat *A, float *out);
+int64_t count_blocks(const CsrDev &c, int32_t m, int32_t n, int bs, cudaStream_t s);
+int64_t sell_padded_size(const CsrDev &c, int32_t m, int C, int sigma, cudaStream_t s);
 
 // Tuning.
 std::vector<SpmvConfig> tune_candidates(const Mat *A);

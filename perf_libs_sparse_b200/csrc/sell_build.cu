@@ -344,6 +344,46 @@ void build_sell(const CsrDev &c, int32_t m, int C, int sigma, SellDev &out,
   out = std::move(S);
 }
 
+// Padded size cs[nC-1] + cl[nC-1]*C of the (C, sigma) layout, without
+// building it (used for the padding-efficiency statistics).
+int64_t sell_padded_size(const CsrDev &c, int32_t m, int C, int sigma, cudaStream_t s) {
+  if (m == 0)
+    return 0;
+  const bool sorted = sigma != 0;
+  const int32_t win = sorted ? sigma : C;
+  const int64_t nC = div_up(m, C);
+  const int64_t nwin = div_up(m, win);
+  const int64_t npos = nwin * win;
+  DevBuf pos_row, pos_len, cl, cs, total;
+  pos_row.reserve(4 * npos);
+  pos_len.reserve(4 * npos);
+  cl.reserve(4 * nC);
+  cs.reserve(8 * nC);
+  total.reserve(8);
+  const int32_t *rp = c.row_ptr.as<int32_t>();
+  if (sorted) {
+    int npow2 = 1;
+    while (npow2 < win)
+      npow2 <<= 1;
+    const size_t smem = sizeof(unsigned long long) * npow2;
+    PLS_CUDA(cudaFuncSetAttribute(k_window_sort, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+    k_window_sort<<<(unsigned)nwin, kSortThreads, smem, s>>>(m, win, npow2, rp, pos_row.as<int32_t>(),
+                                                             pos_len.as<int32_t>());
+  } else {
+    k_identity_positions<<<(unsigned)div_up(npos, 256), 256, 0, s>>>(
+        npos, m, rp, pos_row.as<int32_t>(), pos_len.as<int32_t>());
+  }
+  k_chunk_width<<<(unsigned)div_up(nC, 256), 256, 0, s>>>(nC, C, sorted, pos_len.as<int32_t>(),
+                                                          cl.as<int32_t>());
+  k_chunk_starts<<<1, 1024, 0, s>>>(nC, C, cl.as<int32_t>(), cs.as<int64_t>(), total.as<int64_t>());
+  PLS_LAUNCH_CHECK();
+  int64_t t = 0;
+  PLS_CUDA(cudaMemcpyAsync(&t, total.p, 8, cudaMemcpyDeviceToHost, s));
+  PLS_CUDA(cudaStreamSynchronize(s));
+  return t;
+}
+
 // Split chunks wider than 2*slice_w into column slices of slice_w so that a
 // few very wide chunks (power-law row lengths) spread over many lane groups.
 // Items are ordered widest work first so the long slices start early.

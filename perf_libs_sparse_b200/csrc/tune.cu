@@ -164,8 +164,6 @@ std::vector<SpmvConfig> tune_candidates(const Mat *A) {
     for (int sigma : {0, 32, 256, 1024, 4096, 16384}) {
       if (sigma != 0 && (sigma < C || sigma % C != 0))
         continue;
-      if (sigma > 0 && A && sigma > 4 * std::max(A->m, 1) && sigma > 32)
-        continue;
       SpmvConfig c;
       c.kind = Kind::SELL;
       c.C = C;

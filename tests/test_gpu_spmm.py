@@ -138,7 +138,7 @@ def test_stencil_spmm_storage_modes(storage, tol):
         A = pls.SpMat.csr(m, n, rp, c, v.astype(dt))
         A.set_storage(storage)
         B = pls.SpMat.dense(pls.ROW_MAJOR, n, k, k, Bd.astype(dt).reshape(-1))
-        Cm = pls.SpMat.null(m, k)
+        Cm = pls.SpMat.null(m, k, dtype=dt)
         assert pls.spmm_exec(pls.OPERATION_NOTRANS, pls.OPERATION_NOTRANS, 1.0, A, B, 0.0, Cm) == 0
         got = Cm.export_dense().astype(np.float64)
         assert scaled_err(got, ref, rp, c, v, Bd, 1.0, 0.0, None) <= tol
