@@ -269,7 +269,7 @@ def run_b200(args):
     K, Wm = args.steps, max(args.warmup, 3)
     # Keep the GPU busy ~0.5 s before the timed region so that the clock
     # samples see the kernel under load.
-    soak = max(1, int(0.5 / max(bytes_step / 6.0e12, 1e-6)))
+    soak = max(1, int(args.soak_seconds / max(bytes_step / 6.0e12, 1e-6)))
     with ClockSampler(local) as clk:
         timed(A, soak, 1)
         ms_tuned = timed(A, K, Wm)
@@ -372,6 +372,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--soak-seconds", type=float, default=0.5,
+                    help="untimed load before the timed region, so the clock samples see the GPU busy")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

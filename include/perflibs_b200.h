@@ -102,11 +102,13 @@ perflibs_status_t perflibs_b200_spmat_exec_info(perflibs_spmat_t A,
                                                 int64_t *n_split);
 
 /* Timings the last exhaustive tune measured: up to `cap` rows of
- * (kind, C, sigma, tpr) in cfg4 and milliseconds in ms. Returns the count
- * in *count. */
+ * (kind, C, sigma, tpr) in cfg4, milliseconds in ms and the SELL padding
+ * efficiency nnz / padded size in beta (1 for CSR rows); any output may be
+ * NULL. Returns the count in *count. */
 perflibs_status_t perflibs_b200_spmat_tune_table(perflibs_spmat_t A,
                                                  int32_t cap, int32_t *cfg4,
-                                                 double *ms, int32_t *count);
+                                                 double *ms, double *beta,
+                                                 int32_t *count);
 
 /* The SELL-C-sigma layout held on the device (after optimize picked SELL or
  * after perflibs_b200_spmat_build_sell): info7 = {nC, C, sigma, col_bytes,

@@ -112,7 +112,7 @@ def lib():
             "perflibs_b200_spmat_set_tuner": [vp, i],
             "perflibs_b200_spmat_force_config": [vp, i, i, i, i],
             "perflibs_b200_spmat_get_config": [vp, vp, vp, vp, vp, vp],
-            "perflibs_b200_spmat_tune_table": [vp, i32, vp, vp, vp],
+            "perflibs_b200_spmat_tune_table": [vp, i32, vp, vp, vp, vp],
             "perflibs_b200_spmat_exec_info": [vp, vp, vp, vp],
             "perflibs_b200_spmat_export_sell": [vp, vp, vp, vp, vp, vp, vp, vp, vp],
             "perflibs_b200_spmat_build_sell": [vp, i, i],
@@ -253,13 +253,16 @@ class SpMat:
                "exec_info")
         return {"kernels_per_spmv": k.value, "n_items": it.value, "n_split": sp.value}
 
-    def tune_table(self):
+    def tune_table(self, with_beta=False):
         cnt = C.c_int32()
-        lib().perflibs_b200_spmat_tune_table(self.h, 0, None, None, C.byref(cnt))
+        lib().perflibs_b200_spmat_tune_table(self.h, 0, None, None, None, C.byref(cnt))
         n = cnt.value
         cfg = np.zeros((max(n, 1), 4), np.int32)
         ms = np.zeros(max(n, 1))
-        lib().perflibs_b200_spmat_tune_table(self.h, n, _p(cfg), _p(ms), C.byref(cnt))
+        beta = np.zeros(max(n, 1))
+        lib().perflibs_b200_spmat_tune_table(self.h, n, _p(cfg), _p(ms), _p(beta), C.byref(cnt))
+        if with_beta:
+            return cfg[:n], ms[:n], beta[:n]
         return cfg[:n], ms[:n]
 
     # -------------------------------------------------------- execution

@@ -1460,7 +1460,7 @@ perflibs_status_t perflibs_b200_spmat_exec_info(perflibs_spmat_t A, int32_t *ker
 }
 
 perflibs_status_t perflibs_b200_spmat_tune_table(perflibs_spmat_t A, int32_t cap, int32_t *cfg4,
-                                                 double *ms, int32_t *count) {
+                                                 double *ms, double *beta, int32_t *count) {
   if (!A || !count)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
   const int32_t n = (int32_t)A->tune_table.size();
@@ -1474,6 +1474,8 @@ perflibs_status_t perflibs_b200_spmat_tune_table(perflibs_spmat_t A, int32_t cap
     }
     if (ms)
       ms[i] = t.ms;
+    if (beta)
+      beta[i] = t.beta;
   }
   *count = n;
   return PERFLIBS_STATUS_SUCCESS;

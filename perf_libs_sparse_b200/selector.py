@@ -307,13 +307,11 @@ def build_corpus(n_mats: int, out_dir: str, seed: int = 4, log_every: int = 50):
             A.hint(HINT_SPMV_INVOCATIONS, INVOCATIONS_MANY)
             A.set_tuner(TUNE_EXHAUSTIVE)
             _check(A.optimize(), "optimize")
-            cfg, ms = A.tune_table()
+            cfg, ms, betas = A.tune_table(with_beta=True)
             assert len(ms) == len(cands)
             nnz = int(rp[-1].item())
-            # padding efficiency of every SELL candidate (for the reference rule)
-            betas = np.ones(len(cands))
             d = {"idx": i, "family": fam, "m": m, "n": n, "nnz": nnz, "features": feat.tolist(),
-                 "ms": ms.tolist()}
+                 "ms": ms.tolist(), "beta": betas.tolist()}
             f.write(json.dumps(d) + "\n")
             f.flush()
             done[i] = d
@@ -323,18 +321,6 @@ def build_corpus(n_mats: int, out_dir: str, seed: int = 4, log_every: int = 50):
             if log_every and (i + 1) % log_every == 0:
                 print(f"corpus {i + 1}/{n_mats} {time.time() - t0:.0f}s", flush=True)
     return [done[i] for i in range(n_mats)]
-
-
-def sell_betas(m, n, rp, col, vals, cands):
-    """Padding efficiency of every SELL candidate, from its built layout."""
-    out = np.ones(len(cands))
-    A = create_from_device(m, n, rp, col, vals)
-    for i, c in enumerate(cands):
-        if c[0] == KIND_SELL:
-            _check(A.build_sell(int(c[1]), int(c[2])), "build_sell")
-            s = A.export_sell_info()
-            out[i] = s
-    return out
 
 
 def evaluate(corpus, n_train: int, out_dir: str, epochs=400, batch=128, lr=3e-3, seed=0):
@@ -360,7 +346,10 @@ def evaluate(corpus, n_train: int, out_dir: str, epochs=400, batch=128, lr=3e-3,
     tpr = np.clip(2 ** np.floor(np.log2(np.maximum(mean_len, 1))), 1, 32).astype(int)
     plain_idx = np.array([int(np.flatnonzero((cands[:, 0] == KIND_CSR) & (cands[:, 3] == t))[0]) for t in tpr])
     plain = Th[np.arange(len(Th)), plain_idx]
-    bytes_ = nnz[n_train:] * 12 + (m[n_train:] + 1) * 4 + n[n_train:] * 8 + m[n_train:] * 8
+    betas = np.array([d["beta"] for d in corpus[n_train:]], np.float64)
+    rule_idx = np.array([reference_rule(cands, betas[i], plain_idx[i]) for i in range(len(Th))])
+    rule = Th[np.arange(len(Th)), rule_idx]
+    bytes_ =nnz[n_train:] * 12 + (m[n_train:] + 1) * 4 + n[n_train:] * 8 + m[n_train:] * 8
     rep = {
         "n_train": int(n_train), "n_heldout": int(len(Th)), "n_classes": int(len(cands)),
         "train_final_loss": float(loss), "train_seconds": train_s,
@@ -369,6 +358,9 @@ def evaluate(corpus, n_train: int, out_dir: str, epochs=400, batch=128, lr=3e-3,
         "top1_accuracy": float((cls == Th.argmin(1)).mean()),
         "speedup_vs_plain_csr_geomean": float(np.exp(np.log(plain / chosen).mean())),
         "exhaustive_speedup_vs_plain_csr_geomean": float(np.exp(np.log(plain / best).mean())),
+        "speedup_vs_reference_rule_geomean": float(np.exp(np.log(rule / chosen).mean())),
+        "reference_rule_regret_mean": float((rule / best - 1.0).mean()),
+        "plain_csr_regret_mean": float((plain / best - 1.0).mean()),
         "heldout_gbs_selected_total": float(bytes_.sum() / (chosen.sum() * 1e-3) / 1e9),
         "heldout_gbs_plain_csr_total": float(bytes_.sum() / (plain.sum() * 1e-3) / 1e9),
     }

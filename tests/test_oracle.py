@@ -114,6 +114,25 @@ def test_port_matches_reference_live():
                 assert np.all(np.isfinite(yp))
 
 
+def test_mlp_oracle_gradient_finite_differences():
+    """The CPU restatement of the selector MLP is itself checked against
+    central finite differences (FP64)."""
+    from oracle import selector_ref as R
+
+    K = 7
+    rng = np.random.default_rng(0)
+    P = R.H * R.NF + R.H + R.H * R.H + R.H + K * R.H + K
+    p = np.concatenate([rng.normal(0, 0.3, P), rng.normal(0, 1, R.NF), rng.uniform(0.5, 2, R.NF)])
+    X = rng.normal(0, 1, (10, R.NF))
+    T = rng.dirichlet(np.ones(K), 10)
+    loss, g = R.mlp_loss_grad(p, K, X, T)
+    for i in rng.choice(P, 40, replace=False):
+        e = np.zeros_like(p)
+        e[i] = 1e-6
+        fd = (R.mlp_loss_grad(p + e, K, X, T)[0] - R.mlp_loss_grad(p - e, K, X, T)[0]) / 2e-6
+        assert abs(fd - g[i]) <= 1e-6 + 1e-4 * abs(fd), i
+
+
 def test_scs_spmv_equals_csr():
     from perf_libs_sparse_b200 import workloads as W
     rng = np.random.default_rng(3)
