@@ -30,6 +30,30 @@ perflibs_status_t perflibs_b200_spmv_exec_s_dev(
     enum perflibs_sparse_hint_value trans, float alpha, perflibs_spmat_t A,
     const float *x, float beta, float *y, void *stream);
 
+/* SpMV that allocates no device memory (no counterpart in the reference).
+ *
+ * For callers that cannot call cudaMalloc around their SpMV: code whose
+ * device memory is owned by a pool or caching allocator of its own, and
+ * latency-critical loops where cudaMalloc / cudaFree (which can synchronise
+ * the device) must not run. y = alpha*A*x + beta*y, NOTRANS, on device
+ * pointers, asynchronous on `stream` (NULL = the handle's stream).
+ *
+ * A must already hold its SELL-C-sigma layout (perflibs_spmv_optimize chose
+ * SELL, or perflibs_b200_spmat_build_sell / force_config + optimize); other
+ * formats return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR. The partial sums of
+ * sliced wide chunks go to one fixed 16 MiB device array (2^21 FP64
+ * elements) that every GPU loading the library holds until exit; a matrix
+ * that needs more returns PERFLIBS_STATUS_INPUT_PARAMETER_ERROR with the
+ * sizes in the handle's error message. The first call on a device looks the
+ * array's address up (cudaGetSymbolAddress), so make that first call before
+ * any stream capture. All calls share the array: calls that overlap on the
+ * GPU race, so serialise them (one stream, or events between streams). */
+perflibs_status_t perflibs_b200_spmv_exec_d_noalloc(double alpha,
+                                                    perflibs_spmat_t A,
+                                                    const double *x,
+                                                    double beta, double *y,
+                                                    void *stream);
+
 /* C = alpha*A*B + beta*C for a sparse A (NOTRANS), row-major dense device
  * B (ldb >= k) and C (ldc >= k) with k columns. beta == 0 overwrites C. */
 perflibs_status_t perflibs_b200_spmm_exec_d_dev(double alpha,

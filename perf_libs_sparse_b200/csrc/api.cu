@@ -1338,6 +1338,36 @@ perflibs_status_t perflibs_b200_spmv_exec_s_dev(enum perflibs_sparse_hint_value 
   return spmv_exec_dev<float>(trans, alpha, A, x, beta, y, stream);
 }
 
+// No device allocation on this path: no staging buffers, no format or
+// storage conversion, no tuning — only the SELL kernels, with their
+// partial sums in the library's fixed scratch array.
+perflibs_status_t perflibs_b200_spmv_exec_d_noalloc(double alpha, perflibs_spmat_t A,
+                                                    const double *x, double beta, double *y,
+                                                    void *stream) {
+  if (!A)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  return guarded(A, [&]() -> perflibs_status_t {
+    if (A->dt != Dt::F64)
+      return param_error(A, 2, "The matrix handle has a different data type.");
+    if (A->fmt != Fmt::SELL)
+      return param_error(A, 2, "The allocation-free SpMV needs a handle holding its SELL-C-sigma "
+                               "layout (optimize it first).");
+    if (A->sell.vt != A->csr.evt())
+      return param_error(A, 2, "The storage mode changed since optimize; optimize again.");
+    if (!x || !y)
+      return param_error(A, !x ? 3 : 5);
+    DeviceGuard g(A->device);
+    cudaStream_t s = stream ? (cudaStream_t)stream : stream_of(A);
+    if (alpha == 0.0) {
+      scal<double>(A->m, beta, y, s);
+      return PERFLIBS_STATUS_SUCCESS;
+    }
+    spmv_sell_scratch<double>(A->sell, x, y, alpha, beta, noalloc_scratch_address(A->device),
+                              noalloc_scratch_capacity(), s);
+    return PERFLIBS_STATUS_SUCCESS;
+  });
+}
+
 }  // extern "C"
 
 template <class X>

@@ -273,6 +273,13 @@ void spmv_sell(const SellDev &s, const X *x, X *y, X alpha, X beta,
 template <class X>
 void spmv_bsr(const BsrDev &b, const X *x, X *y, X alpha, X beta,
               cudaStream_t s);
+// Allocation-free variant of spmv_sell: partial sums in a fixed device
+// array (see spmv.cu).
+int64_t noalloc_scratch_capacity();
+void *noalloc_scratch_address(int device);
+template <class X>
+void spmv_sell_scratch(const SellDev &s, const X *x, X *y, X alpha, X beta,
+                       void *scratch, int64_t capacity, cudaStream_t st);
 template <class X>
 void spmv_csr_trans(const CsrDev &c, int32_t m, int32_t n, const X *x, X *y,
                     X alpha, X beta, cudaStream_t s);

@@ -9,6 +9,8 @@
 //     result depends only on that row (no atomics on the NOTRANS path);
 //   * grids launch one thread group per row / chunk and let the block
 //     scheduler balance uneven rows across the 148 SMs.
+#include <mutex>
+
 #include "common.cuh"
 #include "pls_internal.hpp"
 
@@ -345,6 +347,86 @@ void spmv_sell(const SellDev &s, const X *x, X *y, X alpha, X beta,
   });
   PLS_LAUNCH_CHECK();
 }
+
+// -------------------------------------- SELL SpMV without allocation
+
+// Scratch of the allocation-free SELL entry point: the partial sums of the
+// column slices of wide chunks, in a fixed device array instead of a
+// per-handle cudaMalloc buffer. Every GPU that loads the library holds these
+// 16 MiB until the process exits. All calls share it, so calls that overlap
+// on the GPU (different streams, or different host threads) race on it.
+constexpr int64_t kNoAllocScratchElems = int64_t(1) << 21;  // FP64 elements
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchElems];
+
+namespace {
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[64] = {};
+}  // namespace
+
+int64_t noalloc_scratch_capacity() { return kNoAllocScratchElems; }
+
+// Device address of the scratch array for `device`. In host code the array's
+// name is only a host-side stand-in, so the address comes from
+// cudaGetSymbolAddress, once per device, with that device current (the
+// caller's DeviceGuard makes it current).
+void *noalloc_scratch_address(int device) {
+  std::lock_guard<std::mutex> g(g_noalloc_mu);
+  void *&a = g_noalloc_addr[device & 63];
+  if (!a) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+      throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE,
+                  std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    a = p;
+  }
+  return a;
+}
+
+// The sliced SELL SpMV (k_sell_items + k_sell_combine, or k_sell when no
+// chunk is sliced) with its partial sums in `scratch` (capacity in FP64
+// elements). Every slot a call reads was written earlier in the same call,
+// so nothing needs clearing between calls.
+template <class X>
+void spmv_sell_scratch(const SellDev &s, const X *x, X *y, X alpha, X beta, void *scratch,
+                       int64_t capacity, cudaStream_t st) {
+  if (s.nC == 0)
+    return;
+  const int64_t slots = s.n_split > 0 ? (int64_t)(s.part.bytes / (sizeof(double) * s.C)) : 0;
+  if (slots * s.C > capacity)
+    throw Error(PERFLIBS_STATUS_INPUT_PARAMETER_ERROR,
+                "this matrix needs " + std::to_string(slots * s.C) +
+                    " scratch elements; the fixed scratch holds " + std::to_string(capacity));
+  SellDev view;  // the handle's layout, partial sums redirected to `scratch`
+  view.C = s.C;
+  view.nC = s.nC;
+  view.col_bytes = s.col_bytes;
+  view.vt = s.vt;
+  view.n_items = s.n_items;
+  view.n_split = s.n_split;
+  view.cs.p = s.cs.p;
+  view.cl.p = s.cl.p;
+  view.col_min.p = s.col_min.p;
+  view.permd2in.p = s.permd2in.p;
+  view.vals.p = s.vals.p;
+  view.offsets.p = s.offsets.p;
+  view.items.p = s.items.p;
+  view.split_chunks.p = s.split_chunks.p;
+  view.part.p = scratch;
+  try {
+    spmv_sell<X>(view, x, y, alpha, beta, st);
+  } catch (...) {
+    // `view` borrows every pointer: release nothing.
+    view.cs.p = view.cl.p = view.col_min.p = view.permd2in.p = nullptr;
+    view.vals.p = view.offsets.p = view.items.p = view.split_chunks.p = view.part.p = nullptr;
+    throw;
+  }
+  view.cs.p = view.cl.p = view.col_min.p = view.permd2in.p = nullptr;
+  view.vals.p = view.offsets.p = view.items.p = view.split_chunks.p = view.part.p = nullptr;
+}
+
+template void spmv_sell_scratch<double>(const SellDev &, const double *, double *, double,
+                                        double, void *, int64_t, cudaStream_t);
 
 // ------------------------------------------------------------ transpose
 
