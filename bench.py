@@ -245,7 +245,7 @@ def run_b200(args):
     def step(M):
         M.spmv_dev(xd.data_ptr(), yd.data_ptr(), 1.0, 0.0, sp)
 
-    def timed(M, K, Wm):
+    def timed(M, K, Wm, label="untimed"):
         with torch.cuda.stream(stream):
             for _ in range(Wm):
                 step(M)
@@ -254,11 +254,13 @@ def run_b200(args):
                 torch.distributed.barrier()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.nvtx.range_push(label)
             e0.record(stream)
             for _ in range(K):
                 step(M)
             e1.record(stream)
             torch.cuda.synchronize()
+            torch.cuda.nvtx.range_pop()
             ms = e0.elapsed_time(e1)
         if world > 1:
             t = torch.tensor([ms], device=dev)
@@ -272,7 +274,7 @@ def run_b200(args):
     soak = max(1, int(args.soak_seconds / max(bytes_step / 6.0e12, 1e-6)))
     with ClockSampler(local) as clk:
         timed(A, soak, 1)
-        ms_tuned = timed(A, K, Wm)
+        ms_tuned = timed(A, K, Wm, "timed")
     ms_plain = timed(A_plain, K, Wm)
 
     # Parity of the timed result (full size) against the oracle.
@@ -365,8 +367,136 @@ def run_b200(args):
     return 0
 
 
+def run_extra(args):
+    """Non-default workloads, one JSON line each (N = 1):
+    c1  FP64 CSR SpMV, 5-point Laplacian 512^2 (21 MB: L2-resident, so a
+        256 MB buffer is written between steps and only the SpMV is timed);
+    c3  CSR SpMM on the 27-point 128^3 stencil, k = --k, value storage
+        --storage (native = FP64 A, B, C; fp32 / bf16 = FP32 B, C and FP32 /
+        BF16 A values, FP32 accumulation), max relative error vs the FP64
+        oracle reported;
+    c4  the 512-instance uneven batch (FP32) in one persistent launch per
+        step (a CUDA graph), row tile picked by the batch autotuner."""
+    import torch
+
+    import oracle
+    import perf_libs_sparse_b200 as pls
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    hbm, peak_kind = peaks()
+    K, Wm = args.steps, max(args.warmup, 3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(step, flush=None):
+        with torch.cuda.stream(stream):
+            for _ in range(Wm):
+                step()
+            torch.cuda.synchronize()
+            if flush is None:
+                e0.record(stream)
+                for _ in range(K):
+                    step()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                return e0.elapsed_time(e1) / K
+            tot = 0.0
+            for _ in range(K):
+                flush()
+                e0.record(stream)
+                step()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                tot += e0.elapsed_time(e1)
+            return tot / K
+
+    line = {"n_gpus": 1, "steps": K, "warmup": Wm, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "data": "synthetic", "unit": "GB/s"}
+    if args.workload == "c1":
+        m, n, rp, c, v = W.laplacian_2d(512)
+        x = W.uniform_vector(n, 0)
+        A = pls.SpMat.csr(m, n, rp, c, v)
+        A.set_stream(sp)
+        assert A.optimize() == 0
+        xd = torch.tensor(x, device="cuda")
+        yd = torch.zeros(m, dtype=torch.float64, device="cuda")
+        flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        ms = timed(lambda: A.spmv_dev(xd.data_ptr(), yd.data_ptr(), 1.0, 0.0, sp),
+                   flush=lambda: flush_buf.fill_(1))
+        torch.cuda.synchronize()
+        y = yd.cpu().numpy()
+        y_ref = oracle.csr_spmv(rp, c, v, x)
+        sc = oracle.csr_absdot(rp, c, v, x)
+        err = float((np.abs(y - y_ref) / np.maximum(np.maximum(np.abs(y_ref), sc), 1e-300)).max())
+        b = W.algorithmic_bytes_spmv(m, n, int(rp[-1]), 8, 8, False)
+        line.update(metric="SpMV GB/s (algorithmic bytes), FP64, 2D Laplacian 512^2", dtype="f64",
+                    value=b / ms / 1e6, ms_per_step=ms, max_rel_err=err,
+                    config={"workload": "C1 Laplacian 512x512 n=262144 nnz=1308672", **A.config(),
+                            "l2": "256 MB written between steps, SpMV alone timed"})
+    elif args.workload == "c3":
+        m, n, rp, c, v = W.stencil_27pt(128, seed=2)
+        k = args.k
+        B = np.random.default_rng(2).uniform(-1, 1, (n, k))
+        native = args.storage == "native"
+        dt = np.float64 if native else np.float32
+        tdt = torch.float64 if native else torch.float32
+        A = pls.SpMat.csr(m, n, rp, c, v.astype(dt))
+        A.set_storage({"native": pls.STORAGE_NATIVE, "fp32": pls.STORAGE_FP32, "bf16": pls.STORAGE_BF16}[args.storage])
+        A.set_stream(sp)
+        assert A.optimize() == 0
+        Bd = torch.tensor(B, dtype=tdt, device="cuda")
+        Cd = torch.zeros((m, k), dtype=tdt, device="cuda")
+        ms = timed(lambda: A.spmm_dev(Bd.data_ptr(), k, k, Cd.data_ptr(), k, 1.0, 0.0, sp))
+        torch.cuda.synchronize()
+        got = Cd.cpu().numpy().astype(np.float64)
+        rows = np.random.default_rng(7).choice(m, 20000, replace=False)
+        rows.sort()
+        # error on a row sample against the FP64 oracle (same seeds)
+        sub_rp = np.concatenate([[0], np.cumsum(rp[rows + 1] - rp[rows])]).astype(np.int32)
+        idx = np.concatenate([np.arange(rp[r], rp[r + 1]) for r in rows])
+        ref = oracle.csr_spmm(sub_rp, c[idx], v[idx], B, k)
+        scale = oracle.csr_spmm(sub_rp, c[idx], np.abs(v[idx]), np.abs(B), k)
+        err = float((np.abs(got[rows] - ref) / np.maximum(np.maximum(np.abs(ref), scale), 1e-300)).max())
+        sv = 8 if native else (4 if args.storage == "fp32" else 2)
+        sb = 8 if native else 4
+        b = W.algorithmic_bytes_spmm(m, n, int(rp[-1]), k, sv, sb, False)
+        line.update(metric=f"SpMM GB/s (algorithmic bytes), 27-point 128^3, k={k}, storage {args.storage}",
+                    dtype={"native": "f64", "fp32": "f32", "bf16": "bf16 values, f32 accumulate"}[args.storage],
+                    value=b / ms / 1e6, ms_per_step=ms, max_rel_err=err, gflops=2.0 * int(rp[-1]) * k / ms / 1e6,
+                    config={"workload": "C3 27-point stencil 128^3 n=2097152 nnz=55742968", "k": k,
+                            "storage": args.storage, "l2": "inputs exceed L2; no flush"})
+    elif args.workload == "c4":
+        inst = W.batched_instances(512, seed=3)
+        mats, Bs, Cs = [], [], []
+        for d in inst:
+            if d["kind"] == "bsr":
+                mats.append(pls.SpMat.bsr(d["layout"], d["m"], d["n"], d["bs"], d["row_ptr"], d["col"], d["vals"]))
+            else:
+                mats.append(pls.SpMat.csr(d["m"], d["n"], d["row_ptr"], d["col"], d["vals"]))
+            Bs.append(torch.tensor(d["B"], device="cuda"))
+            Cs.append(torch.zeros((d["m"], d["k"]), dtype=torch.float32, device="cuda"))
+        ks = [d["k"] for d in inst]
+        bt = pls.Batch(mats, ks, [b_.data_ptr() for b_ in Bs], ks, [c_.data_ptr() for c_ in Cs], ks, stream=sp)
+        tile, _ = bt.tune()
+        ms = timed(lambda: bt.exec(1.0, 0.0))
+        b = sum(W.algorithmic_bytes_spmm(d["m"], d["n"], W.instance_nnz(d), d["k"], 4, 4, False) for d in inst)
+        line.update(metric="Batched SpMM GB/s (algorithmic bytes), 512 uneven FP32 instances, one persistent launch",
+                    dtype="f32", value=b / ms / 1e6, ms_per_step=ms,
+                    config={"workload": "C4 512 instances n in [1024, 65536], k in [1, 64]", "tile_rows": tile,
+                            **bt.info(), "rows_total": int(sum(d["m"] for d in inst))})
+    line["roofline"] = {"bound": "hbm", "achieved": line["value"], "peak": hbm, "unit": "GB/s",
+                        "frac": line["value"] / hbm, "peak_source": peak_kind}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4"],
+                    help="c2 (default, the headline) or one of the other configurations")
+    ap.add_argument("--k", type=int, default=32, help="right-hand sides for --workload c3")
+    ap.add_argument("--storage", default="native", choices=["native", "fp32", "bf16"])
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
@@ -377,6 +507,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "c2":
+        return run_extra(args)
     return run_b200(args)
 
 

@@ -235,6 +235,35 @@ perflibs_status_t perflibs_b200_selector_predict(perflibs_b200_selector_t S,
 perflibs_status_t perflibs_b200_spmat_set_selector(perflibs_spmat_t A,
                                                    perflibs_b200_selector_t S);
 
+/* ---- batched uneven SpMM ---------------------------------------------------
+ * Many independent products C_i = alpha*A_i*B_i + beta*C_i (FP32 CSR or BSR
+ * handles A_i, each with its own row-major device B_i (ldb_i) and C_i
+ * (ldc_i) and its own k_i) in ONE persistent kernel launch: a work list of
+ * (instance, row tile) items is consumed by a grid sized to the SMs through
+ * an atomic counter, so uneven instances balance without waits. exec
+ * replays a CUDA graph holding the counter reset and the launch. */
+typedef struct perflibs_b200_batch_s *perflibs_b200_batch_t;
+perflibs_status_t perflibs_b200_batch_create(
+    perflibs_b200_batch_t *Bt, int32_t count, const perflibs_spmat_t *mats,
+    const int32_t *k, const float *const *B, const int64_t *ldb,
+    float *const *C, const int64_t *ldc, void *stream);
+/* Rows per work item (0 = the autotuned value). */
+perflibs_status_t perflibs_b200_batch_set_tile(perflibs_b200_batch_t Bt,
+                                               int32_t rows_per_item);
+/* Time each candidate tile (rows per item) and keep the fastest;
+ * best_tile / best_ms may be NULL. */
+perflibs_status_t perflibs_b200_batch_tune(perflibs_b200_batch_t Bt,
+                                           int32_t *best_tile,
+                                           float *best_ms);
+perflibs_status_t perflibs_b200_batch_exec(perflibs_b200_batch_t Bt,
+                                           float alpha, float beta);
+/* Work items and kernel launches of one exec. */
+perflibs_status_t perflibs_b200_batch_info(perflibs_b200_batch_t Bt,
+                                           int64_t *n_items,
+                                           int32_t *launches_per_exec,
+                                           int32_t *tile);
+perflibs_status_t perflibs_b200_batch_destroy(perflibs_b200_batch_t Bt);
+
 /* Library / device information: SM count, L2 bytes, device ordinal. */
 perflibs_status_t perflibs_b200_device_info(int32_t *sm_count,
                                             int64_t *l2_bytes,

@@ -398,6 +398,62 @@ class SpMat:
             pass
 
 
+class Batch:
+    """perflibs_b200_batch_t: many independent FP32 SpMMs in one persistent
+    launch. B and C are lists of device pointers (int) with their leading
+    dimensions; the handles must stay unchanged while the batch exists."""
+
+    def __init__(self, mats, ks, Bptrs, ldbs, Cptrs, ldcs, stream: int = 0):
+        L = lib()
+        vp = C.c_void_p
+        for name, args in {"perflibs_b200_batch_create": [vp, C.c_int32, vp, vp, vp, vp, vp, vp, vp],
+                           "perflibs_b200_batch_set_tile": [vp, C.c_int32],
+                           "perflibs_b200_batch_tune": [vp, vp, vp],
+                           "perflibs_b200_batch_exec": [vp, C.c_float, C.c_float],
+                           "perflibs_b200_batch_info": [vp, vp, vp, vp],
+                           "perflibs_b200_batch_destroy": [vp]}.items():
+            getattr(L, name).argtypes = args
+            getattr(L, name).restype = C.c_int
+        n = len(mats)
+        self._mats = list(mats)  # keep the handles alive
+        hs = (C.c_void_p * n)(*[m.h.value for m in mats])
+        k = np.ascontiguousarray(ks, np.int32)
+        ldb = np.ascontiguousarray(ldbs, np.int64)
+        ldc = np.ascontiguousarray(ldcs, np.int64)
+        bp = (C.c_void_p * n)(*Bptrs)
+        cp = (C.c_void_p * n)(*Cptrs)
+        self.h = C.c_void_p()
+        _check(L.perflibs_b200_batch_create(C.byref(self.h), n, hs, _p(k), bp, _p(ldb), cp, _p(ldc),
+                                            C.c_void_p(stream)), "batch_create")
+
+    def tune(self):
+        t, ms = C.c_int32(), C.c_float()
+        _check(lib().perflibs_b200_batch_tune(self.h, C.byref(t), C.byref(ms)), "batch_tune")
+        return t.value, ms.value
+
+    def set_tile(self, rows):
+        _check(lib().perflibs_b200_batch_set_tile(self.h, rows), "batch_set_tile")
+
+    def exec(self, alpha=1.0, beta=0.0):
+        _check(lib().perflibs_b200_batch_exec(self.h, alpha, beta), "batch_exec")
+
+    def info(self):
+        n, l, t = C.c_int64(), C.c_int32(), C.c_int32()
+        _check(lib().perflibs_b200_batch_info(self.h, C.byref(n), C.byref(l), C.byref(t)), "batch_info")
+        return {"n_items": n.value, "launches": l.value, "tile": t.value}
+
+    def destroy(self):
+        if self.h is not None and self.h.value:
+            lib().perflibs_b200_batch_destroy(self.h)
+        self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
 def spmm_optimize(transA, transB, alpha_hint, A: SpMat, B: SpMat, beta_hint, Cm: SpMat):
     return lib().perflibs_spmm_optimize(transA, transB, alpha_hint, A.h, B.h, beta_hint, Cm.h)
 

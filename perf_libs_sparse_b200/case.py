@@ -59,7 +59,10 @@ def main():
         A.force_config(KIND_CSR_SPLIT, 0, 0, args.tpr or 1024)
     assert A.optimize() == 0
     tdt = torch.float32 if args.fp32_api else torch.float64
-    s = torch.cuda.current_stream()
+    # A dedicated stream: the library's device entry points treat a NULL
+    # stream as "the handle's own stream", so torch's default stream (handle
+    # 0) would not be the stream the events below are recorded on.
+    s = torch.cuda.Stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if args.k > 0:
         B = torch.rand((n, args.k), dtype=tdt, device="cuda") * 2 - 1

@@ -1,0 +1,359 @@
+// Batched uneven SpMM in one persistent launch.
+//
+// Instances are FP32 CSR or BSR handles, each with its own dense row-major
+// B_i / C_i and k_i. The work is cut into items of R rows (R block-aligned
+// for BSR), sorted by estimated work (rows x nonzeros per row x k, largest
+// first), and consumed by a grid of (SMs x resident blocks) CTAs: each warp
+// takes the next item from a global atomic counter until the list is empty.
+// Nothing ever waits on another warp, so there is no spin and no deadlock
+// whatever the scheduling; the counter is reset by a memset node in the same
+// CUDA graph that holds the launch.
+//
+// Inside an item, a group of L lanes (L = the power of two covering k_i,
+// at most 32) owns one row: lane s accumulates columns s, s+L, ... of the
+// row's output over the row's nonzeros in stored order (CSR), or over the
+// block row's blocks and each block's columns (BSR).
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "common.cuh"
+#include "pls_internal.hpp"
+
+namespace pls {
+
+namespace {
+
+struct InstDesc {
+  const int32_t *rp;
+  const int32_t *col;
+  const float *val;
+  const float *B;
+  float *C;
+  int64_t ldb, ldc;
+  int32_t m, k, bs, layout, lanes, is_bsr;
+};
+
+struct Item {
+  int32_t inst, row0, row1, pad;
+};
+
+constexpr int kMaxColsPerLane = 4;  // k <= 32 * 4 per pass
+
+__global__ void __launch_bounds__(256)
+    k_batch_spmm(const InstDesc *__restrict__ inst, const Item *__restrict__ items,
+                 int64_t n_items, unsigned long long *__restrict__ counter, float alpha,
+                 float beta, int beta_nz) {
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    unsigned long long it = 0;
+    if (lane == 0)
+      it = atomicAdd(counter, 1ull);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    if (it >= (unsigned long long)n_items)
+      return;
+    const Item w = items[it];
+    const InstDesc d = inst[w.inst];
+    const int L = d.lanes;
+    const int g = lane / L, s = lane % L, groups = 32 / L;
+    for (int32_t r = w.row0 + g; r < w.row1; r += groups) {
+      for (int kk0 = 0; kk0 < d.k; kk0 += L * kMaxColsPerLane) {
+        float acc[kMaxColsPerLane];
+#pragma unroll
+        for (int q = 0; q < kMaxColsPerLane; ++q)
+          acc[q] = 0.f;
+        if (!d.is_bsr) {
+          for (int32_t p = d.rp[r]; p < d.rp[r + 1]; ++p) {
+            const float a = ld_stream(d.val + p);
+            const float *brow = d.B + (int64_t)ld_stream(d.col + p) * d.ldb;
+#pragma unroll
+            for (int q = 0; q < kMaxColsPerLane; ++q) {
+              const int kk = kk0 + s + q * L;
+              if (kk < d.k)
+                acc[q] = fmaf(a, __ldg(brow + kk), acc[q]);
+            }
+          }
+        } else {
+          const int bs = d.bs;
+          const int32_t br = r / bs;
+          const int i = r % bs;
+          const int64_t E = (int64_t)bs * bs;
+          for (int32_t b = d.rp[br]; b < d.rp[br + 1]; ++b) {
+            const float *blk = d.val + b * E;
+            const int64_t c0 = (int64_t)d.col[b] * bs;
+            for (int jj = 0; jj < bs; ++jj) {
+              const float a = d.layout == PERFLIBS_ROW_MAJOR ? blk[i * bs + jj] : blk[jj * bs + i];
+              const float *brow = d.B + (c0 + jj) * d.ldb;
+#pragma unroll
+              for (int q = 0; q < kMaxColsPerLane; ++q) {
+                const int kk = kk0 + s + q * L;
+                if (kk < d.k)
+                  acc[q] = fmaf(a, __ldg(brow + kk), acc[q]);
+              }
+            }
+          }
+        }
+        float *crow = d.C + (int64_t)r * d.ldc;
+#pragma unroll
+        for (int q = 0; q < kMaxColsPerLane; ++q) {
+          const int kk = kk0 + s + q * L;
+          if (kk < d.k)
+            crow[kk] = beta_nz ? fmaf(alpha, acc[q], beta * crow[kk]) : alpha * acc[q];
+        }
+      }
+    }
+  }
+}
+
+int lanes_for(int k) {
+  int L = 1;
+  while (L < 32 && L * kMaxColsPerLane < k)
+    L *= 2;
+  while (L < 32 && L < k && L * 2 <= k)  // at least one column per lane
+    L *= 2;
+  return std::min(L, 32);
+}
+
+}  // namespace
+
+}  // namespace pls
+
+struct perflibs_b200_batch_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<pls::InstDesc> host;
+  std::vector<double> work_per_row;  // nonzeros per row x k (for ordering)
+  pls::DevBuf inst, items, counter;
+  int64_t n_items = 0;
+  int32_t tile = 0;
+  int grid = 0;
+  cudaGraphExec_t graph = nullptr;
+  float g_alpha = 0.f, g_beta = 0.f;
+  bool graph_valid = false;
+  bool own_stream = false;
+  ~perflibs_b200_batch_s() {
+    if (graph)
+      cudaGraphExecDestroy(graph);
+    if (own_stream && stream)
+      cudaStreamDestroy(stream);
+  }
+};
+
+namespace pls {
+
+using Batch = perflibs_b200_batch_s;
+
+namespace {
+
+void build_items(Batch *B, int32_t tile) {
+  std::vector<std::pair<double, Item>> v;
+  for (int32_t i = 0; i < (int32_t)B->host.size(); ++i) {
+    const InstDesc &d = B->host[i];
+    int32_t R = tile;
+    if (d.is_bsr)
+      R = std::max<int32_t>(d.bs, (tile / d.bs) * d.bs);
+    for (int32_t r0 = 0; r0 < d.m; r0 += R) {
+      Item it{i, r0, std::min(d.m, r0 + R), 0};
+      v.push_back({B->work_per_row[i] * (it.row1 - it.row0), it});
+    }
+  }
+  std::stable_sort(v.begin(), v.end(), [](auto &a, auto &b) { return a.first > b.first; });
+  std::vector<Item> items(v.size());
+  for (size_t j = 0; j < v.size(); ++j)
+    items[j] = v[j].second;
+  B->n_items = (int64_t)items.size();
+  B->items.reserve(sizeof(Item) * std::max<size_t>(items.size(), 1));
+  if (!items.empty())
+    PLS_CUDA(cudaMemcpyAsync(B->items.p, items.data(), sizeof(Item) * items.size(),
+                             cudaMemcpyHostToDevice, B->stream));
+  PLS_CUDA(cudaStreamSynchronize(B->stream));
+  B->tile = tile;
+  B->graph_valid = false;
+}
+
+void capture(Batch *B, float alpha, float beta) {
+  if (B->graph) {
+    cudaGraphExecDestroy(B->graph);
+    B->graph = nullptr;
+  }
+  cudaGraph_t g;
+  cudaStream_t s = B->stream;
+  PLS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  cudaMemsetAsync(B->counter.p, 0, 8, s);
+  if (B->n_items > 0)
+    k_batch_spmm<<<B->grid, 256, 0, s>>>(B->inst.as<InstDesc>(), B->items.as<Item>(), B->n_items,
+                                         B->counter.as<unsigned long long>(), alpha, beta,
+                                         beta != 0.f);
+  PLS_CUDA(cudaStreamEndCapture(s, &g));
+  PLS_CUDA(cudaGraphInstantiate(&B->graph, g, 0));
+  cudaGraphDestroy(g);
+  B->g_alpha = alpha;
+  B->g_beta = beta;
+  B->graph_valid = true;
+}
+
+void run(Batch *B, float alpha, float beta) {
+  if (!B->graph_valid || alpha != B->g_alpha || beta != B->g_beta)
+    capture(B, alpha, beta);
+  PLS_CUDA(cudaGraphLaunch(B->graph, B->stream));
+}
+
+}  // namespace
+
+}  // namespace pls
+
+using namespace pls;
+
+extern "C" {
+
+perflibs_status_t perflibs_b200_batch_create(perflibs_b200_batch_t *out, int32_t count,
+                                             const perflibs_spmat_t *mats, const int32_t *k,
+                                             const float *const *Bp, const int64_t *ldb,
+                                             float *const *Cp, const int64_t *ldc, void *stream) {
+  if (!out || count <= 0 || !mats || !k || !Bp || !ldb || !Cp || !ldc)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  try {
+    auto *B = new Batch;
+    cudaGetDevice(&B->device);
+    if (stream) {
+      B->stream = (cudaStream_t)stream;
+    } else {
+      PLS_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
+      B->own_stream = true;
+    }
+    for (int32_t i = 0; i < count; ++i) {
+      Mat *A = mats[i];
+      if (!A || A->dt != Dt::F32 || k[i] < 0 || ldb[i] < k[i] || ldc[i] < k[i] ||
+          !(A->fmt == Fmt::CSR || A->fmt == Fmt::SELL || A->fmt == Fmt::BSR)) {
+        delete B;
+        *out = nullptr;
+        return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+      }
+      InstDesc d{};
+      d.B = Bp[i];
+      d.C = Cp[i];
+      d.ldb = ldb[i];
+      d.ldc = ldc[i];
+      d.m = A->m;
+      d.k = k[i];
+      d.lanes = lanes_for(k[i]);
+      if (A->fmt == Fmt::BSR) {
+        d.is_bsr = 1;
+        d.bs = A->bsr.bs;
+        d.layout = A->bsr.layout;
+        d.rp = A->bsr.row_ptr.as<int32_t>();
+        d.col = A->bsr.col.as<int32_t>();
+        d.val = A->bsr.vals.as<float>();
+      } else {
+        d.is_bsr = 0;
+        d.bs = 1;
+        d.rp = A->csr.row_ptr.as<int32_t>();
+        d.col = A->csr.col.as<int32_t>();
+        d.val = A->csr.vals.as<float>();
+      }
+      B->host.push_back(d);
+      B->work_per_row.push_back(((double)A->nnz / std::max(A->m, 1) + 1.0) * std::max(k[i], 1));
+    }
+    B->inst.reserve(sizeof(InstDesc) * count);
+    PLS_CUDA(cudaMemcpyAsync(B->inst.p, B->host.data(), sizeof(InstDesc) * count,
+                             cudaMemcpyHostToDevice, B->stream));
+    B->counter.reserve(8);
+    int sms = 0, per_sm = 0;
+    PLS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, B->device));
+    PLS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_spmm, 256, 0));
+    B->grid = sms * std::max(per_sm, 1);
+    build_items(B, 64);
+    *out = B;
+    return PERFLIBS_STATUS_SUCCESS;
+  } catch (const Error &e) {
+    *out = nullptr;
+    return e.status;
+  }
+}
+
+perflibs_status_t perflibs_b200_batch_set_tile(perflibs_b200_batch_t B, int32_t rows) {
+  if (!B || rows < 0)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  try {
+    if (rows > 0)
+      build_items(B, rows);
+    return PERFLIBS_STATUS_SUCCESS;
+  } catch (const Error &e) {
+    return e.status;
+  }
+}
+
+perflibs_status_t perflibs_b200_batch_tune(perflibs_b200_batch_t B, int32_t *best_tile,
+                                           float *best_ms) {
+  if (!B)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  try {
+    cudaEvent_t e0, e1;
+    PLS_CUDA(cudaEventCreate(&e0));
+    PLS_CUDA(cudaEventCreate(&e1));
+    int32_t best = 64;
+    float bms = 1e30f;
+    for (int32_t tile : {8, 32, 128, 512, 2048}) {
+      build_items(B, tile);
+      run(B, 1.f, 0.f);
+      run(B, 1.f, 0.f);
+      std::vector<float> t;
+      for (int r = 0; r < 7; ++r) {
+        PLS_CUDA(cudaEventRecord(e0, B->stream));
+        run(B, 1.f, 0.f);
+        PLS_CUDA(cudaEventRecord(e1, B->stream));
+        PLS_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        PLS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        t.push_back(ms);
+      }
+      std::sort(t.begin(), t.end());
+      if (t[t.size() / 2] < bms) {
+        bms = t[t.size() / 2];
+        best = tile;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    build_items(B, best);
+    if (best_tile)
+      *best_tile = best;
+    if (best_ms)
+      *best_ms = bms;
+    return PERFLIBS_STATUS_SUCCESS;
+  } catch (const Error &e) {
+    return e.status;
+  }
+}
+
+perflibs_status_t perflibs_b200_batch_exec(perflibs_b200_batch_t B, float alpha, float beta) {
+  if (!B)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  try {
+    run(B, alpha, beta);
+    return PERFLIBS_STATUS_SUCCESS;
+  } catch (const Error &e) {
+    return e.status;
+  }
+}
+
+perflibs_status_t perflibs_b200_batch_info(perflibs_b200_batch_t B, int64_t *n_items,
+                                           int32_t *launches, int32_t *tile) {
+  if (!B)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  if (n_items)
+    *n_items = B->n_items;
+  if (launches)
+    *launches = B->n_items > 0 ? 1 : 0;
+  if (tile)
+    *tile = B->tile;
+  return PERFLIBS_STATUS_SUCCESS;
+}
+
+perflibs_status_t perflibs_b200_batch_destroy(perflibs_b200_batch_t B) {
+  delete B;
+  return PERFLIBS_STATUS_SUCCESS;
+}
+
+}  // extern "C"

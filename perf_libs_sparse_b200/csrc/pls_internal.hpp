@@ -153,11 +153,12 @@ struct SellDev {
   int32_t max_width = 0;
   DevBuf cs, cl, col_min, permd2in, in2permd, vals, offsets;
   Vt vt = Vt::F64;
-  // Work list of (chunk, column slice) items for chunks wider than
-  // slice_w; empty when every chunk fits one item.
+  // Column slices (chunk, j0, j1, slot) of the chunks wider than split_w;
+  // empty when no chunk is sliced.
   DevBuf items;
   int64_t n_items = 0;
   int slice_w = 0;
+  int32_t split_w = INT32_MAX;
   DevBuf split_chunks;  // (chunk, first slot, slice count) per split chunk
   int64_t n_split = 0;
   DevBuf part;          // partial sums of the split chunks' slices (scratch)

@@ -230,7 +230,7 @@ void build_sell(const CsrDev &c, int32_t m, int C, int sigma, SellDev &out,
   SellDev S;
   S.C = C;
   S.sigma = sigma;
-  S.vt = c.vt;
+  S.vt = c.evt();  // the kernels' value copy (reduced under FP32 / BF16 storage)
   S.nC = div_up(m, C);
   const int64_t nwin = div_up(m, win);
   const int64_t npos = nwin * win;  // >= nC*C
@@ -323,7 +323,7 @@ void build_sell(const CsrDev &c, int32_t m, int C, int sigma, SellDev &out,
       k_fill<V, O><<<blocks, 256, 0, s>>>(
           S.nC, C, S.cs.as<int64_t>(), S.cl.as<int32_t>(),
           S.col_min.as<int32_t>(), S.permd2in.as<int32_t>(), rp,
-          c.col.as<int32_t>(), c.vals.as<V>(), S.vals.as<V>(), S.offsets.as<O>());
+          c.col.as<int32_t>(), (const V *)c.ev(), S.vals.as<V>(), S.offsets.as<O>());
     };
     auto by_width = [&](auto vtag) {
       switch (bytes) {
@@ -384,9 +384,10 @@ int64_t sell_padded_size(const CsrDev &c, int32_t m, int C, int sigma, cudaStrea
   return t;
 }
 
-// Split chunks wider than 2*slice_w into column slices of slice_w so that a
-// few very wide chunks (power-law row lengths) spread over many lane groups.
-// Items are ordered widest work first so the long slices start early.
+// Slice the chunks wider than 2*slice_w into column slices of slice_w so
+// that a few very wide chunks (power-law row lengths) spread over many lane
+// groups; the other chunks stay one lane group each. Slices are ordered by
+// decreasing chunk width so the longest work starts first.
 void sell_build_work_list(SellDev &S, int slice_w, cudaStream_t st) {
   S.items.release();
   S.split_chunks.release();
@@ -394,44 +395,40 @@ void sell_build_work_list(SellDev &S, int slice_w, cudaStream_t st) {
   S.n_items = 0;
   S.n_split = 0;
   S.slice_w = 0;
+  S.split_w = INT32_MAX;
   if (S.nC == 0 || slice_w <= 0 || S.max_width <= 2 * slice_w)
     return;
   std::vector<int32_t> cl(S.nC);
-  PLS_CUDA(cudaMemcpy(cl.data(), S.cl.p, sizeof(int32_t) * S.nC,
-                      cudaMemcpyDeviceToHost));
-  std::vector<int4> split_items, whole_items, splits;
+  PLS_CUDA(cudaMemcpy(cl.data(), S.cl.p, sizeof(int32_t) * S.nC, cudaMemcpyDeviceToHost));
+  std::vector<int64_t> wide;
+  for (int64_t c = 0; c < S.nC; ++c)
+    if (cl[c] > 2 * slice_w)
+      wide.push_back(c);
+  std::stable_sort(wide.begin(), wide.end(),
+                   [&](int64_t a, int64_t b) { return cl[a] > cl[b]; });
+  std::vector<int4> items, splits;
   int32_t slot = 0;
-  for (int64_t c = 0; c < S.nC; ++c) {
+  for (int64_t c : wide) {
     const int32_t w = cl[c];
-    if (w > 2 * slice_w) {
-      const int32_t ns = (int32_t)div_up(w, slice_w);
-      splits.push_back(make_int4((int)c, slot, ns, 0));
-      for (int32_t q = 0; q < ns; ++q)
-        split_items.push_back(make_int4((int)c, q * slice_w,
-                                        std::min(w, (q + 1) * slice_w), slot + q));
-      slot += ns;
-    } else {
-      whole_items.push_back(make_int4((int)c, 0, w, -1));
-    }
+    const int32_t ns = (int32_t)div_up(w, slice_w);
+    splits.push_back(make_int4((int)c, slot, ns, 0));
+    for (int32_t q = 0; q < ns; ++q)
+      items.push_back(make_int4((int)c, q * slice_w, std::min(w, (q + 1) * slice_w), slot + q));
+    slot += ns;
   }
-  std::vector<int4> items;
-  items.reserve(split_items.size() + whole_items.size());
-  items.insert(items.end(), split_items.begin(), split_items.end());
-  items.insert(items.end(), whole_items.begin(), whole_items.end());
   S.n_items = (int64_t)items.size();
   S.n_split = (int64_t)splits.size();
   S.slice_w = slice_w;
+  S.split_w = 2 * slice_w;
   S.items.reserve(sizeof(int4) * items.size());
   PLS_CUDA(cudaMemcpyAsync(S.items.p, items.data(), sizeof(int4) * items.size(),
                            cudaMemcpyHostToDevice, st));
-  S.split_chunks.reserve(sizeof(int4) * std::max<size_t>(splits.size(), 1));
-  if (!splits.empty())
-    PLS_CUDA(cudaMemcpyAsync(S.split_chunks.p, splits.data(),
-                             sizeof(int4) * splits.size(),
-                             cudaMemcpyHostToDevice, st));
+  S.split_chunks.reserve(sizeof(int4) * splits.size());
+  PLS_CUDA(cudaMemcpyAsync(S.split_chunks.p, splits.data(), sizeof(int4) * splits.size(),
+                           cudaMemcpyHostToDevice, st));
   // Partial sums: one accumulator per (slot, row); FP64 covers both
   // accumulator types.
-  S.part.reserve(sizeof(double) * (size_t)std::max<int32_t>(slot, 1) * S.C);
+  S.part.reserve(sizeof(double) * (size_t)slot * S.C);
   PLS_CUDA(cudaStreamSynchronize(st));
 }
 

@@ -46,18 +46,34 @@ __global__ void __launch_bounds__(256)
   const int32_t s = __ldg(rp + row), e = __ldg(rp + row + 1);
   if (skip_len > 0 && e - s > skip_len)
     return;  // uniform across the row's lanes
+  // Groups of G elements per lane: all value / column loads of a group are
+  // issued (predicated past the row end) before the dependent x gathers.
+  constexpr int G = 4;
+  const L2Policy pol = make_l2_policy();
   Acc sum = 0;
-  int32_t j = s + sub;
-#pragma unroll 2
-  for (; j + TPR < e; j += 2 * TPR) {
-    const V v0 = ld_stream(val + j), v1 = ld_stream(val + j + TPR);
-    const int32_t c0 = ld_stream(col + j), c1 = ld_stream(col + j + TPR);
-    sum = fma(to_acc<Acc>(v0), to_acc<Acc>(ld_ro(x + c0)), sum);
-    sum = fma(to_acc<Acc>(v1), to_acc<Acc>(ld_ro(x + c1)), sum);
+  for (int32_t j = s + sub; j < e; j += G * TPR) {
+    V v[G];
+    int32_t c[G];
+#pragma unroll
+    for (int u = 0; u < G; ++u) {
+      const int32_t q = j + u * TPR;
+      if (q < e) {
+        v[u] = ld_stream(val + q, pol.stream);
+        c[u] = ld_stream(col + q, pol.stream);
+      } else {
+        v[u] = from_double<V>(0.0);
+        c[u] = 0;
+      }
+    }
+    Acc xv[G];
+#pragma unroll
+    for (int u = 0; u < G; ++u)
+      xv[u] = j + u * TPR < e ? to_acc<Acc>(ld_keep(x + c[u], pol.keep)) : Acc(0);
+#pragma unroll
+    for (int u = 0; u < G; ++u)
+      if (j + u * TPR < e)
+        sum = fma(to_acc<Acc>(v[u]), xv[u], sum);
   }
-  if (j < e)
-    sum = fma(to_acc<Acc>(ld_stream(val + j)),
-              to_acc<Acc>(ld_ro(x + ld_stream(col + j))), sum);
   if constexpr (TPR > 1)
     sum = group_sum<TPR>(sum, group_mask<TPR>());
   if (sub == 0)
@@ -159,113 +175,97 @@ void spmv_csr_split(const CsrDev &c, int32_t m, const X *x, X *y, X alpha,
 
 // ---------------------------------------------------------- SELL-C-sigma
 
-// One lane per (chunk, row): the row's products are summed strictly in
-// column order j = 0 .. cl-1 over the padded chunk, the order the reference's
-// spmv_scs<T,C> uses (src/sell_c_sigma.cpp:727-775). Lane r of chunk c
-// reads element cs[c] + j*C + r, so the C lanes of a chunk read C
-// consecutive values per step (a full 256-byte line for C=32, FP64).
+// Sum of one SELL row segment: len padded columns starting at vp / op
+// (stride C between consecutive columns of the row). Columns are taken in
+// groups of kSellGroup: all value and offset loads of a group are issued
+// (predicated past len) before any of the group's dependent x gathers, so a
+// short row costs two memory round trips instead of two per column. The
+// products are still added one by one in column order j = 0 .. len-1, the
+// order of the reference's spmv_scs<T,C> (src/sell_c_sigma.cpp:727-775).
+constexpr int kSellGroup = 8;
+
 template <int C, class V, class O, class X>
-__global__ void __launch_bounds__(256)
-    k_sell(int64_t nC, const int64_t *__restrict__ cs,
+__device__ __forceinline__ typename AccOf<V, X>::type sell_row_sum(const V *vp, const O *op,
+                                                                   const X *xb, int32_t len,
+                                                                   const L2Policy &pol) {
+  using Acc = typename AccOf<V, X>::type;
+  Acc acc = 0;
+  for (int32_t j = 0; j < len; j += kSellGroup) {
+    V v[kSellGroup];
+    O o[kSellGroup];
+#pragma unroll
+    for (int u = 0; u < kSellGroup; ++u) {
+      if (j + u < len) {
+        v[u] = ld_stream(vp + u * C, pol.stream);
+        o[u] = ld_stream(op + u * C, pol.stream);
+      } else {
+        v[u] = from_double<V>(0.0);
+        o[u] = 0;
+      }
+    }
+    Acc xv[kSellGroup];
+#pragma unroll
+    for (int u = 0; u < kSellGroup; ++u)
+      xv[u] = j + u < len ? to_acc<Acc>(ld_keep(xb + o[u], pol.keep)) : Acc(0);
+#pragma unroll
+    for (int u = 0; u < kSellGroup; ++u)
+      if (j + u < len)
+        acc = fma(to_acc<Acc>(v[u]), xv[u], acc);
+    vp += kSellGroup * C;
+    op += kSellGroup * C;
+  }
+  return acc;
+}
+
+// One launch, two kinds of blocks. Blocks [0, slice_blocks) take column
+// slices of the few chunks wider than split_w (power-law tails): item =
+// (chunk, j0, j1, slot), partial sum to part[slot*C + r]. The remaining
+// blocks take one chunk per C lanes (lane r = row r of the chunk, so the C
+// lanes read C consecutive values per column: a full 256-byte line for
+// C = 32, FP64) and skip the chunks the slices cover. Slices come first so
+// the longest work starts earliest.
+template <int C, class V, class O, class X>
+__global__ void __launch_bounds__(256, 5)
+    k_sell(int64_t nC, int32_t split_w, int64_t n_items, int64_t slice_blocks,
+           const int4 *__restrict__ items, const int64_t *__restrict__ cs,
            const int32_t *__restrict__ cl, const int32_t *__restrict__ cmin,
            const int32_t *__restrict__ perm, const V *__restrict__ vals,
-           const O *__restrict__ offs, const X *__restrict__ x,
-           X *__restrict__ y, X alpha, X beta, int beta_nz) {
+           const O *__restrict__ offs, const X *__restrict__ x, X *__restrict__ y,
+           typename AccOf<V, X>::type *__restrict__ part, X alpha, X beta, int beta_nz) {
   using Acc = typename AccOf<V, X>::type;
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const L2Policy pol = make_l2_policy();
+  if (blockIdx.x < slice_blocks) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t it = t / C;
+    if (it >= n_items)
+      return;
+    const int r = (int)(t % C);
+    const int4 w = items[it];  // chunk, j0, j1, slot
+    const int64_t base = __ldg(cs + w.x) + (int64_t)w.y * C + r;
+    const X *xb = x + __ldg(cmin + w.x);
+    part[(int64_t)w.w * C + r] =
+        sell_row_sum<C, V, O, X>(vals + base, offs + base, xb, w.z - w.y, pol);
+    return;
+  }
+  const int64_t t = (int64_t)(blockIdx.x - slice_blocks) * blockDim.x + threadIdx.x;
   const int64_t c = t / C;
   if (c >= nC)
     return;
   const int r = (int)(t % C);
   const int32_t w = __ldg(cl + c);
+  if (w > split_w)
+    return;  // sliced chunk: written by k_sell_combine
   const int64_t base = __ldg(cs + c) + r;
-  const X *xb = x + (w > 0 ? __ldg(cmin + c) : 0);
-  const V *vp = vals + base;
-  const O *op = offs + base;
-  Acc acc = 0;
-  int32_t j = 0;
-  for (; j + 4 <= w; j += 4) {
-    const V v0 = ld_stream(vp), v1 = ld_stream(vp + C), v2 = ld_stream(vp + 2 * C),
-            v3 = ld_stream(vp + 3 * C);
-    const O o0 = ld_stream(op), o1 = ld_stream(op + C), o2 = ld_stream(op + 2 * C),
-            o3 = ld_stream(op + 3 * C);
-    const Acc x0 = to_acc<Acc>(ld_ro(xb + o0)), x1 = to_acc<Acc>(ld_ro(xb + o1)),
-              x2 = to_acc<Acc>(ld_ro(xb + o2)), x3 = to_acc<Acc>(ld_ro(xb + o3));
-    acc = fma(to_acc<Acc>(v0), x0, acc);
-    acc = fma(to_acc<Acc>(v1), x1, acc);
-    acc = fma(to_acc<Acc>(v2), x2, acc);
-    acc = fma(to_acc<Acc>(v3), x3, acc);
-    vp += 4 * C;
-    op += 4 * C;
-  }
-  for (; j < w; ++j) {
-    acc = fma(to_acc<Acc>(ld_stream(vp)), to_acc<Acc>(ld_ro(xb + ld_stream(op))), acc);
-    vp += C;
-    op += C;
-  }
+  const int32_t cm = __ldg(cmin + c);
   const int32_t dst = __ldg(perm + c * C + r);
+  const X *xb = x + (w > 0 ? cm : 0);
+  const Acc acc = sell_row_sum<C, V, O, X>(vals + base, offs + base, xb, w, pol);
   if (dst >= 0)
     store_y(y, dst, acc, alpha, beta, beta_nz);
 }
 
-// Work-list variant: item = (chunk, j0, j1, slot). Items with slot < 0 cover
-// a whole chunk and write y; the others write a partial sum for their
-// column slice into part[slot*C + r], combined in slice order by
-// k_sell_combine. Used when a few chunks are much wider than the rest
-// (power-law row lengths), so one wide chunk does not serialise on a single
-// group of lanes.
-template <int C, class V, class O, class X>
-__global__ void __launch_bounds__(256)
-    k_sell_items(int64_t n_items, const int4 *__restrict__ items,
-                 const int64_t *__restrict__ cs, const int32_t *__restrict__ cmin,
-                 const int32_t *__restrict__ perm, const V *__restrict__ vals,
-                 const O *__restrict__ offs, const X *__restrict__ x,
-                 X *__restrict__ y, typename AccOf<V, X>::type *__restrict__ part,
-                 X alpha, X beta, int beta_nz) {
-  using Acc = typename AccOf<V, X>::type;
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t it = t / C;
-  if (it >= n_items)
-    return;
-  const int r = (int)(t % C);
-  const int4 w = items[it];  // chunk, j0, j1, slot
-  const int64_t c = w.x;
-  const int64_t base = __ldg(cs + c) + (int64_t)w.y * C + r;
-  const X *xb = x + (w.z > w.y ? __ldg(cmin + c) : 0);
-  const V *vp = vals + base;
-  const O *op = offs + base;
-  const int32_t len = w.z - w.y;
-  Acc acc = 0;
-  int32_t j = 0;
-  for (; j + 4 <= len; j += 4) {
-    const V v0 = ld_stream(vp), v1 = ld_stream(vp + C), v2 = ld_stream(vp + 2 * C),
-            v3 = ld_stream(vp + 3 * C);
-    const O o0 = ld_stream(op), o1 = ld_stream(op + C), o2 = ld_stream(op + 2 * C),
-            o3 = ld_stream(op + 3 * C);
-    const Acc x0 = to_acc<Acc>(ld_ro(xb + o0)), x1 = to_acc<Acc>(ld_ro(xb + o1)),
-              x2 = to_acc<Acc>(ld_ro(xb + o2)), x3 = to_acc<Acc>(ld_ro(xb + o3));
-    acc = fma(to_acc<Acc>(v0), x0, acc);
-    acc = fma(to_acc<Acc>(v1), x1, acc);
-    acc = fma(to_acc<Acc>(v2), x2, acc);
-    acc = fma(to_acc<Acc>(v3), x3, acc);
-    vp += 4 * C;
-    op += 4 * C;
-  }
-  for (; j < len; ++j) {
-    acc = fma(to_acc<Acc>(ld_stream(vp)), to_acc<Acc>(ld_ro(xb + ld_stream(op))), acc);
-    vp += C;
-    op += C;
-  }
-  if (w.w < 0) {
-    const int32_t dst = __ldg(perm + c * C + r);
-    if (dst >= 0)
-      store_y(y, dst, acc, alpha, beta, beta_nz);
-  } else {
-    part[(int64_t)w.w * C + r] = acc;
-  }
-}
-
-// split: (chunk, first slot, slice count) per split chunk.
+// split: (chunk, first slot, slice count) per sliced chunk; the slices'
+// partial sums are added in slice order.
 template <int C, class Acc, class X>
 __global__ void k_sell_combine(int64_t n_split, const int4 *__restrict__ split,
                                const int32_t *__restrict__ perm,
@@ -290,27 +290,20 @@ static void launch_sell(const SellDev &s, const X *x, X *y, X alpha, X beta,
                         cudaStream_t st) {
   using Acc = typename AccOf<V, X>::type;
   const int bnz = beta != X(0);
-  if (s.n_items == 0) {
-    const int64_t blocks = div_up(s.nC * C, 256);
-    if (blocks == 0)
-      return;
-    k_sell<C, V, O, X><<<(unsigned)blocks, 256, 0, st>>>(
-        s.nC, s.cs.as<int64_t>(), s.cl.as<int32_t>(), s.col_min.as<int32_t>(),
-        s.permd2in.as<int32_t>(), s.vals.as<V>(), s.offsets.as<O>(), x, y,
-        alpha, beta, bnz);
-  } else {
-    const int64_t blocks = div_up(s.n_items * C, 256);
-    Acc *part = (Acc *)s.part.p;  // partial sums (scratch)
-    k_sell_items<C, V, O, X><<<(unsigned)blocks, 256, 0, st>>>(
-        s.n_items, s.items.as<int4>(), s.cs.as<int64_t>(),
-        s.col_min.as<int32_t>(), s.permd2in.as<int32_t>(), s.vals.as<V>(),
-        s.offsets.as<O>(), x, y, part, alpha, beta, bnz);
-    if (s.n_split > 0) {
-      const int64_t b2 = div_up(s.n_split * C, 256);
-      k_sell_combine<C, Acc, X><<<(unsigned)b2, 256, 0, st>>>(
-          s.n_split, s.split_chunks.as<int4>(), s.permd2in.as<int32_t>(), part,
-          y, alpha, beta, bnz);
-    }
+  const bool sliced = s.n_items > 0 && s.n_split > 0;
+  const int64_t slice_blocks = sliced ? div_up(s.n_items * C, 256) : 0;
+  const int64_t chunk_blocks = div_up(s.nC * C, 256);
+  if (slice_blocks + chunk_blocks == 0)
+    return;
+  Acc *part = sliced ? (Acc *)s.part.p : nullptr;  // partial sums (scratch)
+  k_sell<C, V, O, X><<<(unsigned)(slice_blocks + chunk_blocks), 256, 0, st>>>(
+      s.nC, sliced ? s.split_w : INT32_MAX, sliced ? s.n_items : 0, slice_blocks,
+      s.items.as<int4>(), s.cs.as<int64_t>(), s.cl.as<int32_t>(), s.col_min.as<int32_t>(),
+      s.permd2in.as<int32_t>(), s.vals.as<V>(), s.offsets.as<O>(), x, y, part, alpha, beta, bnz);
+  if (sliced) {
+    const int64_t b2 = div_up(s.n_split * C, 256);
+    k_sell_combine<C, Acc, X><<<(unsigned)b2, 256, 0, st>>>(
+        s.n_split, s.split_chunks.as<int4>(), s.permd2in.as<int32_t>(), part, y, alpha, beta, bnz);
   }
 }
 
@@ -404,6 +397,7 @@ void spmv_sell_scratch(const SellDev &s, const X *x, X *y, X alpha, X beta, void
   view.vt = s.vt;
   view.n_items = s.n_items;
   view.n_split = s.n_split;
+  view.split_w = s.split_w;
   view.cs.p = s.cs.p;
   view.cl.p = s.cl.p;
   view.col_min.p = s.col_min.p;

@@ -136,6 +136,66 @@ def random_csr(m: int, n: int, max_len: int, rng: np.random.Generator, base: int
     return (row_ptr + base).astype(np.int32), (col + base).astype(np.int32), vals
 
 
+def batched_instances(count: int = 512, seed: int = 3, n_lo: int = 1024, n_hi: int = 65536,
+                      k_max: int = 64):
+    """The uneven batch: `count` independent FP32 instances, n log-uniform in
+    [n_lo, n_hi], k log-uniform in [1, k_max], of three kinds in turn:
+    banded (full band, half-bandwidth 2-64), random uniform (4-32 unique
+    columns per row), and BSR block-diagonal (block size 4 or 8, each
+    diagonal block filled with probability 0.3-0.9 per entry, zeros kept as
+    explicit block entries). Values U[-1, 1]. Returns a list of dicts with
+    'kind' ('csr' or 'bsr'), 'm', 'n', 'k', the arrays, and 'B' (n x k)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi)))))
+        k = int(round(np.exp(rng.uniform(0.0, np.log(k_max)))))
+        kind = ("banded", "uniform", "bsr")[i % 3]
+        if kind == "banded":
+            hb = int(rng.integers(2, 65))
+            rows = np.arange(n)
+            lo = np.maximum(rows - hb, 0)
+            hi = np.minimum(rows + hb, n - 1)
+            lens = hi - lo + 1
+            row_ptr = np.zeros(n + 1, np.int32)
+            row_ptr[1:] = np.cumsum(lens)
+            col = (np.repeat(lo, lens) + np.arange(row_ptr[-1]) - np.repeat(row_ptr[:-1], lens)).astype(np.int32)
+            vals = rng.uniform(-1, 1, row_ptr[-1]).astype(np.float32)
+            d = dict(kind="csr", m=n, n=n, row_ptr=row_ptr, col=col, vals=vals, band=hb)
+        elif kind == "uniform":
+            lens = rng.integers(4, 33, n)
+            row_ptr = np.zeros(n + 1, np.int32)
+            row_ptr[1:] = np.cumsum(lens)
+            rows = np.repeat(np.arange(n, dtype=np.int64), lens)
+            key = np.unique(rows * n + rng.integers(0, n, row_ptr[-1]))
+            rows = key // n
+            counts = np.bincount(rows, minlength=n)
+            row_ptr[1:] = np.cumsum(counts)
+            col = (key % n).astype(np.int32)
+            vals = rng.uniform(-1, 1, len(col)).astype(np.float32)
+            d = dict(kind="csr", m=n, n=n, row_ptr=row_ptr, col=col, vals=vals)
+        else:
+            bs = int(rng.choice([4, 8]))
+            nb = max(1, n // bs)
+            n = nb * bs
+            fill = rng.uniform(0.3, 0.9)
+            blocks = rng.uniform(-1, 1, (nb, bs * bs)).astype(np.float32)
+            blocks[rng.random((nb, bs * bs)) >= fill] = 0.0
+            d = dict(kind="bsr", m=n, n=n, bs=bs, layout=91, row_ptr=np.arange(nb + 1, dtype=np.int32),
+                     col=np.arange(nb, dtype=np.int32), vals=blocks.reshape(-1), fill=fill)
+        d["k"] = k
+        d["B"] = rng.uniform(-1, 1, (d["n"], k)).astype(np.float32)
+        out.append(d)
+    return out
+
+
+def instance_nnz(d) -> int:
+    """Stored entries of an instance (BSR counts whole blocks)."""
+    if d["kind"] == "bsr":
+        return len(d["col"]) * d["bs"] * d["bs"]
+    return int(d["row_ptr"][-1])
+
+
 def uniform_vector(n: int, seed: int, dtype=np.float64) -> np.ndarray:
     return np.random.default_rng(seed).uniform(-1.0, 1.0, n).astype(dtype)
 
