@@ -280,7 +280,6 @@ def run_b200(args):
     # Parity of the timed result (full size) against the oracle.
     import oracle
 
-    y_gpu = yd.cpu().numpy()
     step(A)
     torch.cuda.synchronize()
     y_gpu = yd.cpu().numpy()
@@ -288,7 +287,53 @@ def run_b200(args):
     scale = oracle.csr_absdot(rp, c, v, x)
     den = np.maximum(np.abs(y_ref), scale)
     den[den == 0] = 1
-    max_rel = float((np.abs(y_gpu - y_ref) / den).max())
+
+    def rel_err(y):
+        return float((np.abs(y - y_ref) / den).max())
+
+    max_rel = rel_err(y_gpu)
+    # FP64 inf-norm check of the result: ||y - y_ref||_inf / (||A||_inf ||x||_inf),
+    # with ||A||_inf from the library's own FP64 norm.
+    a_inf = float(A.norm(pls.NORM_INF))
+    x_inf = float(np.abs(x).max())
+
+    def inf_check(y):
+        return float(np.abs(y - y_ref).max() / max(a_inf * x_inf, 1e-300))
+
+    # The learned selector (the trained parameters shipped with the package)
+    # picks the layout; FP64, FP32 and BF16 value storage, each timed like
+    # the tuned arm and checked against the FP64 oracle.
+    from perf_libs_sparse_b200 import selector as selmod
+
+    selector_arms = {}
+    S = selmod.default_selector()
+    if S is not None:
+        for name, storage, tol in (("fp64", pls.STORAGE_NATIVE, 1e-12),
+                                   ("fp32", pls.STORAGE_FP32, 1e-5),
+                                   ("bf16", pls.STORAGE_BF16, 1e-2)):
+            As = pls.SpMat.csr(m, n, rp, c, v)
+            As.set_stream(sp)
+            As.set_storage(storage)
+            As.hint(pls.HINT_SPMV_INVOCATIONS, pls.INVOCATIONS_MANY)
+            As.set_tuner(pls.TUNE_SELECTOR)
+            S.attach(As)
+            t0 = time.perf_counter()
+            assert As.optimize() == 0
+            t_sel = time.perf_counter() - t0
+            ms_s = timed(As, K, Wm)
+            step(As)
+            torch.cuda.synchronize()
+            ys = yd.cpu().numpy()
+            cfg_s = As.config()
+            selector_arms[name] = {
+                "format": {0: "CSR", 1: "SELL-C-sigma", 2: "CSR-split"}[cfg_s["kind"]],
+                "C": cfg_s["C"], "sigma": cfg_s["sigma"], "tpr": cfg_s["tpr"],
+                "ms_per_step": ms_s, "speedup_vs_plain_csr_fp64": ms_plain / ms_s,
+                "max_rel_err": rel_err(ys), "tolerance": tol, "inf_norm_check": inf_check(ys),
+                "optimize_s": t_sel,
+            }
+            As.destroy()
+        selector_arms["fp64"]["regret_vs_exhaustive"] = selector_arms["fp64"]["ms_per_step"] / ms_tuned - 1.0
 
     # End to end through the drop-in call with pinned host buffers.
     xh = torch.tensor(x).pin_memory()
@@ -343,6 +388,9 @@ def run_b200(args):
         "plain_csr": {"value": bytes_step / (ms_plain * 1e-3) / 1e9 * world, "ms_per_step": ms_plain},
         "speedup_vs_plain_csr": ms_plain / ms_tuned,
         "max_rel_err": max_rel,
+        "inf_norm_check": inf_check(y_gpu),
+        "gflops": 2.0 * nnz / (ms_tuned * 1e-3) / 1e9 * world,
+        "selector": selector_arms or None,
         "e2e": {"value": bytes_step / e2e_s / 1e9 * world, "unit": "GB/s",
                 "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": m * 8, "ms_per_step": e2e_s * 1e3},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
@@ -458,14 +506,20 @@ def run_extra(args):
         ref = oracle.csr_spmm(sub_rp, c[idx], v[idx], B, k)
         scale = oracle.csr_spmm(sub_rp, c[idx], np.abs(v[idx]), np.abs(B), k)
         err = float((np.abs(got[rows] - ref) / np.maximum(np.maximum(np.abs(ref), scale), 1e-300)).max())
+        # FP64 inf-norm check on the same rows: max row sum |C - C_ref| over
+        # ||A||_inf ||B||_inf (||A||_inf from the library's FP64 norm).
+        inf_chk = float(np.abs(got[rows] - ref).sum(axis=1).max()
+                        / max(float(A.norm(pls.NORM_INF)) * float(np.abs(B).sum(axis=1).max()), 1e-300))
         sv = 8 if native else (4 if args.storage == "fp32" else 2)
         sb = 8 if native else 4
         b = W.algorithmic_bytes_spmm(m, n, int(rp[-1]), k, sv, sb, False)
         line.update(metric=f"SpMM GB/s (algorithmic bytes), 27-point 128^3, k={k}, storage {args.storage}",
                     dtype={"native": "f64", "fp32": "f32", "bf16": "bf16 values, f32 accumulate"}[args.storage],
-                    value=b / ms / 1e6, ms_per_step=ms, max_rel_err=err, gflops=2.0 * int(rp[-1]) * k / ms / 1e6,
+                    value=b / ms / 1e6, ms_per_step=ms, max_rel_err=err, inf_norm_check=inf_chk,
+                    gflops=2.0 * int(rp[-1]) * k / ms / 1e6,
                     config={"workload": "C3 27-point stencil 128^3 n=2097152 nnz=55742968", "k": k,
-                            "storage": args.storage, "l2": "inputs exceed L2; no flush"})
+                            "storage": args.storage, "l2": "inputs exceed L2; no flush",
+                            "spmm": A.spmm_info()})
     elif args.workload == "c4":
         inst = W.batched_instances(512, seed=3)
         mats, Bs, Cs = [], [], []

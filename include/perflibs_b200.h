@@ -87,8 +87,9 @@ perflibs_status_t perflibs_b200_spmat_set_storage(perflibs_spmat_t A,
  * src/matvec.cpp:624-627):
  *   EXHAUSTIVE: time every candidate (CSR threads-per-row x SELL C x sigma)
  *               with CUDA events and keep the fastest;
- *   SELECTOR:   ask the learned selector (perflibs_b200_selector_load) and
- *               fall back to EXHAUSTIVE when none is loaded;
+ *   SELECTOR:   ask the learned selector attached with
+ *               perflibs_b200_spmat_set_selector, and fall back to
+ *               EXHAUSTIVE when none is attached;
  *   NONE:       keep the default CSR kernel. */
 enum perflibs_b200_tuner {
   PERFLIBS_B200_TUNE_EXHAUSTIVE = 0,
@@ -124,6 +125,26 @@ perflibs_status_t perflibs_b200_spmat_exec_info(perflibs_spmat_t A,
                                                 int32_t *kernels_per_spmv,
                                                 int64_t *n_items,
                                                 int64_t *n_split);
+
+/* SpMM kernels for a CSR A. The staged kernel copies, for every block of R
+ * rows of A, the rows of B the block needs into shared memory (TMA bulk
+ * copies) and multiplies from there; the row-group kernel reads B through
+ * the caches. When the staged kernel applies (B rows reused inside row
+ * blocks, B 16-byte aligned, ldb and k multiples of 16 bytes), the first
+ * SpMM of each (k, ldb, value type) times both on scratch output and keeps
+ * the faster. set_spmm_path overrides that: -1 measured choice (default),
+ * 0 row-group kernel, 1 staged kernel whenever it applies. */
+perflibs_status_t perflibs_b200_spmat_set_spmm_path(perflibs_spmat_t A, int32_t path);
+
+/* SpMM plan of the handle: the staged tiles' block height R (0 when none
+ * were built: the staged kernel does not apply), the B rows staged per
+ * column tile over all blocks and the copy runs; the path the last SpMM
+ * took (1 staged, 0 row-group, -1 none yet); and the two timings of the
+ * measured choice in milliseconds (0 when not measured). Any output may be
+ * NULL. */
+perflibs_status_t perflibs_b200_spmat_spmm_info(perflibs_spmat_t A, int32_t *tile_rows,
+                                                int64_t *staged_rows, int64_t *runs,
+                                                int32_t *path, float *ms_staged, float *ms_rows);
 
 /* Timings the last exhaustive tune measured: up to `cap` rows of
  * (kind, C, sigma, tpr) in cfg4, milliseconds in ms and the SELL padding
@@ -167,7 +188,11 @@ perflibs_status_t perflibs_b200_spmat_export_bsr_d(
 
 /* ---- creation from device arrays ---------------------------------------
  * A CSR handle whose arrays already live in HBM (0- or 1-based, as
- * row_ptr[0] says; the arrays are copied, the caller keeps ownership). */
+ * row_ptr[0] says; the arrays are copied, the caller keeps ownership).
+ * `stream` is the stream the arrays were written on; the copies are ordered
+ * after it. With NULL the call first waits for all prior work on the device
+ * (the arrays may come from any stream, and the library's own stream does
+ * not wait for the legacy default stream). */
 perflibs_status_t perflibs_b200_spmat_create_csr_d_dev(
     perflibs_spmat_t *A, int32_t m, int32_t n, const int32_t *row_ptr,
     const int32_t *col_indx, const double *vals, void *stream);
@@ -271,6 +296,24 @@ perflibs_status_t perflibs_b200_device_info(int32_t *sm_count,
 
 /* Version string of the library build. */
 const char *perflibs_b200_version(void);
+
+/* ---- Matrix Market input (host only) ----------------------------------
+ * Reads a coordinate .mtx file (fields real / integer / pattern; symmetry
+ * general / symmetric / skew-symmetric / hermitian, the mirrored entries
+ * added as the reference's benchmark driver does,
+ * bench/pl_bench_sparse_x_dense.c:124-240) into a 0-based CSR ordered by
+ * (row, column), every entry kept. The arrays are malloc'ed; the caller
+ * frees them. INPUT_PARAMETER_ERROR for an unreadable or unsupported file. */
+perflibs_status_t perflibs_b200_read_mtx(const char *path, int32_t *m, int32_t *n,
+                                         int64_t *nnz, int32_t **row_ptr,
+                                         int32_t **col_indx, double **vals);
+
+/* The handle's error record (what perflibs_spmat_print_err prints): the
+ * status of the last failed call (0 when none), the 1-based argument
+ * position for input errors, and the message (NUL-terminated, truncated to
+ * msg_len - 1 characters). Any pointer may be NULL. */
+perflibs_status_t perflibs_b200_spmat_get_error(perflibs_const_spmat_t A, int32_t *type,
+                                                int32_t *code, char *msg, int32_t msg_len);
 
 #ifdef __cplusplus
 }

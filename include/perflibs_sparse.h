@@ -126,6 +126,31 @@ perflibs_status_t perflibs_spmat_create_dense_d(
     perflibs_int_t n, perflibs_int_t lda, const double *vals,
     perflibs_int_t flags);
 
+/* include/perflibs_sparse.h:176-184. The handle is converted to CSR on the
+ * device at creation (columns ascending per row). */
+perflibs_status_t perflibs_spmat_create_csc_s(perflibs_spmat_t *A, perflibs_int_t m,
+                                              perflibs_int_t n, const perflibs_int_t *row_indx,
+                                              const perflibs_int_t *col_ptr, const float *vals,
+                                              perflibs_int_t flags);
+perflibs_status_t perflibs_spmat_create_csc_d(perflibs_spmat_t *A, perflibs_int_t m,
+                                              perflibs_int_t n, const perflibs_int_t *row_indx,
+                                              const perflibs_int_t *col_ptr, const double *vals,
+                                              perflibs_int_t flags);
+
+/* include/perflibs_sparse.h:193-200 (0-based indices). Converted to CSR on
+ * the device at creation: entries sorted by (row, column), duplicates kept
+ * and added by the kernels. */
+perflibs_status_t perflibs_spmat_create_coo_s(perflibs_spmat_t *A, perflibs_int_t m,
+                                              perflibs_int_t n, perflibs_int_t nnz,
+                                              const perflibs_int_t *row_indx,
+                                              const perflibs_int_t *col_indx, const float *vals,
+                                              perflibs_int_t flags);
+perflibs_status_t perflibs_spmat_create_coo_d(perflibs_spmat_t *A, perflibs_int_t m,
+                                              perflibs_int_t n, perflibs_int_t nnz,
+                                              const perflibs_int_t *row_indx,
+                                              const perflibs_int_t *col_indx, const double *vals,
+                                              perflibs_int_t flags);
+
 /* include/perflibs_sparse.h:225-234 */
 perflibs_status_t perflibs_spmat_create_bsr_s(
     perflibs_spmat_t *A, enum perflibs_dense_layout block_layout,

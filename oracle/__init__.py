@@ -59,6 +59,8 @@ def port():
         L.orc_csr_spmm_s.argtypes = [i32, vp, vp, vp, vp, i64, vp, i64, i32, f, f]
         L.orc_csr_inf_norm_d.argtypes = [i32, vp, vp]
         L.orc_csr_inf_norm_d.restype = d
+        L.orc_coo2csr_d.argtypes = [i32, i32, i64, vp, vp, vp, vp, vp, vp]
+        L.orc_csc2csr_d.argtypes = [i32, i32, vp, vp, vp, vp, vp, vp]
     return _port
 
 
@@ -77,6 +79,8 @@ def ref():
         L.perflibs_spmat_create_csr_d.argtypes = [vp, i32, i32, vp, vp, vp, i32]
         L.perflibs_spmat_create_csr_s.argtypes = [vp, i32, i32, vp, vp, vp, i32]
         L.perflibs_spmat_create_bsr_d.argtypes = [vp, C.c_int, i32, i32, i32, vp, vp, vp, i32]
+        L.perflibs_spmat_create_coo_d.argtypes = [vp, i32, i32, i32, vp, vp, vp, i32]
+        L.perflibs_spmat_create_csc_d.argtypes = [vp, i32, i32, vp, vp, vp, i32]
         L.perflibs_spmat_create_dense_d.argtypes = [vp, C.c_int, i32, i32, i32, vp, i32]
         L.perflibs_spmat_create_dense_s.argtypes = [vp, C.c_int, i32, i32, i32, vp, i32]
         L.perflibs_spmat_create_null.argtypes = [i32, i32]
@@ -228,6 +232,32 @@ def csr_inf_norm(row_ptr, vals):
     return port().orc_csr_inf_norm_d(len(row_ptr) - 1, _p(row_ptr), _p(vals))
 
 
+def coo2csr(m, n, row, col, vals):
+    """0-based COO -> CSR by (row, column), duplicates kept in input order."""
+    row = np.ascontiguousarray(row, np.int32)
+    col = np.ascontiguousarray(col, np.int32)
+    vals = np.ascontiguousarray(vals, np.float64)
+    nnz = len(vals)
+    rp = np.zeros(m + 1, np.int32)
+    c = np.zeros(max(nnz, 1), np.int32)
+    v = np.zeros(max(nnz, 1))
+    port().orc_coo2csr_d(m, n, nnz, _p(row), _p(col), _p(vals), _p(rp), _p(c), _p(v))
+    return rp, c[:nnz], v[:nnz]
+
+
+def csc2csr(m, n, row_indx, col_ptr, vals):
+    """CSC -> CSR with ascending columns per row (keeps col_ptr[0]'s base)."""
+    row_indx = np.ascontiguousarray(row_indx, np.int32)
+    col_ptr = np.ascontiguousarray(col_ptr, np.int32)
+    vals = np.ascontiguousarray(vals, np.float64)
+    nnz = int(col_ptr[n] - col_ptr[0])
+    rp = np.zeros(m + 1, np.int32)
+    c = np.zeros(max(nnz, 1), np.int32)
+    v = np.zeros(max(nnz, 1))
+    port().orc_csc2csr_d(m, n, _p(row_indx), _p(col_ptr), _p(vals), _p(rp), _p(c), _p(v))
+    return rp, c[:nnz], v[:nnz]
+
+
 # ------------------------------------------------------------ reference API
 
 
@@ -272,6 +302,47 @@ class RefMatrix:
         if st != 0:
             raise RuntimeError(f"reference create_csr failed: {st}")
         return RefMatrix(h)
+
+    @staticmethod
+    def coo(m, n, row, col, vals):
+        L = ref()
+        h = C.c_void_p()
+        row = np.ascontiguousarray(row, np.int32)
+        col = np.ascontiguousarray(col, np.int32)
+        vals = np.ascontiguousarray(vals, np.float64)
+        st = L.perflibs_spmat_create_coo_d(C.byref(h), m, n, len(vals), _p(row), _p(col), _p(vals), 0)
+        if st != 0:
+            raise RuntimeError(f"reference create_coo failed: {st}")
+        return RefMatrix(h)
+
+    @staticmethod
+    def csc(m, n, row_indx, col_ptr, vals):
+        L = ref()
+        h = C.c_void_p()
+        row_indx = np.ascontiguousarray(row_indx, np.int32)
+        col_ptr = np.ascontiguousarray(col_ptr, np.int32)
+        vals = np.ascontiguousarray(vals, np.float64)
+        st = L.perflibs_spmat_create_csc_d(C.byref(h), m, n, _p(row_indx), _p(col_ptr), _p(vals), 0)
+        if st != 0:
+            raise RuntimeError(f"reference create_csc failed: {st}")
+        return RefMatrix(h)
+
+    def export_csr(self, m, index_base=0):
+        """The reference's own export (it converts the handle to CSR first)."""
+        L = ref()
+        rows, cols = C.c_int32(), C.c_int32()
+        rp, ci, vv = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        st = L.perflibs_spmat_export_csr_d(self.h, index_base, C.byref(rows), C.byref(cols),
+                                           C.byref(rp), C.byref(ci), C.byref(vv))
+        if st != 0:
+            raise RuntimeError(f"reference export_csr failed: {st}")
+        r = np.ctypeslib.as_array(C.cast(rp, C.POINTER(C.c_int32)), (rows.value + 1,)).copy()
+        nnz = int(r[-1] - r[0])
+        c = np.ctypeslib.as_array(C.cast(ci, C.POINTER(C.c_int32)), (max(nnz, 1),))[:nnz].copy()
+        v = np.ctypeslib.as_array(C.cast(vv, C.POINTER(C.c_double)), (max(nnz, 1),))[:nnz].copy()
+        for ptr in (rp, ci, vv):
+            L.free_ptr(ptr)
+        return r, c, v
 
     def hint(self, hint, value):
         return ref().perflibs_spmat_hint(self.h, hint, value)

@@ -478,3 +478,71 @@ double orc_csr_inf_norm_d(int32_t m, const int32_t *row_ptr,
   }
   return mx;
 }
+
+/* ------------------------------------------------------- COO / CSC input -- */
+
+/* coo2csr (compressed_sparse_rows.cpp:591-640): entries ordered by the key
+ * row*n + col, every entry kept (duplicates too), row_ptr from the row
+ * counts. The reference sorts (value, key) pairs with std::sort on the key,
+ * which leaves the order of equal keys unspecified; this restatement keeps
+ * equal keys in input order (two stable counting passes: by column, then by
+ * row). Indices are 0-based (the C interface's COO base). */
+void orc_coo2csr_d(int32_t m, int32_t n, int64_t nnz, const int32_t *row,
+                   const int32_t *col, const double *vals, int32_t *row_ptr,
+                   int32_t *col_out, double *vals_out) {
+  int64_t *cnt = (int64_t *)calloc((size_t)(n > m ? n : m) + 1, sizeof(int64_t));
+  int64_t *tmp = (int64_t *)malloc(sizeof(int64_t) * (size_t)(nnz > 0 ? nnz : 1));
+  int64_t *ord = (int64_t *)malloc(sizeof(int64_t) * (size_t)(nnz > 0 ? nnz : 1));
+  /* pass 1: stable by column */
+  for (int64_t i = 0; i < nnz; ++i)
+    cnt[col[i] + 1]++;
+  for (int32_t j = 0; j < n; ++j)
+    cnt[j + 1] += cnt[j];
+  for (int64_t i = 0; i < nnz; ++i)
+    tmp[cnt[col[i]]++] = i;
+  /* pass 2: stable by row */
+  memset(cnt, 0, sizeof(int64_t) * ((size_t)(n > m ? n : m) + 1));
+  for (int64_t i = 0; i < nnz; ++i)
+    cnt[row[i] + 1]++;
+  for (int32_t r = 0; r < m; ++r)
+    cnt[r + 1] += cnt[r];
+  for (int32_t r = 0; r <= m; ++r)
+    row_ptr[r] = (int32_t)cnt[r];
+  for (int64_t t = 0; t < nnz; ++t) {
+    const int64_t i = tmp[t];
+    ord[cnt[row[i]]++] = i;
+  }
+  for (int64_t t = 0; t < nnz; ++t) {
+    col_out[t] = col[ord[t]];
+    vals_out[t] = vals[ord[t]];
+  }
+  free(cnt);
+  free(tmp);
+  free(ord);
+}
+
+/* csc2csr (compressed_sparse_rows.cpp:750-800): count entries per row, scan,
+ * then walk the columns in order and append each entry to its row, so the
+ * columns of every row come out ascending. Index base from col_ptr[0]; the
+ * output keeps that base. */
+void orc_csc2csr_d(int32_t m, int32_t n, const int32_t *row_indx,
+                   const int32_t *col_ptr, const double *vals, int32_t *row_ptr,
+                   int32_t *col_out, double *vals_out) {
+  const int32_t base = col_ptr[0];
+  const int64_t nnz = (int64_t)col_ptr[n] - base;
+  int64_t *next = (int64_t *)calloc((size_t)m + 1, sizeof(int64_t));
+  for (int64_t k = 0; k < nnz; ++k)
+    next[row_indx[k] - base + 1]++;
+  for (int32_t r = 0; r < m; ++r)
+    next[r + 1] += next[r];
+  for (int32_t r = 0; r <= m; ++r)
+    row_ptr[r] = (int32_t)next[r] + base;
+  for (int32_t j = 0; j < n; ++j)
+    for (int64_t k = col_ptr[j] - base; k < col_ptr[j + 1] - base; ++k) {
+      const int32_t r = row_indx[k] - base;
+      const int64_t o = next[r]++;
+      col_out[o] = j + base;
+      vals_out[o] = vals[k];
+    }
+  free(next);
+}

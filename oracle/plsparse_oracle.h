@@ -143,6 +143,19 @@ void orc_csr_spmm_s(int32_t m, const int32_t *row_ptr, const int32_t *col,
 double orc_csr_inf_norm_d(int32_t m, const int32_t *row_ptr,
                           const double *vals);
 
+/* ---- COO / CSC input (src/compressed_sparse_rows.cpp) ---- */
+/* coo2csr (:591-640), 0-based: entries by (row, column), all kept; equal
+ * positions in input order (the reference's std::sort leaves them
+ * unspecified). row_ptr has m+1 entries, col_out / vals_out nnz. */
+void orc_coo2csr_d(int32_t m, int32_t n, int64_t nnz, const int32_t *row,
+                   const int32_t *col, const double *vals, int32_t *row_ptr,
+                   int32_t *col_out, double *vals_out);
+/* csc2csr (:750-800): columns ascending in every row; keeps the base of
+ * col_ptr[0]. */
+void orc_csc2csr_d(int32_t m, int32_t n, const int32_t *row_indx,
+                   const int32_t *col_ptr, const double *vals, int32_t *row_ptr,
+                   int32_t *col_out, double *vals_out);
+
 #ifdef __cplusplus
 }
 #endif

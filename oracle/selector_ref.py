@@ -138,3 +138,12 @@ def mlp_loss_grad(params, K, X, T):
     gb1 = dh1.sum(0)
     grad = np.concatenate([gW1.ravel(), gb1, gW2.ravel(), gb2, gW3.ravel(), gb3])
     return loss, grad
+
+
+def mlp_predict(params, K, X):
+    """Class scores (logits) of the MLP for feature rows X, FP64."""
+    W1, b1, W2, b2, W3, b3, mean, istd = split_params(np.asarray(params, np.float64), K)
+    xn = (np.asarray(X, np.float64) - mean) * istd
+    h1 = np.maximum(xn @ W1.T + b1, 0)
+    h2 = np.maximum(h1 @ W2.T + b2, 0)
+    return h2 @ W3.T + b3

@@ -84,6 +84,10 @@ def lib():
             "perflibs_spmat_create_dense_d": [vp, i, i32, i32, i32, vp, i32],
             "perflibs_spmat_create_bsr_s": [vp, i, i32, i32, i32, vp, vp, vp, i32],
             "perflibs_spmat_create_bsr_d": [vp, i, i32, i32, i32, vp, vp, vp, i32],
+            "perflibs_spmat_create_csc_s": [vp, i32, i32, vp, vp, vp, i32],
+            "perflibs_spmat_create_csc_d": [vp, i32, i32, vp, vp, vp, i32],
+            "perflibs_spmat_create_coo_s": [vp, i32, i32, i32, vp, vp, vp, i32],
+            "perflibs_spmat_create_coo_d": [vp, i32, i32, i32, vp, vp, vp, i32],
             "perflibs_spmat_create_null": [i32, i32],
             "perflibs_spmat_create_identity": [i32],
             "perflibs_spmat_destroy": [vp],
@@ -104,6 +108,10 @@ def lib():
             "perflibs_spnorm_exec_s": [vp, i, vp],
             "perflibs_spnorm_exec_d": [vp, i, vp],
             "perflibs_spmat_print_err": [vp],
+            "perflibs_b200_spmat_get_error": [vp, vp, vp, vp, i32],
+            "perflibs_b200_spmat_spmm_info": [vp, vp, vp, vp, vp, vp, vp],
+            "perflibs_b200_spmat_set_spmm_path": [vp, i32],
+            "perflibs_b200_read_mtx": [C.c_char_p, vp, vp, vp, vp, vp, vp],
             "perflibs_b200_spmv_exec_d_dev": [i, d, vp, vp, d, vp, vp],
             "perflibs_b200_spmv_exec_s_dev": [i, f, vp, vp, f, vp, vp],
             "perflibs_b200_spmm_exec_d_dev": [d, vp, vp, i64, i32, d, vp, i64, vp],
@@ -172,6 +180,37 @@ class SpMat:
         M.status = st
         if check:
             _check(st, "create_csr")
+        return M
+
+    @staticmethod
+    def coo(m, n, row, col, vals, flags=0, check=True):
+        """COO input (0-based, any order, duplicates allowed); the library
+        converts it to CSR on the device."""
+        vals = np.ascontiguousarray(vals)
+        row = np.ascontiguousarray(row, np.int32)
+        col = np.ascontiguousarray(col, np.int32)
+        h = C.c_void_p()
+        fn = lib().perflibs_spmat_create_coo_s if vals.dtype == np.float32 else lib().perflibs_spmat_create_coo_d
+        st = fn(C.byref(h), m, n, len(vals), _p(row), _p(col), _p(vals), flags)
+        M = SpMat(h, vals.dtype)
+        M.status = st
+        if check:
+            _check(st, "create_coo")
+        return M
+
+    @staticmethod
+    def csc(m, n, row_indx, col_ptr, vals, flags=0, check=True):
+        """CSC input (0- or 1-based, as col_ptr[0] says)."""
+        vals = np.ascontiguousarray(vals)
+        row_indx = np.ascontiguousarray(row_indx, np.int32)
+        col_ptr = np.ascontiguousarray(col_ptr, np.int32)
+        h = C.c_void_p()
+        fn = lib().perflibs_spmat_create_csc_s if vals.dtype == np.float32 else lib().perflibs_spmat_create_csc_d
+        st = fn(C.byref(h), m, n, _p(row_indx), _p(col_ptr), _p(vals), flags)
+        M = SpMat(h, vals.dtype)
+        M.status = st
+        if check:
+            _check(st, "create_csc")
         return M
 
     @staticmethod
@@ -386,6 +425,32 @@ class SpMat:
     def print_err(self):
         lib().perflibs_spmat_print_err(self.h)
 
+    def error(self):
+        """(status, argument position, message) of the handle's last error."""
+        t, c = C.c_int32(), C.c_int32()
+        buf = C.create_string_buffer(512)
+        lib().perflibs_b200_spmat_get_error(self.h, C.byref(t), C.byref(c), buf, 512)
+        return t.value, c.value, buf.value.decode(errors="replace")
+
+    def error_code(self):
+        return self.error()[1]
+
+    def spmm_info(self):
+        """SpMM plan: tile_rows (0 = no staged tiles), staged_rows, runs,
+        path of the last SpMM (1 staged, 0 row group, -1 none) and the two
+        timings of the measured choice (ms, 0 when not measured)."""
+        r, u, n, pth = C.c_int32(), C.c_int64(), C.c_int64(), C.c_int32()
+        ms_s, ms_r = C.c_float(), C.c_float()
+        _check(lib().perflibs_b200_spmat_spmm_info(self.h, C.byref(r), C.byref(u), C.byref(n),
+                                                   C.byref(pth), C.byref(ms_s), C.byref(ms_r)),
+               "spmm_info")
+        return {"tile_rows": r.value, "staged_rows": u.value, "runs": n.value, "path": pth.value,
+                "ms_staged": ms_s.value, "ms_rows": ms_r.value}
+
+    def set_spmm_path(self, path):
+        """-1 measured choice (default), 0 row-group kernel, 1 staged kernel."""
+        _check(lib().perflibs_b200_spmat_set_spmm_path(self.h, path), "set_spmm_path")
+
     def destroy(self):
         if self.h is not None and self.h.value:
             lib().perflibs_spmat_destroy(self.h)
@@ -456,6 +521,28 @@ class Batch:
 
 def spmm_optimize(transA, transB, alpha_hint, A: SpMat, B: SpMat, beta_hint, Cm: SpMat):
     return lib().perflibs_spmm_optimize(transA, transB, alpha_hint, A.h, B.h, beta_hint, Cm.h)
+
+
+def read_mtx(path):
+    """Matrix Market coordinate file -> (m, n, row_ptr, col, vals), 0-based
+    CSR ordered by (row, column), symmetric files expanded (host only)."""
+    L = lib()
+    m, n, nnz = C.c_int32(), C.c_int32(), C.c_int64()
+    rp, ci, vv = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    st = L.perflibs_b200_read_mtx(os.fsencode(path), C.byref(m), C.byref(n), C.byref(nnz),
+                                  C.byref(rp), C.byref(ci), C.byref(vv))
+    _check(st, "read_mtx")
+    libc = C.CDLL(None)
+    libc.free.argtypes = [C.c_void_p]
+    try:
+        k = nnz.value
+        row_ptr = np.ctypeslib.as_array(C.cast(rp, C.POINTER(C.c_int32)), (m.value + 1,)).copy()
+        col = np.ctypeslib.as_array(C.cast(ci, C.POINTER(C.c_int32)), (max(k, 1),))[:k].copy()
+        vals = np.ctypeslib.as_array(C.cast(vv, C.POINTER(C.c_double)), (max(k, 1),))[:k].copy()
+    finally:
+        for ptr in (rp, ci, vv):
+            libc.free(ptr)
+    return m.value, n.value, row_ptr, col, vals
 
 
 def spmm_exec(transA, transB, alpha, A: SpMat, B: SpMat, beta, Cm: SpMat):

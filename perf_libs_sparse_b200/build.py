@@ -19,6 +19,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libplsparse_b200.so")
+DRIVERS = os.path.join(HERE, "drivers")
+BENCH_DRIVER = os.path.join(HERE, "bench_sparse_x_dense")
 ROOT = os.path.dirname(HERE)
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -48,7 +50,9 @@ def stale() -> bool:
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    for d in (CSRC, os.path.join(ROOT, "include")):
+    if not os.path.exists(BENCH_DRIVER):
+        return True
+    for d in (CSRC, DRIVERS, os.path.join(ROOT, "include")):
         for f in os.listdir(d):
             if os.path.getmtime(os.path.join(d, f)) > t:
                 return True
@@ -67,12 +71,28 @@ def build(verbose_ptxas: bool = False, force: bool = False) -> str:
             sys.stderr.write(log)
     objs = [o for o, _ in results]
     tmp = LIB + ".tmp"
-    cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs]
+    cmd = [nvcc(), *ARCH, "-shared", "-Xlinker", "-soname=libplsparse_b200.so", "-o", tmp, *objs]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     os.replace(tmp, LIB)
+    _build_driver()
     return LIB
+
+
+def _build_driver() -> None:
+    """The Matrix Market SpMM driver (drivers/bench_sparse_x_dense.c), a
+    plain C program on the drop-in interface, linked to the library next to
+    it (rpath $ORIGIN)."""
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        raise RuntimeError("no C compiler for the driver")
+    cmd = [cc, "-O2", "-std=c11", f"-I{os.path.join(ROOT, 'include')}",
+           os.path.join(DRIVERS, "bench_sparse_x_dense.c"), LIB, "-Wl,-rpath,$ORIGIN", "-lm",
+           "-o", BENCH_DRIVER]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"driver build failed:\n{r.stdout}\n{r.stderr}")
 
 
 if __name__ == "__main__":

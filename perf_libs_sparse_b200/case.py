@@ -88,7 +88,8 @@ def main():
     else:
         b = W.algorithmic_bytes_spmv(m, n, nnz, sv, sx, False)
     print(json.dumps({"matrix": args.matrix, "m": m, "nnz": nnz, "k": args.k, "config": A.config(),
-                      "exec_info": A.exec_info(), "ms": ms, "gbs": b / ms / 1e6, "bytes": b}))
+                      "exec_info": A.exec_info(), "spmm": A.spmm_info() if args.k > 0 else None,
+                      "ms": ms, "gbs": b / ms / 1e6, "bytes": b}))
 
 
 if __name__ == "__main__":

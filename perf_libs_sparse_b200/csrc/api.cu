@@ -230,6 +230,115 @@ perflibs_status_t create_csr(Mat **out, int32_t m, int32_t n, const int32_t *row
     upload_index(c.row_ptr, row_ptr, (int64_t)m + 1, A->index_base, s);
     upload_index(c.col, col, A->nnz, A->index_base, s);
     upload(c.vals, vals, sizeof(T) * A->nnz, s);
+    // Indices are checked before any kernel uses them (the reference reads
+    // them as they are).
+    const auto bad = check_compressed(m, n, A->nnz, c.row_ptr.as<int32_t>(), c.col.as<int32_t>(), s);
+    if (bad.first >= 0)
+      return param_error(A, 4, "row_ptr decreases or leaves [0, nnz] at row " + std::to_string(bad.first));
+    if (bad.second >= 0)
+      return param_error(A, 5, "col_indx[" + std::to_string(bad.second) + "] is outside [0, n)");
+    A->cfg = default_config(A);
+    return PERFLIBS_STATUS_SUCCESS;
+  });
+}
+
+// COO input (0-based, the C interface's base: src/matrix_api.cpp:95-101),
+// converted to CSR on the device at creation; the handle is a CSR handle
+// from then on, as the reference's handle becomes one when it is converted
+// (src/convert.cpp:112-116).
+template <class T>
+perflibs_status_t create_coo(Mat **out, int32_t m, int32_t n, int32_t nnz, const int32_t *row,
+                             const int32_t *col, const T *vals, int32_t flags) {
+  (void)flags;
+  if (!out)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  Mat *A = nullptr;
+  try {
+    A = new_mat(dt_of<T>(), Fmt::CSR);
+  } catch (const Error &e) {
+    *out = nullptr;
+    return e.status;
+  }
+  *out = A;
+  return guarded(A, [&]() -> perflibs_status_t {
+    // src/coordinate_list.cpp:140-151 checks m and n; a negative nnz and
+    // indices out of range are rejected here too (the reference reads them
+    // as they are).
+    if (m < 0)
+      return param_error(A, 2);
+    if (n < 0)
+      return param_error(A, 3);
+    if (nnz < 0)
+      return param_error(A, 4);
+    if (nnz > 0 && (!row || !col || !vals))
+      return param_error(A, !row ? 5 : !col ? 6 : 7);
+    A->m = m;
+    A->n = n;
+    A->index_base = 0;
+    A->nnz = nnz;
+    DeviceGuard g(A->device);
+    cudaStream_t s = stream_of(A);
+    DevBuf drow, dcol, dval;
+    upload(drow, row, sizeof(int32_t) * (size_t)nnz, s);
+    upload(dcol, col, sizeof(int32_t) * (size_t)nnz, s);
+    upload(dval, vals, sizeof(T) * (size_t)nnz, s);
+    const int64_t bad = coo_to_csr(m, n, nnz, drow.as<int32_t>(), dcol.as<int32_t>(), dval.p,
+                                   native_vt(A->dt), A->csr, s);
+    if (bad >= 0)
+      return param_error(A, row[bad] < 0 || row[bad] >= m ? 5 : 6,
+                         "entry " + std::to_string(bad) + " is outside the matrix");
+    A->cfg = default_config(A);
+    return PERFLIBS_STATUS_SUCCESS;
+  });
+}
+
+// CSC input: the CSC arrays are the CSR of A^T, transposed on the device
+// into the CSR of A (columns ascending in each row, the order of the
+// reference's csc2csr: src/compressed_sparse_rows.cpp:750-800).
+template <class T>
+perflibs_status_t create_csc(Mat **out, int32_t m, int32_t n, const int32_t *row_indx,
+                             const int32_t *col_ptr, const T *vals, int32_t flags) {
+  (void)flags;
+  if (!out)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  Mat *A = nullptr;
+  try {
+    A = new_mat(dt_of<T>(), Fmt::CSR);
+  } catch (const Error &e) {
+    *out = nullptr;
+    return e.status;
+  }
+  *out = A;
+  return guarded(A, [&]() -> perflibs_status_t {
+    // src/compressed_sparse_columns.cpp:162-178
+    if (m < 0)
+      return param_error(A, 2);
+    if (n < 0)
+      return param_error(A, 3);
+    if (!col_ptr || (col_ptr[0] != 0 && col_ptr[0] != 1))
+      return param_error(A, 4);
+    A->m = m;
+    A->n = n;
+    A->index_base = col_ptr[0];
+    A->nnz = (int64_t)col_ptr[n] - A->index_base;
+    if (A->nnz < 0)
+      return param_error(A, 5, "col_ptr[n] is below col_ptr[0]");
+    if (A->nnz > 0 && (!row_indx || !vals))
+      return param_error(A, !row_indx ? 4 : 6);
+    DeviceGuard g(A->device);
+    cudaStream_t s = stream_of(A);
+    CsrDev t;  // CSR of A^T: n rows, m columns
+    t.nnz = A->nnz;
+    t.vt = native_vt(A->dt);
+    upload_index(t.row_ptr, col_ptr, (int64_t)n + 1, A->index_base, s);
+    upload_index(t.col, row_indx, A->nnz, A->index_base, s);
+    upload(t.vals, vals, sizeof(T) * A->nnz, s);
+    const auto bad = check_compressed(n, m, A->nnz, t.row_ptr.as<int32_t>(), t.col.as<int32_t>(), s);
+    if (bad.first >= 0)
+      return param_error(A, 5, "col_ptr decreases or leaves [0, nnz] at column " + std::to_string(bad.first));
+    if (bad.second >= 0)
+      return param_error(A, 4, "row_indx[" + std::to_string(bad.second) + "] is outside [0, m)");
+    build_csr_transpose(t, n, m, A->csr, s);
     PLS_CUDA(cudaStreamSynchronize(s));
     A->cfg = default_config(A);
     return PERFLIBS_STATUS_SUCCESS;
@@ -279,7 +388,11 @@ perflibs_status_t create_bsr(Mat **out, int layout, int32_t m, int32_t n, int32_
     upload_index(b.row_ptr, row_ptr, (int64_t)b.mb + 1, A->index_base, s);
     upload_index(b.col, col, b.nnzb, A->index_base, s);
     upload(b.vals, vals, sizeof(T) * A->nnz, s);
-    PLS_CUDA(cudaStreamSynchronize(s));
+    const auto bad = check_compressed(b.mb, b.nb, b.nnzb, b.row_ptr.as<int32_t>(), b.col.as<int32_t>(), s);
+    if (bad.first >= 0)
+      return param_error(A, 6, "row_ptr decreases or leaves [0, nnzb] at block row " + std::to_string(bad.first));
+    if (bad.second >= 0)
+      return param_error(A, 7, "col_indx[" + std::to_string(bad.second) + "] is outside [0, n / bs)");
     return PERFLIBS_STATUS_SUCCESS;
   });
 }
@@ -1001,6 +1114,34 @@ perflibs_status_t perflibs_spmat_create_bsr_d(perflibs_spmat_t *A,
   return create_bsr<double>(A, block_layout, m, n, block_size, row_ptr, col_indx, vals, flags);
 }
 
+// include/perflibs_sparse.h:176-208 (reference)
+perflibs_status_t perflibs_spmat_create_csc_s(perflibs_spmat_t *A, perflibs_int_t m,
+                                              perflibs_int_t n, const perflibs_int_t *row_indx,
+                                              const perflibs_int_t *col_ptr, const float *vals,
+                                              perflibs_int_t flags) {
+  return create_csc<float>(A, m, n, row_indx, col_ptr, vals, flags);
+}
+perflibs_status_t perflibs_spmat_create_csc_d(perflibs_spmat_t *A, perflibs_int_t m,
+                                              perflibs_int_t n, const perflibs_int_t *row_indx,
+                                              const perflibs_int_t *col_ptr, const double *vals,
+                                              perflibs_int_t flags) {
+  return create_csc<double>(A, m, n, row_indx, col_ptr, vals, flags);
+}
+perflibs_status_t perflibs_spmat_create_coo_s(perflibs_spmat_t *A, perflibs_int_t m,
+                                              perflibs_int_t n, perflibs_int_t nnz,
+                                              const perflibs_int_t *row_indx,
+                                              const perflibs_int_t *col_indx, const float *vals,
+                                              perflibs_int_t flags) {
+  return create_coo<float>(A, m, n, nnz, row_indx, col_indx, vals, flags);
+}
+perflibs_status_t perflibs_spmat_create_coo_d(perflibs_spmat_t *A, perflibs_int_t m,
+                                              perflibs_int_t n, perflibs_int_t nnz,
+                                              const perflibs_int_t *row_indx,
+                                              const perflibs_int_t *col_indx, const double *vals,
+                                              perflibs_int_t flags) {
+  return create_coo<double>(A, m, n, nnz, row_indx, col_indx, vals, flags);
+}
+
 // src/matrix_state.cpp:39-58: NULL for negative sizes.
 perflibs_spmat_t perflibs_spmat_create_null(perflibs_int_t m, perflibs_int_t n) {
   if (m < 0 || n < 0)
@@ -1325,6 +1466,52 @@ void perflibs_spmat_print_err(perflibs_spmat_t A) {
 }
 
 // ---------------------------------------------------------- extensions
+
+perflibs_status_t perflibs_b200_spmat_set_spmm_path(perflibs_spmat_t A, int32_t path) {
+  if (!A || path < -1 || path > 1)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  A->csr.tiles.forced = path;
+  A->csr.tiles.choice_sig = -1;
+  A->csr.tiles.last_path = -1;
+  return PERFLIBS_STATUS_SUCCESS;
+}
+
+perflibs_status_t perflibs_b200_spmat_spmm_info(perflibs_spmat_t A, int32_t *tile_rows,
+                                                int64_t *staged_rows, int64_t *runs,
+                                                int32_t *path, float *ms_staged, float *ms_rows) {
+  if (!A)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  const TileDev &t = A->csr.tiles;
+  if (tile_rows)
+    *tile_rows = t.filled ? t.R : 0;
+  if (staged_rows)
+    *staged_rows = t.filled ? t.total_uniq : 0;
+  if (runs)
+    *runs = t.filled ? t.n_runs : 0;
+  if (path)
+    *path = t.last_path;
+  if (ms_staged)
+    *ms_staged = t.choice_sig >= 0 ? t.ms_staged : 0.f;
+  if (ms_rows)
+    *ms_rows = t.choice_sig >= 0 ? t.ms_rows : 0.f;
+  return PERFLIBS_STATUS_SUCCESS;
+}
+
+perflibs_status_t perflibs_b200_spmat_get_error(perflibs_const_spmat_t A, int32_t *type,
+                                                int32_t *code, char *msg, int32_t msg_len) {
+  if (!A)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  if (type)
+    *type = A->err_type;
+  if (code)
+    *code = A->err_code;
+  if (msg && msg_len > 0) {
+    const size_t n = std::min<size_t>(A->err_msg.size(), (size_t)msg_len - 1);
+    std::memcpy(msg, A->err_msg.data(), n);
+    msg[n] = 0;
+  }
+  return PERFLIBS_STATUS_SUCCESS;
+}
 
 perflibs_status_t perflibs_b200_spmv_exec_d_dev(enum perflibs_sparse_hint_value trans,
                                                 double alpha, perflibs_spmat_t A,
@@ -1670,6 +1857,11 @@ perflibs_status_t perflibs_b200_spmat_create_csr_d_dev(perflibs_spmat_t *out, in
       return param_error(A, 3);
     if (!row_ptr)
       return param_error(A, 4);
+    // With no stream named, the arrays may still be being written on any
+    // stream (the library's own stream does not wait for the legacy default
+    // stream), so wait for all prior work on the device first.
+    if (!stream)
+      PLS_CUDA(cudaDeviceSynchronize());
     cudaStream_t s = stream ? (cudaStream_t)stream : stream_of(A);
     int32_t ends[2] = {0, 0};
     PLS_CUDA(cudaMemcpyAsync(&ends[0], row_ptr, 4, cudaMemcpyDeviceToHost, s));
@@ -1701,7 +1893,11 @@ perflibs_status_t perflibs_b200_spmat_create_csr_d_dev(perflibs_spmat_t *out, in
         k_sub_base<<<(unsigned)div_up(A->nnz, 256), 256, 0, s>>>(A->nnz, 1, c.col.as<int32_t>());
       PLS_LAUNCH_CHECK();
     }
-    PLS_CUDA(cudaStreamSynchronize(s));
+    const auto bad = check_compressed(m, n, A->nnz, c.row_ptr.as<int32_t>(), c.col.as<int32_t>(), s);
+    if (bad.first >= 0)
+      return param_error(A, 4, "row_ptr decreases or leaves [0, nnz] at row " + std::to_string(bad.first));
+    if (bad.second >= 0)
+      return param_error(A, 5, "col_indx[" + std::to_string(bad.second) + "] is outside [0, n)");
     A->cfg = default_config(A);
     return PERFLIBS_STATUS_SUCCESS;
   });

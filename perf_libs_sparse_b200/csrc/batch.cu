@@ -9,10 +9,10 @@
 // whatever the scheduling; the counter is reset by a memset node in the same
 // CUDA graph that holds the launch.
 //
-// Inside an item, a group of L lanes (L = the power of two covering k_i,
-// at most 32) owns one row: lane s accumulates columns s, s+L, ... of the
-// row's output over the row's nonzeros in stored order (CSR), or over the
-// block row's blocks and each block's columns (BSR).
+// Inside an item, rows go through the row-group loop of spmm_rows.cuh with
+// the instance's own lane shape (TK lanes over C's columns, 16-byte vectors
+// when its B and C allow, TN lanes over a row's entries); a BSR instance is
+// read as scalar rows whose entries are (block, column-in-block) pairs.
 #include <algorithm>
 #include <cstring>
 #include <numeric>
@@ -20,6 +20,7 @@
 
 #include "common.cuh"
 #include "pls_internal.hpp"
+#include "spmm_rows.cuh"
 
 namespace pls {
 
@@ -32,87 +33,48 @@ struct InstDesc {
   const float *B;
   float *C;
   int64_t ldb, ldc;
-  int32_t m, k, bs, layout, lanes, is_bsr;
+  int32_t m, k, bs, layout, is_bsr;
+  int32_t lg_tk, lg_tn, path;  // path: 0 = VEC 4, 1 = VEC 1 x 1, 2 = VEC 1 x 2
 };
 
 struct Item {
   int32_t inst, row0, row1, pad;
 };
 
-constexpr int kMaxColsPerLane = 4;  // k <= 32 * 4 per pass
-
 __global__ void __launch_bounds__(256)
     k_batch_spmm(const InstDesc *__restrict__ inst, const Item *__restrict__ items,
                  int64_t n_items, unsigned long long *__restrict__ counter, float alpha,
                  float beta, int beta_nz) {
+  const L2Policy pol = make_l2_policy();
   const int lane = threadIdx.x & 31;
-  for (;;) {
-    unsigned long long it = 0;
+  unsigned long long it = 0;
+  if (lane == 0)
+    it = atomicAdd(counter, 1ull);
+  it = __shfl_sync(0xffffffffu, it, 0);
+  while (it < (unsigned long long)n_items) {
+    // Take the next ticket now; its round trip overlaps this item's loads.
+    unsigned long long next = 0;
     if (lane == 0)
-      it = atomicAdd(counter, 1ull);
-    it = __shfl_sync(0xffffffffu, it, 0);
-    if (it >= (unsigned long long)n_items)
-      return;
+      next = atomicAdd(counter, 1ull);
     const Item w = items[it];
     const InstDesc d = inst[w.inst];
-    const int L = d.lanes;
-    const int g = lane / L, s = lane % L, groups = 32 / L;
-    for (int32_t r = w.row0 + g; r < w.row1; r += groups) {
-      for (int kk0 = 0; kk0 < d.k; kk0 += L * kMaxColsPerLane) {
-        float acc[kMaxColsPerLane];
-#pragma unroll
-        for (int q = 0; q < kMaxColsPerLane; ++q)
-          acc[q] = 0.f;
-        if (!d.is_bsr) {
-          for (int32_t p = d.rp[r]; p < d.rp[r + 1]; ++p) {
-            const float a = ld_stream(d.val + p);
-            const float *brow = d.B + (int64_t)ld_stream(d.col + p) * d.ldb;
-#pragma unroll
-            for (int q = 0; q < kMaxColsPerLane; ++q) {
-              const int kk = kk0 + s + q * L;
-              if (kk < d.k)
-                acc[q] = fmaf(a, __ldg(brow + kk), acc[q]);
-            }
-          }
-        } else {
-          const int bs = d.bs;
-          const int32_t br = r / bs;
-          const int i = r % bs;
-          const int64_t E = (int64_t)bs * bs;
-          for (int32_t b = d.rp[br]; b < d.rp[br + 1]; ++b) {
-            const float *blk = d.val + b * E;
-            const int64_t c0 = (int64_t)d.col[b] * bs;
-            for (int jj = 0; jj < bs; ++jj) {
-              const float a = d.layout == PERFLIBS_ROW_MAJOR ? blk[i * bs + jj] : blk[jj * bs + i];
-              const float *brow = d.B + (c0 + jj) * d.ldb;
-#pragma unroll
-              for (int q = 0; q < kMaxColsPerLane; ++q) {
-                const int kk = kk0 + s + q * L;
-                if (kk < d.k)
-                  acc[q] = fmaf(a, __ldg(brow + kk), acc[q]);
-              }
-            }
-          }
-        }
-        float *crow = d.C + (int64_t)r * d.ldc;
-#pragma unroll
-        for (int q = 0; q < kMaxColsPerLane; ++q) {
-          const int kk = kk0 + s + q * L;
-          if (kk < d.k)
-            crow[kk] = beta_nz ? fmaf(alpha, acc[q], beta * crow[kk]) : alpha * acc[q];
-        }
-      }
+    const MixedRows A{d.rp, d.col, d.val, d.bs, d.layout == PERFLIBS_ROW_MAJOR, d.is_bsr};
+    const int lg_g = d.lg_tk + d.lg_tn;
+    for (int32_t r0 = w.row0; r0 < w.row1; r0 += (32 >> lg_g)) {
+      const int32_t row = r0 + (lane >> lg_g);
+      const bool live = row < w.row1;
+      if (d.path == 0)
+        spmm_row_group<4, 1, float, float>(A, row, live, d.lg_tk, d.lg_tn, d.B, d.ldb, d.C,
+                                           d.ldc, d.k, alpha, beta, beta_nz, pol);
+      else if (d.path == 1)
+        spmm_row_group<1, 1, float, float>(A, row, live, d.lg_tk, d.lg_tn, d.B, d.ldb, d.C,
+                                           d.ldc, d.k, alpha, beta, beta_nz, pol);
+      else
+        spmm_row_group<1, 2, float, float>(A, row, live, d.lg_tk, d.lg_tn, d.B, d.ldb, d.C,
+                                           d.ldc, d.k, alpha, beta, beta_nz, pol);
     }
+    it = __shfl_sync(0xffffffffu, next, 0);
   }
-}
-
-int lanes_for(int k) {
-  int L = 1;
-  while (L < 32 && L * kMaxColsPerLane < k)
-    L *= 2;
-  while (L < 32 && L < k && L * 2 <= k)  // at least one column per lane
-    L *= 2;
-  return std::min(L, 32);
 }
 
 }  // namespace
@@ -237,7 +199,6 @@ perflibs_status_t perflibs_b200_batch_create(perflibs_b200_batch_t *out, int32_t
       d.ldc = ldc[i];
       d.m = A->m;
       d.k = k[i];
-      d.lanes = lanes_for(k[i]);
       if (A->fmt == Fmt::BSR) {
         d.is_bsr = 1;
         d.bs = A->bsr.bs;
@@ -252,6 +213,21 @@ perflibs_status_t perflibs_b200_batch_create(perflibs_b200_batch_t *out, int32_t
         d.col = A->csr.col.as<int32_t>();
         d.val = A->csr.vals.as<float>();
       }
+      if (d.is_bsr && (int64_t)A->bsr.nnzb * d.bs > INT32_MAX) {
+        delete B;
+        *out = nullptr;
+        return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+      }
+      // Lane shape and vector width per instance: 16-byte vectors when k
+      // fills at least one and its B and C rows are 16-byte aligned (one
+      // vector tile per pass), else scalar columns with up to two per lane.
+      const bool v4 = k[i] >= 4 && (uintptr_t)Bp[i] % 16 == 0 && (uintptr_t)Cp[i] % 16 == 0 &&
+                      ldb[i] % 4 == 0 && ldc[i] % 4 == 0;
+      const RowsShape sh =
+          rows_shape(k[i], v4 ? 4 : 1, (double)A->nnz / std::max(A->m, 1), v4 ? 1 : 2);
+      d.lg_tk = sh.lg_tk;
+      d.lg_tn = sh.lg_tn;
+      d.path = v4 ? 0 : (sh.nv == 2 ? 2 : 1);
       B->host.push_back(d);
       B->work_per_row.push_back(((double)A->nnz / std::max(A->m, 1) + 1.0) * std::max(k[i], 1));
     }

@@ -418,6 +418,151 @@ void build_csr_transpose(const CsrDev &c, int32_t m, int32_t n, CsrDev &out,
   out = std::move(T);
 }
 
+namespace {
+
+// Key row * n + col per entry (the reference's coo2csr ordering key,
+// src/compressed_sparse_rows.cpp:591-640) and the entry's index; records
+// the first entry with an index out of range.
+__global__ void k_coo_keys(int64_t nnz, int32_t m, int32_t n, const int32_t *__restrict__ row,
+                           const int32_t *__restrict__ col, unsigned long long *__restrict__ key,
+                           int32_t *__restrict__ idx, unsigned long long *__restrict__ bad) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nnz)
+    return;
+  const int32_t r = row[i], c = col[i];
+  const bool ok = r >= 0 && r < m && c >= 0 && c < n;
+  if (!ok)
+    atomicMin(bad, (unsigned long long)i);
+  key[i] = ok ? (unsigned long long)r * (unsigned long long)n + (unsigned long long)c : 0ull;
+  idx[i] = (int32_t)i;
+}
+
+template <class V>
+__global__ void k_gather_entries(int64_t nnz, const int32_t *__restrict__ perm,
+                                 const int32_t *__restrict__ col, const V *__restrict__ val,
+                                 int32_t *__restrict__ ocol, V *__restrict__ oval) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nnz)
+    return;
+  const int32_t p = perm[i];
+  ocol[i] = col[p];
+  oval[i] = val[p];
+}
+
+}  // namespace
+
+namespace {
+
+__global__ void k_check_compressed(int32_t rows, int32_t cols, int64_t nnz,
+                                   const int32_t *__restrict__ ptr,
+                                   const int32_t *__restrict__ idx,
+                                   unsigned long long *__restrict__ bad) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < rows) {
+    const int32_t a = ptr[i], b = ptr[i + 1];
+    if (a < 0 || b < a || b > nnz)
+      atomicMin(bad, (unsigned long long)i);
+  }
+  if (i < nnz) {
+    const int32_t c = idx[i];
+    if (c < 0 || c >= cols)
+      atomicMin(bad + 1, (unsigned long long)i);
+  }
+}
+
+}  // namespace
+
+// Structure check of 0-based compressed arrays before any kernel indexes
+// with them: the first row whose pointers are decreasing or outside
+// [0, nnz], and the first entry whose index is outside [0, cols); -1 each
+// when there is none.
+std::pair<int64_t, int64_t> check_compressed(int32_t rows, int32_t cols, int64_t nnz,
+                                             const int32_t *ptr, const int32_t *idx,
+                                             cudaStream_t s) {
+  const int64_t work = std::max<int64_t>(rows, nnz);
+  if (work == 0)
+    return {-1, -1};
+  DevBuf bad;
+  bad.reserve(16);
+  PLS_CUDA(cudaMemsetAsync(bad.p, 0xff, 16, s));
+  k_check_compressed<<<(unsigned)div_up(work, 256), 256, 0, s>>>(
+      rows, cols, nnz, ptr, idx, bad.as<unsigned long long>());
+  PLS_LAUNCH_CHECK();
+  unsigned long long h[2];
+  PLS_CUDA(cudaMemcpyAsync(h, bad.p, 16, cudaMemcpyDeviceToHost, s));
+  PLS_CUDA(cudaStreamSynchronize(s));
+  return {h[0] == ~0ull ? -1 : (int64_t)h[0], h[1] == ~0ull ? -1 : (int64_t)h[1]};
+}
+
+// The entries sorted by (row, column) with a stable radix sort, so equal
+// positions keep their input order (the reference's std::sort leaves their
+// order unspecified; the values are all kept either way); row_ptr from the
+// per-row counts.
+int64_t coo_to_csr(int32_t m, int32_t n, int64_t nnz, const int32_t *row, const int32_t *col,
+                   const void *vals, Vt vt, CsrDev &out, cudaStream_t s) {
+  CsrDev R;
+  R.vt = vt;
+  R.nnz = nnz;
+  R.row_ptr.reserve(sizeof(int32_t) * ((size_t)m + 1));
+  R.col.reserve(sizeof(int32_t) * std::max<int64_t>(nnz, 1));
+  R.vals.reserve(vt_size(vt) * std::max<int64_t>(nnz, 1));
+  PLS_CUDA(cudaMemsetAsync(R.row_ptr.p, 0, sizeof(int32_t) * ((size_t)m + 1), s));
+  if (nnz > 0) {
+    DevBuf key, key_out, idx, idx_out, cnt, bad;
+    key.reserve(8 * nnz);
+    key_out.reserve(8 * nnz);
+    idx.reserve(4 * nnz);
+    idx_out.reserve(4 * nnz);
+    cnt.reserve(sizeof(int32_t) * ((size_t)m + 1));
+    bad.reserve(8);
+    PLS_CUDA(cudaMemsetAsync(bad.p, 0xff, 8, s));
+    k_coo_keys<<<(unsigned)div_up(nnz, 256), 256, 0, s>>>(nnz, m, n, row, col,
+                                                           key.as<unsigned long long>(),
+                                                           idx.as<int32_t>(),
+                                                           bad.as<unsigned long long>());
+    PLS_LAUNCH_CHECK();
+    unsigned long long first_bad = 0;
+    PLS_CUDA(cudaMemcpyAsync(&first_bad, bad.p, 8, cudaMemcpyDeviceToHost, s));
+    PLS_CUDA(cudaStreamSynchronize(s));
+    if (first_bad != ~0ull)
+      return (int64_t)first_bad;
+    const unsigned long long span = (unsigned long long)m * (unsigned long long)n;
+    int end_bit = 1;
+    while (end_bit < 64 && (span >> end_bit) != 0)
+      ++end_bit;
+    {
+      size_t tb = 0;
+      cub::DeviceRadixSort::SortPairs(nullptr, tb, key.as<unsigned long long>(),
+                                      key_out.as<unsigned long long>(), idx.as<int32_t>(),
+                                      idx_out.as<int32_t>(), (int)nnz, 0, end_bit, s);
+      CubTemp tmp;
+      PLS_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(tb), tb, key.as<unsigned long long>(),
+                                               key_out.as<unsigned long long>(),
+                                               idx.as<int32_t>(), idx_out.as<int32_t>(),
+                                               (int)nnz, 0, end_bit, s));
+    }
+    PLS_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int32_t) * ((size_t)m + 1), s));
+    k_count_keys<<<(unsigned)div_up(nnz, 256), 256, 0, s>>>(nnz, row, cnt.as<int32_t>());
+    {
+      size_t tb = 0;
+      cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.as<int32_t>(), R.row_ptr.as<int32_t>(),
+                                    m + 1, s);
+      CubTemp tmp;
+      PLS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(tb), tb, cnt.as<int32_t>(),
+                                             R.row_ptr.as<int32_t>(), m + 1, s));
+    }
+    with_vt(vt, [&](auto tag) {
+      using V = typename decltype(tag)::type;
+      k_gather_entries<V><<<(unsigned)div_up(nnz, 256), 256, 0, s>>>(
+          nnz, idx_out.as<int32_t>(), col, (const V *)vals, R.col.as<int32_t>(), R.vals.as<V>());
+    });
+    PLS_LAUNCH_CHECK();
+  }
+  PLS_CUDA(cudaStreamSynchronize(s));
+  out = std::move(R);
+  return -1;
+}
+
 void bsr_to_csr(const BsrDev &b, int32_t m, bool drop_zeros, CsrDev &out,
                 cudaStream_t s) {
   CsrDev R;

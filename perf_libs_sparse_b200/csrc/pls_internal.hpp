@@ -25,6 +25,7 @@
 #include <cstdio>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/perflibs_b200.h"
@@ -127,6 +128,67 @@ struct SpmvConfig {
 
 // ------------------------------------------------------------ formats
 
+// A 4-byte flag in mapped pinned host memory: kernels write it through the
+// device pointer, the host reads it without synchronising.
+struct HostFlag {
+  int *host = nullptr;
+  int *dev = nullptr;
+  HostFlag() = default;
+  HostFlag(const HostFlag &) = delete;
+  HostFlag &operator=(const HostFlag &) = delete;
+  HostFlag(HostFlag &&o) noexcept : host(o.host), dev(o.dev) { o.host = o.dev = nullptr; }
+  HostFlag &operator=(HostFlag &&o) noexcept {
+    if (this != &o) {
+      release();
+      host = o.host;
+      dev = o.dev;
+      o.host = o.dev = nullptr;
+    }
+    return *this;
+  }
+  ~HostFlag() { release(); }
+  void release() {
+    if (host)
+      cudaFreeHost(host);
+    host = dev = nullptr;
+  }
+  void alloc() {
+    if (host)
+      return;
+    void *h = nullptr, *d = nullptr;
+    PLS_CUDA(cudaHostAlloc(&h, sizeof(int), cudaHostAllocMapped));
+    *(volatile int *)h = 0;
+    PLS_CUDA(cudaHostGetDevicePointer(&d, h, 0));
+    host = (int *)h;
+    dev = (int *)d;
+  }
+};
+
+// Row-block tiles of the staged SpMM (spmm_tiled.cu): for every block of R
+// rows, its distinct columns as runs (c0, len, u0) and every nonzero's row
+// in the staged tile.
+struct TileDev {
+  int R = 0;
+  int64_t nblocks = 0;
+  int32_t max_uniq = 0, max_bnnz = 0;
+  int64_t total_uniq = 0, n_runs = 0;
+  bool filled = false;
+  // Smallest tile row width (bytes) found unsuitable (INT64_MAX: none).
+  int64_t unsuitable_from = INT64_MAX;
+  DevBuf nuniq, run_ptr, runs, local;
+  HostFlag err;
+  // Measured choice between the staged and the row-group SpMM for the call
+  // signature `choice_sig` (k, ldb, value and API types): 1 staged, 0 row
+  // group, -1 not measured; with both timings (ms).
+  int64_t choice_sig = -1;
+  int choice = -1;
+  float ms_staged = 0.f, ms_rows = 0.f;
+  // Path forced by perflibs_b200_spmat_set_spmm_path: -1 measured choice,
+  // 0 row group, 1 staged (when it applies).
+  int forced = -1;
+  int last_path = -1;  // path of the last SpMM: 1 staged, 0 row group
+};
+
 struct CsrDev {
   DevBuf row_ptr, col, vals;  // vals in the API type (authoritative)
   int64_t nnz = 0;
@@ -143,6 +205,8 @@ struct CsrDev {
   DevBuf long_rows;
   int n_long = 0;
   int long_threshold = 0;
+  // Staged-SpMM tiles (built on the first suitable SpMM).
+  TileDev tiles;
 };
 
 struct SellDev {
@@ -162,6 +226,9 @@ struct SellDev {
   DevBuf split_chunks;  // (chunk, first slot, slice count) per split chunk
   int64_t n_split = 0;
   DevBuf part;          // partial sums of the split chunks' slices (scratch)
+  // Chunk indices by decreasing width (stable); the SpMV kernel takes chunks
+  // in this order. Empty when all chunks have the same width.
+  DevBuf order;
 };
 
 struct BsrDev {
@@ -294,8 +361,14 @@ void scal(int64_t n, X beta, X *y, cudaStream_t s);
 
 // SpMM: C = alpha*A*B + beta*C, row-major B (ldb) and C (ldc), k columns.
 template <class X>
-void spmm_csr(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
+void spmm_csr(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
               int64_t ldc, int k, X alpha, X beta, cudaStream_t s);
+// Staged SpMM for matrices whose row blocks reuse B rows; false (nothing
+// launched) when the matrix, k or B's layout does not suit it. With
+// launch = false it only builds the tiles and says whether it applies.
+template <class X>
+bool spmm_tiled(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64_t ldc, int k,
+                X alpha, X beta, cudaStream_t s, bool launch = true);
 template <class X>
 void spmm_bsr(const BsrDev &b, const X *B, int64_t ldb, X *C, int64_t ldc,
               int k, X alpha, X beta, cudaStream_t s);
@@ -318,6 +391,17 @@ void build_csr_transpose(const CsrDev &c, int32_t m, int32_t n, CsrDev &out,
                          cudaStream_t s);
 void bsr_to_csr(const BsrDev &b, int32_t m, bool drop_zeros, CsrDev &out,
                 cudaStream_t s);
+// First bad row (pointers decreasing or outside [0, nnz]) and first bad
+// entry (index outside [0, cols)) of 0-based compressed device arrays, -1
+// when none.
+std::pair<int64_t, int64_t> check_compressed(int32_t rows, int32_t cols, int64_t nnz,
+                                             const int32_t *ptr, const int32_t *idx,
+                                             cudaStream_t s);
+// COO (0-based device arrays, any order, duplicates allowed) -> CSR sorted by
+// (row, column), duplicates kept in input order. Returns -1, or the first
+// entry whose row or column is out of range (then `out` is untouched).
+int64_t coo_to_csr(int32_t m, int32_t n, int64_t nnz, const int32_t *row, const int32_t *col,
+                   const void *vals, Vt vt, CsrDev &out, cudaStream_t s);
 void csr_to_bsr(const CsrDev &c, int32_t m, int32_t n, int bs, int layout,
                 BsrDev &out, cudaStream_t s);
 void csr_build_long_rows(CsrDev &c, int32_t m, int threshold, cudaStream_t s);

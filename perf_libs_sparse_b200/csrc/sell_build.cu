@@ -291,8 +291,27 @@ void build_sell(const CsrDev &c, int32_t m, int C, int sigma, SellDev &out,
       std::vector<int32_t> clh(S.nC);
       PLS_CUDA(cudaMemcpy(clh.data(), S.cl.p, sizeof(int32_t) * S.nC,
                           cudaMemcpyDeviceToHost));
-      for (auto v : clh)
+      int64_t wsum = 0;
+      for (auto v : clh) {
         wmax = std::max(wmax, v);
+        wsum += v;
+      }
+      // Longest-first processing order over the whole matrix: the widest
+      // chunks start first and the launch ends on the narrowest, and chunks
+      // of one block have similar widths, so its warps finish together. It
+      // costs one dependent load per chunk, so it is kept for layouts whose
+      // widest chunk is more than twice the mean width (power-law rows),
+      // where the uneven tail is what it removes.
+      if ((int64_t)wmax * S.nC > 2 * wsum) {
+        std::vector<int32_t> ord(S.nC);
+        for (int64_t i = 0; i < S.nC; ++i)
+          ord[i] = (int32_t)i;
+        std::stable_sort(ord.begin(), ord.end(),
+                         [&](int32_t a, int32_t b) { return clh[a] > clh[b]; });
+        S.order.reserve(sizeof(int32_t) * S.nC);
+        PLS_CUDA(cudaMemcpy(S.order.p, ord.data(), sizeof(int32_t) * S.nC,
+                            cudaMemcpyHostToDevice));
+      }
     }
     S.max_width = wmax;
   }

@@ -1,195 +1,125 @@
 // Sparse x dense SpMM kernels: C = alpha*A*B + beta*C with row-major dense
 // B (ldb) and C (ldc), k right-hand sides.
 //
-// CSR: a group of L lanes per row of A, each lane owning VEC consecutive
-// columns of C per k-tile (128-bit loads of B and C rows). For every nonzero
-// a_ij of the row the group reads row j of B, which for the structured
-// matrices of this path (stencils, banded) was read moments earlier by a
-// neighbouring row and is served from L2; the unique rows of B are counted
-// once in the algorithmic bytes. The per-element sum runs over the row's
-// nonzeros in stored order, the order of the reference's row kernel
-// (src/compressed_sparse_rows.cpp:1699-1745).
+// CSR: the row-group loop of spmm_rows.cuh, one group of TK x TN lanes per
+// row of A (TK over C's columns with 16-byte vectors when aligned, TN over
+// the row's nonzeros, four nonzeros in flight per lane). For the structured
+// matrices of this path (stencils, banded) row j of B was read moments
+// earlier by a neighbouring row and is served from L1 / L2; the unique rows
+// of B are counted once in the algorithmic bytes.
 //
 // BSR: a warp per block row, lanes over C's columns; each lane keeps bs
 // accumulators (one per scalar row of the block row).
 #include "common.cuh"
 #include "pls_internal.hpp"
+#include "spmm_rows.cuh"
 
 namespace pls {
 
-template <class X, int VEC> struct VecT;
-template <> struct VecT<double, 1> { using T = double; };
-template <> struct VecT<double, 2> { using T = double2; };
-template <> struct VecT<float, 1> { using T = float; };
-template <> struct VecT<float, 2> { using T = float2; };
-template <> struct VecT<float, 4> { using T = float4; };
-
-template <class X, int VEC>
-__device__ __forceinline__ void ld_vec(const X *p, X (&v)[VEC]) {
-  if constexpr (VEC == 1) {
-    v[0] = __ldg(p);
-  } else {
-    using T = typename VecT<X, VEC>::T;
-    const T t = __ldg(reinterpret_cast<const T *>(p));
-    const X *e = reinterpret_cast<const X *>(&t);
-#pragma unroll
-    for (int i = 0; i < VEC; ++i)
-      v[i] = e[i];
-  }
-}
-
-template <class X, int VEC>
-__device__ __forceinline__ void ld_vec_plain(const X *p, X (&v)[VEC]) {
-  if constexpr (VEC == 1) {
-    v[0] = *p;
-  } else {
-    using T = typename VecT<X, VEC>::T;
-    const T t = *reinterpret_cast<const T *>(p);
-    const X *e = reinterpret_cast<const X *>(&t);
-#pragma unroll
-    for (int i = 0; i < VEC; ++i)
-      v[i] = e[i];
-  }
-}
-
-template <class X, int VEC>
-__device__ __forceinline__ void st_vec(X *p, const X (&v)[VEC]) {
-  if constexpr (VEC == 1) {
-    *p = v[0];
-  } else {
-    using T = typename VecT<X, VEC>::T;
-    T t;
-    X *e = reinterpret_cast<X *>(&t);
-#pragma unroll
-    for (int i = 0; i < VEC; ++i)
-      e[i] = v[i];
-    *reinterpret_cast<T *>(p) = t;
-  }
-}
-
-// L lanes per row, VEC columns per lane per tile; `vec_ok` says whether the
-// full-width vector path is aligned for this call (else VEC must be 1).
-template <int L, int VEC, class V, class X>
+template <int VEC, int NV, class V, class X>
 __global__ void __launch_bounds__(256)
-    k_spmm_csr(int32_t m, const int32_t *__restrict__ rp,
+    k_spmm_csr(int32_t m, int lg_tk, int lg_tn, const int32_t *__restrict__ rp,
                const int32_t *__restrict__ col, const V *__restrict__ val,
-               const X *__restrict__ B, int64_t ldb, X *__restrict__ C,
-               int64_t ldc, int k, X alpha, X beta, int beta_nz) {
+               const X *__restrict__ B, int64_t ldb, X *__restrict__ C, int64_t ldc, int k,
+               X alpha, X beta, int beta_nz) {
   using Acc = typename AccOf<V, X>::type;
-  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t row = gid / L;
-  if (row >= m)
-    return;
-  const int lane = (int)(gid % L);
-  const int32_t s = __ldg(rp + row), e = __ldg(rp + row + 1);
-  X *crow = C + row * ldc;
-  for (int k0 = lane * VEC; k0 < k; k0 += L * VEC) {
-    const bool full = k0 + VEC <= k;
-    Acc acc[VEC];
-#pragma unroll
-    for (int v = 0; v < VEC; ++v)
-      acc[v] = 0;
-    int32_t p = s;
-    for (; p + 1 < e; p += 2) {
-      const Acc a0 = to_acc<Acc>(ld_stream(val + p)), a1 = to_acc<Acc>(ld_stream(val + p + 1));
-      const int32_t c0 = ld_stream(col + p), c1 = ld_stream(col + p + 1);
-      X b0[VEC], b1[VEC];
-      if (full) {
-        ld_vec<X, VEC>(B + (int64_t)c0 * ldb + k0, b0);
-        ld_vec<X, VEC>(B + (int64_t)c1 * ldb + k0, b1);
-      } else {
-#pragma unroll
-        for (int v = 0; v < VEC; ++v) {
-          b0[v] = k0 + v < k ? __ldg(B + (int64_t)c0 * ldb + k0 + v) : X(0);
-          b1[v] = k0 + v < k ? __ldg(B + (int64_t)c1 * ldb + k0 + v) : X(0);
-        }
-      }
-#pragma unroll
-      for (int v = 0; v < VEC; ++v) {
-        acc[v] = fma(a0, to_acc<Acc>(b0[v]), acc[v]);
-        acc[v] = fma(a1, to_acc<Acc>(b1[v]), acc[v]);
-      }
-    }
-    if (p < e) {
-      const Acc a0 = to_acc<Acc>(ld_stream(val + p));
-      const int32_t c0 = ld_stream(col + p);
-      X b0[VEC];
-      if (full) {
-        ld_vec<X, VEC>(B + (int64_t)c0 * ldb + k0, b0);
-      } else {
-#pragma unroll
-        for (int v = 0; v < VEC; ++v)
-          b0[v] = k0 + v < k ? __ldg(B + (int64_t)c0 * ldb + k0 + v) : X(0);
-      }
-#pragma unroll
-      for (int v = 0; v < VEC; ++v)
-        acc[v] = fma(a0, to_acc<Acc>(b0[v]), acc[v]);
-    }
-    X out[VEC];
-    if (beta_nz) {
-      X cold[VEC];
-      if (full) {
-        ld_vec_plain<X, VEC>(crow + k0, cold);
-      } else {
-#pragma unroll
-        for (int v = 0; v < VEC; ++v)
-          cold[v] = k0 + v < k ? crow[k0 + v] : X(0);
-      }
-#pragma unroll
-      for (int v = 0; v < VEC; ++v)
-        out[v] = (X)acc[v] * alpha + beta * cold[v];
-    } else {
-#pragma unroll
-      for (int v = 0; v < VEC; ++v)
-        out[v] = (X)acc[v] * alpha;
-    }
-    if (full) {
-      st_vec<X, VEC>(crow + k0, out);
-    } else {
-#pragma unroll
-      for (int v = 0; v < VEC; ++v)
-        if (k0 + v < k)
-          crow[k0 + v] = out[v];
-    }
-  }
-}
-
-template <int L, int VEC, class V, class X>
-static void launch_spmm_csr(const CsrDev &c, int32_t m, const X *B, int64_t ldb,
-                            X *C, int64_t ldc, int k, X alpha, X beta,
-                            cudaStream_t s) {
-  const int64_t blocks = div_up((int64_t)m * L, 256);
-  k_spmm_csr<L, VEC, V, X><<<(unsigned)blocks, 256, 0, s>>>(
-      m, c.row_ptr.as<int32_t>(), c.col.as<int32_t>(), (const V *)c.ev(), B, ldb, C,
-      ldc, k, alpha, beta, beta != X(0));
+  const L2Policy pol = make_l2_policy();
+  const int lg_g = lg_tk + lg_tn;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t row = (warp << (5 - lg_g)) + ((threadIdx.x & 31) >> lg_g);
+  const CsrRows<V> A{rp, col, val};
+  spmm_row_group<VEC, NV, Acc, X>(A, row, row < m, lg_tk, lg_tn, B, ldb, C, ldc, k, alpha, beta,
+                                  beta_nz, pol);
 }
 
 template <int VEC, class V, class X>
-static void spmm_csr_lanes(const CsrDev &c, int32_t m, const X *B, int64_t ldb,
-                           X *C, int64_t ldc, int k, X alpha, X beta,
-                           cudaStream_t s) {
-  const int groups = (int)div_up(k, VEC);
-  if (groups <= 1)
-    launch_spmm_csr<1, VEC, V, X>(c, m, B, ldb, C, ldc, k, alpha, beta, s);
-  else if (groups <= 2)
-    launch_spmm_csr<2, VEC, V, X>(c, m, B, ldb, C, ldc, k, alpha, beta, s);
-  else if (groups <= 4)
-    launch_spmm_csr<4, VEC, V, X>(c, m, B, ldb, C, ldc, k, alpha, beta, s);
-  else if (groups <= 8)
-    launch_spmm_csr<8, VEC, V, X>(c, m, B, ldb, C, ldc, k, alpha, beta, s);
-  else if (groups <= 16)
-    launch_spmm_csr<16, VEC, V, X>(c, m, B, ldb, C, ldc, k, alpha, beta, s);
+static void launch_spmm_csr(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
+                            int64_t ldc, int k, X alpha, X beta, cudaStream_t s) {
+  const RowsShape sh = rows_shape(k, VEC, (double)c.nnz / std::max<int32_t>(m, 1));
+  const int64_t rows_per_block = (int64_t)8 << (5 - (sh.lg_tk + sh.lg_tn));
+  const unsigned blocks = (unsigned)div_up(m, rows_per_block);
+  const int bnz = beta != X(0);
+  if (sh.nv == 2)
+    k_spmm_csr<VEC, 2, V, X><<<blocks, 256, 0, s>>>(m, sh.lg_tk, sh.lg_tn, c.row_ptr.as<int32_t>(),
+        c.col.as<int32_t>(), (const V *)c.ev(), B, ldb, C, ldc, k, alpha, beta, bnz);
   else
-    launch_spmm_csr<32, VEC, V, X>(c, m, B, ldb, C, ldc, k, alpha, beta, s);
+    k_spmm_csr<VEC, 1, V, X><<<blocks, 256, 0, s>>>(m, sh.lg_tk, sh.lg_tn, c.row_ptr.as<int32_t>(),
+        c.col.as<int32_t>(), (const V *)c.ev(), B, ldb, C, ldc, k, alpha, beta, bnz);
 }
 
+// Row-group SpMM (the launch half of spmm_csr).
 template <class X>
-void spmm_csr(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
+static void spmm_rows(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64_t ldc,
+                      int k, X alpha, X beta, cudaStream_t s);
+
+// The first SpMM of a call signature on a matrix the staged kernel applies
+// to runs both kernels on a scratch C (beta = 0, CUDA events, one warm-up
+// and two timed runs each) and keeps the faster; later calls with that
+// signature use the kept choice. Matrices it does not apply to (B rows not
+// reused inside row blocks, B not 16-byte aligned) always take the
+// row-group kernel.
+template <class X>
+void spmm_csr(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
               int64_t ldc, int k, X alpha, X beta, cudaStream_t s) {
   if (m == 0 || k == 0)
     return;
+  const int64_t sig = ((int64_t)k << 32) ^ (ldb << 8) ^ ((int64_t)sizeof(X) << 4) ^
+                      (int64_t)c.evt();
+  TileDev &t = c.tiles;
+  if (t.forced == 0) {
+    spmm_rows<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s);
+    t.last_path = 0;
+    return;
+  }
+  if (t.forced == 1) {
+    const bool staged = spmm_tiled<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s, true);
+    if (!staged)
+      spmm_rows<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s);
+    t.last_path = staged ? 1 : 0;
+    return;
+  }
+  if (t.choice_sig != sig) {
+    t.choice = 0;
+    if (spmm_tiled<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s, false)) {
+      DevBuf scratch;
+      scratch.reserve(sizeof(X) * (size_t)m * k);
+      X *sc = scratch.as<X>();
+      cudaEvent_t e0, e1;
+      PLS_CUDA(cudaEventCreate(&e0));
+      PLS_CUDA(cudaEventCreate(&e1));
+      auto time2 = [&](auto &&run) {
+        run();
+        PLS_CUDA(cudaEventRecord(e0, s));
+        run();
+        run();
+        PLS_CUDA(cudaEventRecord(e1, s));
+        PLS_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        PLS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        return ms / 2;
+      };
+      t.ms_rows = time2([&] { spmm_rows<X>(c, m, B, ldb, sc, (int64_t)k, k, X(1), X(0), s); });
+      t.ms_staged =
+          time2([&] { spmm_tiled<X>(c, m, B, ldb, sc, (int64_t)k, k, X(1), X(0), s, true); });
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      t.choice = t.ms_staged < t.ms_rows ? 1 : 0;
+    }
+    t.choice_sig = sig;
+  }
+  if (t.choice == 1 && spmm_tiled<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s, true)) {
+    t.last_path = 1;
+    return;
+  }
+  spmm_rows<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s);
+  t.last_path = 0;
+}
+
+template <class X>
+static void spmm_rows(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64_t ldc,
+                      int k, X alpha, X beta, cudaStream_t s) {
   constexpr int VMAX = 16 / sizeof(X);
-  const bool aligned = ((uintptr_t)B % 16 == 0) && ((uintptr_t)C % 16 == 0) &&
+  const bool aligned = k >= VMAX && ((uintptr_t)B % 16 == 0) && ((uintptr_t)C % 16 == 0) &&
                        (ldb % VMAX == 0) && (ldc % VMAX == 0);
   with_vt(c.evt(), [&](auto tag) {
     using V = typename decltype(tag)::type;
@@ -197,9 +127,9 @@ void spmm_csr(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
       throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE, "FP64 storage with FP32 API");
     } else {
       if (aligned)
-        spmm_csr_lanes<VMAX, V, X>(c, m, B, ldb, C, ldc, k, alpha, beta, s);
+        launch_spmm_csr<VMAX, V, X>(c, m, B, ldb, C, ldc, k, alpha, beta, s);
       else
-        spmm_csr_lanes<1, V, X>(c, m, B, ldb, C, ldc, k, alpha, beta, s);
+        launch_spmm_csr<1, V, X>(c, m, B, ldb, C, ldc, k, alpha, beta, s);
     }
   });
   PLS_LAUNCH_CHECK();
@@ -323,9 +253,9 @@ void spmm_bsr(const BsrDev &b, const X *B, int64_t ldb, X *C, int64_t ldc,
   PLS_LAUNCH_CHECK();
 }
 
-template void spmm_csr<float>(const CsrDev &, int32_t, const float *, int64_t,
+template void spmm_csr<float>(CsrDev &, int32_t, const float *, int64_t,
                               float *, int64_t, int, float, float, cudaStream_t);
-template void spmm_csr<double>(const CsrDev &, int32_t, const double *, int64_t,
+template void spmm_csr<double>(CsrDev &, int32_t, const double *, int64_t,
                                double *, int64_t, int, double, double,
                                cudaStream_t);
 template void spmm_bsr<float>(const BsrDev &, const float *, int64_t, float *,

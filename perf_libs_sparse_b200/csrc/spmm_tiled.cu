@@ -1,0 +1,615 @@
+// Tiled CSR SpMM: the rows of B that a block of R consecutive rows of A
+// needs are copied once into shared memory by the bulk-copy (TMA) engine,
+// and every product reads B from there.
+//
+// For stencil and banded matrices consecutive rows of A touch the same rows
+// of B (a 27-point stencil row reads 27 rows of B, but a block of R rows
+// reads only about 9 (R + 2) distinct ones), so staging the block's distinct
+// B rows once cuts the L2 -> SM traffic for B about threefold, replaces the
+// per-product gathers with a few large asynchronous copies, and lets the
+// column index shrink to a 16-bit index into the staged tile.
+//
+// Preprocessing (once per matrix and block height, optimize / first call):
+//   for every block of R rows, the distinct columns of its nonzeros in
+//   ascending order, grouped into runs of consecutive columns
+//   (c0, len, u0: the run's first column, length and first tile row), and
+//   for every nonzero its tile row `local` (uint16). Both come from a CUB
+//   block radix sort of the block's (column, position) keys in shared
+//   memory, one CTA per block; blocks with more than kTileCap nonzeros make
+//   the matrix unsuitable (it then keeps the row-group kernel).
+//
+// Kernel: persistent, one 512-thread CTA per SM, walking the items (row
+// block, column tile of KT columns) in order with two stage buffers in
+// shared memory. For each item, warp 0 posts the item's byte count on the
+// buffer's mbarrier and issues cp.async.bulk copies of:
+//   * the block's B rows, one copy per run (whole rows when the tile spans
+//     all k columns and B is packed, else one per B row segment);
+//   * the 16-byte aligned interior of the block's values and tile rows
+//     (the few unaligned elements at either end are copied by the lanes,
+//     as are the block's row pointers).
+// While the copies of item i + 1 land in one buffer, the CTA computes item
+// i from the other, reading only shared memory. Thread 0 waits on the
+// barrier with an iteration limit; on expiry the CTA records the failure in
+// a mapped host flag, waits again with a limit for its own copies and stops
+// (the host reports it on the next call). Lanes over the tile's columns
+// (VEC-wide shared loads) and warps over the block's rows accumulate
+// sum_p val[p] * tile[local[p]][:] in stored order per element, the order
+// of the reference's row kernel (src/compressed_sparse_rows.cpp:1699-1745),
+// and write C.
+//
+// Whether this kernel or the row-group one runs is measured (spmm.cu).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "pls_internal.hpp"
+#include "spmm_rows.cuh"
+
+namespace pls {
+
+namespace {
+
+constexpr int kTileThreads = 256;
+constexpr int kTileItems = 16;
+constexpr int kTileCap = kTileThreads * kTileItems;  // nonzeros per block
+
+using TileSort = cub::BlockRadixSort<unsigned long long, kTileThreads, kTileItems>;
+using TileScan = cub::BlockScan<int, kTileThreads>;
+
+// Sort the block's (column << 16 | position) keys; returns the nonzero count
+// (or -1 when above kTileCap). keys[i] is the i-th key of this thread's
+// blocked arrangement (thread t holds sorted ranks t*kTileItems + i).
+__device__ int tile_sorted_keys(int32_t m, int R, const int32_t *__restrict__ rp,
+                                const int32_t *__restrict__ col,
+                                typename TileSort::TempStorage &ts,
+                                unsigned long long (&keys)[kTileItems]) {
+  const int64_t r0 = (int64_t)blockIdx.x * R;
+  const int64_t r1 = r0 + R < (int64_t)m ? r0 + R : (int64_t)m;
+  const int32_t p0 = rp[r0], p1 = rp[r1];
+  const int cnt = p1 - p0;
+  if (cnt > kTileCap)
+    return -1;
+#pragma unroll
+  for (int i = 0; i < kTileItems; ++i) {
+    const int q = threadIdx.x * kTileItems + i;
+    keys[i] = q < cnt ? ((unsigned long long)(uint32_t)col[p0 + q] << 16) | (unsigned long long)q
+                      : ~0ull;
+  }
+  TileSort(ts).Sort(keys);
+  return cnt;
+}
+
+union TilePrepStorage {
+  typename TileSort::TempStorage sort;
+  typename TileScan::TempStorage scan;
+};
+
+// Pass 1: distinct columns and runs per block (-1 when over the cap).
+__global__ void __launch_bounds__(kTileThreads)
+    k_tile_count(int32_t m, int R, const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+                 int32_t *__restrict__ nuniq, int32_t *__restrict__ nruns,
+                 int32_t *__restrict__ bnnz) {
+  __shared__ TilePrepStorage st;
+  __shared__ unsigned long long edge[kTileThreads];  // last key of each thread
+  unsigned long long keys[kTileItems];
+  const int cnt = tile_sorted_keys(m, R, rp, col, st.sort, keys);
+  if (threadIdx.x == 0)
+    bnnz[blockIdx.x] = cnt;
+  if (cnt < 0) {
+    if (threadIdx.x == 0) {
+      nuniq[blockIdx.x] = -1;
+      nruns[blockIdx.x] = 0;
+    }
+    return;
+  }
+  edge[threadIdx.x] = keys[kTileItems - 1];
+  __syncthreads();
+  unsigned long long prev = threadIdx.x ? edge[threadIdx.x - 1] : ~0ull;
+  int u = 0, r = 0;
+#pragma unroll
+  for (int i = 0; i < kTileItems; ++i) {
+    const int q = threadIdx.x * kTileItems + i;
+    if (q < cnt) {
+      const uint32_t c = (uint32_t)(keys[i] >> 16);
+      const bool first = q == 0;
+      const uint32_t pc = (uint32_t)(prev >> 16);
+      const bool is_new = first || c != pc;
+      u += is_new;
+      r += is_new && (first || c != pc + 1);
+    }
+    prev = keys[i];
+  }
+  __syncthreads();
+  int tu = 0, tr = 0, dummy = 0;
+  TileScan(st.scan).ExclusiveSum(u, dummy, tu);
+  __syncthreads();
+  TileScan(st.scan).ExclusiveSum(r, dummy, tr);
+  if (threadIdx.x == 0) {
+    nuniq[blockIdx.x] = tu;
+    nruns[blockIdx.x] = tr;
+  }
+}
+
+// Pass 2: runs (c0, len, u0) at run_ptr[block] and the tile row of every
+// nonzero.
+__global__ void __launch_bounds__(kTileThreads)
+    k_tile_fill(int32_t m, int R, const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+                const int32_t *__restrict__ run_ptr, const int32_t *__restrict__ nuniq,
+                int4 *__restrict__ runs, uint16_t *__restrict__ local) {
+  __shared__ TilePrepStorage st;
+  __shared__ unsigned long long edge[kTileThreads];
+  unsigned long long keys[kTileItems];
+  const int cnt = tile_sorted_keys(m, R, rp, col, st.sort, keys);
+  if (cnt < 0)
+    return;
+  const int32_t p0 = rp[(int64_t)blockIdx.x * R];
+  edge[threadIdx.x] = keys[kTileItems - 1];
+  __syncthreads();
+  unsigned long long prev = threadIdx.x ? edge[threadIdx.x - 1] : ~0ull;
+  int fu[kTileItems], fr[kTileItems];
+  int u = 0, r = 0;
+#pragma unroll
+  for (int i = 0; i < kTileItems; ++i) {
+    const int q = threadIdx.x * kTileItems + i;
+    fu[i] = fr[i] = 0;
+    if (q < cnt) {
+      const uint32_t c = (uint32_t)(keys[i] >> 16);
+      const uint32_t pc = (uint32_t)(prev >> 16);
+      const bool first = q == 0;
+      fu[i] = first || c != pc;
+      fr[i] = fu[i] && (first || c != pc + 1);
+    }
+    u += fu[i];
+    r += fr[i];
+    prev = keys[i];
+  }
+  __syncthreads();
+  int ub = 0, rb = 0;
+  TileScan(st.scan).ExclusiveSum(u, ub);
+  __syncthreads();
+  TileScan(st.scan).ExclusiveSum(r, rb);
+  const int32_t base = run_ptr[blockIdx.x];
+  const int32_t nu = nuniq[blockIdx.x];
+  const int32_t nr = run_ptr[blockIdx.x + 1] - base;
+  // run starts: (c0, -, u0); lengths follow from the next run's u0
+#pragma unroll
+  for (int i = 0; i < kTileItems; ++i) {
+    const int q = threadIdx.x * kTileItems + i;
+    ub += fu[i];
+    rb += fr[i];
+    if (q < cnt) {
+      const int uidx = ub - 1;  // tile row of this key's column
+      local[p0 + (int)(keys[i] & 0xffffull)] = (uint16_t)uidx;
+      if (fr[i])
+        runs[base + rb - 1] = make_int4((int)(keys[i] >> 16), 0, uidx, 0);
+    }
+  }
+  __syncthreads();
+  __threadfence_block();
+  for (int j = threadIdx.x; j < nr; j += blockDim.x) {
+    const int next_u0 = j + 1 < nr ? runs[base + j + 1].z : nu;
+    runs[base + j].y = next_u0 - runs[base + j].z;
+  }
+}
+
+// ---- the SpMM kernel ----------------------------------------------------
+
+constexpr int kStageThreads = 512;
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,
+                                         uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool bar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for the phase with `parity`: polls back to back first (the
+// copies usually land within a few microseconds), then with short sleeps;
+// gives up after about a second.
+__device__ __forceinline__ bool bar_wait_bounded(uint64_t *bar, uint32_t parity) {
+  for (int it = 0; it < (1 << 22); ++it) {
+    if (bar_try_wait(bar, parity))
+      return true;
+    if (it >= 1024)
+      __nanosleep(256);
+  }
+  return false;
+}
+
+// Byte layout of one stage buffer (all offsets multiples of 16): the B tile,
+// the block's values and tile rows (each placed at its global address's
+// offset within 16 bytes, so that the 16-byte aligned interior can be bulk
+// copied), and the block's row pointers.
+struct StageLayout {
+  uint32_t tile, vals, local, rp, bytes;
+};
+
+__host__ __device__ inline uint32_t up16(uint32_t x) { return (x + 15u) & ~15u; }
+
+// Interior [a0, a1) (bytes, 16-aligned) of elements [p0, p1) of size es.
+__device__ __forceinline__ void interior(int64_t p0, int64_t p1, int es, int64_t &a0,
+                                         int64_t &a1) {
+  a0 = (p0 * es + 15) & ~int64_t(15);
+  a1 = (p1 * es) & ~int64_t(15);
+  if (a1 <= a0)
+    a0 = a1 = 0;
+}
+
+// Copy elements [p0, p1) of `src` (element size es) into `dst`, element p at
+// byte (p * es) - floor16(p0 * es), i.e. at index p - p0 from
+// dst + (p0 * es) % 16: the aligned interior by one bulk copy (issued by
+// lane 0), the rest by the warp's lanes with plain loads.
+template <class T>
+__device__ __forceinline__ void stage_range(int lane, unsigned char *dst, const T *src, int64_t p0,
+                                            int64_t p1, uint64_t *bar) {
+  constexpr int es = sizeof(T);
+  int64_t a0, a1;
+  interior(p0, p1, es, a0, a1);
+  const int64_t base = (p0 * es) & ~int64_t(15);
+  if (lane == 0 && a1 > a0)
+    bulk_g2s(dst + (a0 - base), reinterpret_cast<const unsigned char *>(src) + a0,
+             (uint32_t)(a1 - a0), bar);
+  T *d = reinterpret_cast<T *>(dst + (p0 * es - base));  // d[p - p0]
+  const int64_t i0 = a1 > a0 ? a0 / es : p1;  // first interior element
+  const int64_t i1 = a1 > a0 ? a1 / es : p1;  // first element after it
+  for (int64_t p = p0 + lane; p < i0; p += 32)
+    d[p - p0] = src[p];
+  for (int64_t p = i1 + lane; p < p1; p += 32)
+    d[p - p0] = src[p];
+}
+
+// Warp 0: post the byte count of item (blk, k0) on `bar` and issue its
+// copies into the stage buffer `sb`.
+template <class V, class X>
+__device__ __forceinline__ void stage_item(int lane, unsigned char *sb, const StageLayout &L,
+                                           uint64_t *bar, int32_t m, int R, int64_t blk, int k0,
+                                           int kw, int stride, int whole_rows, int k,
+                                           const int32_t *__restrict__ rp, const V *__restrict__ val,
+                                           const uint16_t *__restrict__ local,
+                                           const int32_t *__restrict__ run_ptr,
+                                           const int4 *__restrict__ runs,
+                                           const int32_t *__restrict__ nuniq,
+                                           const X *__restrict__ B, int64_t ldb) {
+  const int64_t r0 = blk * R;
+  const int64_t r1 = r0 + R < (int64_t)m ? r0 + R : (int64_t)m;
+  const int64_t p0 = rp[r0], p1 = rp[r1];
+  if (lane == 0) {
+    int64_t va0, va1, la0, la1;
+    interior(p0, p1, sizeof(V), va0, va1);
+    interior(p0, p1, 2, la0, la1);
+    const uint64_t tx = (uint64_t)nuniq[blk] * (uint64_t)kw * sizeof(X) + (uint64_t)(va1 - va0) +
+                        (uint64_t)(la1 - la0);
+    // the buffer's previous contents were read through the generic proxy
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"((uint32_t)tx)
+                 : "memory");
+  }
+  __syncwarp();
+  X *tile = reinterpret_cast<X *>(sb + L.tile);
+  const int32_t q0 = run_ptr[blk], q1 = run_ptr[blk + 1];
+  for (int32_t q = q0 + lane; q < q1; q += 32) {
+    const int4 run = runs[q];  // c0, len, u0
+    if (whole_rows) {
+      bulk_g2s(tile + (int64_t)run.z * stride, B + (int64_t)run.x * ldb,
+               (uint32_t)run.y * (uint32_t)k * (uint32_t)sizeof(X), bar);
+    } else {
+      for (int i = 0; i < run.y; ++i)
+        bulk_g2s(tile + (int64_t)(run.z + i) * stride, B + (int64_t)(run.x + i) * ldb + k0,
+                 (uint32_t)kw * (uint32_t)sizeof(X), bar);
+    }
+  }
+  stage_range<V>(lane, sb + L.vals, val, p0, p1, bar);
+  stage_range<uint16_t>(lane, sb + L.local, local, p0, p1, bar);
+  int32_t *srp = reinterpret_cast<int32_t *>(sb + L.rp);
+  for (int64_t i = lane; i <= r1 - r0; i += 32)
+    srp[i] = rp[r0 + i];
+}
+
+// Persistent: one CTA per SM walks the items (row block, column tile) in
+// order item = tile * nblocks + block, two stage buffers in flight: while it
+// computes item i from one buffer, the copies of item i + 1 land in the
+// other. The inner loop reads only shared memory.
+template <int VEC, class V, class X>
+__global__ void __launch_bounds__(kStageThreads, 1)
+    k_spmm_tiled(int32_t m, int R, int64_t nblocks, int ktiles, const int32_t *__restrict__ rp,
+                 const V *__restrict__ val, const uint16_t *__restrict__ local,
+                 const int32_t *__restrict__ run_ptr, const int4 *__restrict__ runs,
+                 const int32_t *__restrict__ nuniq, const X *__restrict__ B, int64_t ldb,
+                 X *__restrict__ C, int64_t ldc, int k, int KT, int whole_rows, StageLayout L,
+                 X alpha, X beta, int beta_nz, int *__restrict__ err) {
+  using Acc = typename AccOf<V, X>::type;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bars[2];
+  __shared__ int ok_s;
+  const int64_t n_items = nblocks * ktiles;
+  if ((int64_t)blockIdx.x >= n_items)
+    return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int stride = whole_rows ? k : KT;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bars[0])) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bars[1])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  unsigned char *sbuf[2] = {smem_raw, smem_raw + L.bytes};
+  auto issue = [&](int64_t it, int b) {
+    const int64_t blk = it % nblocks;
+    const int k0 = (int)(it / nblocks) * KT;
+    const int kw = min(KT, k - k0);
+    stage_item<V, X>(lane, sbuf[b], L, &bars[b], m, R, blk, k0, kw, stride, whole_rows, k, rp, val,
+                     local, run_ptr, runs, nuniq, B, ldb);
+  };
+  if (warp == 0)
+    issue(blockIdx.x, 0);
+
+  // Lanes over the tile's columns (VEC each; the power of two covering the
+  // tile, at most 32 since KT <= 32 * VEC), several rows per warp.
+  int lanes = 1;
+  while (lanes < 32 && lanes * VEC < KT)
+    lanes <<= 1;
+  const int rows_per_warp = 32 / lanes;
+  const int sub = lane % lanes;
+  const int c = sub * VEC;
+
+  uint32_t phase[2] = {0u, 0u};
+  int b = 0;
+  for (int64_t it = blockIdx.x; it < n_items; it += gridDim.x) {
+    if (threadIdx.x == 0)
+      ok_s = bar_wait_bounded(&bars[b], phase[b]);
+    __syncthreads();
+    if (!ok_s) {
+      // The copies did not land in time: record it, give the copies in
+      // flight another bounded wait (the CTA's shared memory must outlive
+      // them) and stop; the rest of C is left untouched.
+      if (threadIdx.x == 0) {
+        *(volatile int *)err = 1;
+        __threadfence_system();
+        bar_wait_bounded(&bars[b], phase[b]);
+      }
+      __syncthreads();
+      return;
+    }
+    phase[b] ^= 1u;
+    const int64_t next = it + gridDim.x;
+    if (warp == 0 && next < n_items)
+      issue(next, b ^ 1);
+
+    const int64_t blk = it % nblocks;
+    const int k0 = (int)(it / nblocks) * KT;
+    const int kw = min(KT, k - k0);
+    const bool col_ok = c < kw;
+    const unsigned char *sb = sbuf[b];
+    const X *tile = reinterpret_cast<const X *>(sb + L.tile);
+    const int32_t *srp = reinterpret_cast<const int32_t *>(sb + L.rp);
+    const int64_t r0 = blk * R;
+    const int rows_here = (int)(m - r0 < (int64_t)R ? m - r0 : (int64_t)R);
+    const int32_t p0 = srp[0];
+    // element p of the block at index p - p0 (see stage_range)
+    const V *sv = reinterpret_cast<const V *>(sb + L.vals + (((int64_t)p0 * sizeof(V)) & 15));
+    const uint16_t *sl = reinterpret_cast<const uint16_t *>(sb + L.local + (((int64_t)p0 * 2) & 15));
+    for (int rr = warp * rows_per_warp + lane / lanes; rr < rows_here;
+         rr += (kStageThreads / 32) * rows_per_warp) {
+      const int32_t s = srp[rr], e = srp[rr + 1];
+      Acc acc[VEC];
+#pragma unroll
+      for (int v = 0; v < VEC; ++v)
+        acc[v] = Acc(0);
+      if (col_ok) {
+        for (int32_t p = s - p0; p < e - p0; ++p) {
+          const Acc a = to_acc<Acc>(sv[p]);
+          const X *tp = tile + (int64_t)sl[p] * stride + c;
+          X bv[VEC];
+          if (c + VEC <= kw) {
+            ld_vec_plain<X, VEC>(tp, bv);
+          } else {
+#pragma unroll
+            for (int v = 0; v < VEC; ++v)
+              bv[v] = c + v < kw ? tp[v] : X(0);
+          }
+#pragma unroll
+          for (int v = 0; v < VEC; ++v)
+            acc[v] = fma(a, to_acc<Acc>(bv[v]), acc[v]);
+        }
+        X *cp = C + (r0 + rr) * ldc + k0 + c;
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) {
+          if (c + v < kw) {
+            X o = (X)acc[v] * alpha;
+            if (beta_nz)
+              o += beta * cp[v];
+            cp[v] = o;
+          }
+        }
+      }
+    }
+    __syncthreads();  // every read of this buffer done before it is refilled
+    b ^= 1;
+  }
+}
+
+}  // namespace
+
+// ---- host side --------------------------------------------------------------
+
+namespace {
+
+// Pass 1 for block height R: per-block distinct-column counts (device, kept
+// in t.nuniq), run counts and nonzero counts (host). False when some block
+// is over the cap or has more than 65535 distinct columns.
+bool tile_counts(const CsrDev &c, int32_t m, int R, TileDev &t, std::vector<int32_t> &runs_per,
+                 cudaStream_t s) {
+  const int64_t nb = div_up(m, R);
+  std::vector<int32_t> hu(nb), hn(nb);
+  runs_per.assign(nb, 0);
+  DevBuf nruns, bnnz;
+  t.nuniq.reserve(sizeof(int32_t) * nb);
+  nruns.reserve(sizeof(int32_t) * nb);
+  bnnz.reserve(sizeof(int32_t) * nb);
+  k_tile_count<<<(unsigned)nb, kTileThreads, 0, s>>>(m, R, c.row_ptr.as<int32_t>(),
+                                                     c.col.as<int32_t>(), t.nuniq.as<int32_t>(),
+                                                     nruns.as<int32_t>(), bnnz.as<int32_t>());
+  PLS_LAUNCH_CHECK();
+  PLS_CUDA(cudaMemcpyAsync(hu.data(), t.nuniq.p, sizeof(int32_t) * nb, cudaMemcpyDeviceToHost, s));
+  PLS_CUDA(cudaMemcpyAsync(runs_per.data(), nruns.p, sizeof(int32_t) * nb, cudaMemcpyDeviceToHost,
+                           s));
+  PLS_CUDA(cudaMemcpyAsync(hn.data(), bnnz.p, sizeof(int32_t) * nb, cudaMemcpyDeviceToHost, s));
+  PLS_CUDA(cudaStreamSynchronize(s));
+  t.R = R;
+  t.nblocks = nb;
+  t.max_uniq = 0;
+  t.max_bnnz = 0;
+  t.total_uniq = 0;
+  t.filled = false;
+  for (int64_t b = 0; b < nb; ++b) {
+    if (hu[b] < 0 || hu[b] > 65535 || hn[b] < 0)
+      return false;
+    t.max_uniq = std::max(t.max_uniq, hu[b]);
+    t.max_bnnz = std::max(t.max_bnnz, hn[b]);
+    t.total_uniq += hu[b];
+  }
+  return true;
+}
+
+// Pass 2: run table and per-nonzero tile rows for the counted R.
+void tile_fill(const CsrDev &c, int32_t m, TileDev &t, const std::vector<int32_t> &runs_per,
+               cudaStream_t s) {
+  const int64_t nb = t.nblocks;
+  std::vector<int32_t> ptr(nb + 1, 0);
+  for (int64_t b = 0; b < nb; ++b)
+    ptr[b + 1] = ptr[b] + runs_per[b];
+  t.n_runs = ptr[nb];
+  t.run_ptr.reserve(sizeof(int32_t) * (nb + 1));
+  PLS_CUDA(cudaMemcpyAsync(t.run_ptr.p, ptr.data(), sizeof(int32_t) * (nb + 1),
+                           cudaMemcpyHostToDevice, s));
+  t.runs.reserve(sizeof(int4) * std::max<int64_t>(t.n_runs, 1));
+  t.local.reserve(sizeof(uint16_t) * std::max<int64_t>(c.nnz, 1));
+  k_tile_fill<<<(unsigned)nb, kTileThreads, 0, s>>>(
+      m, t.R, c.row_ptr.as<int32_t>(), c.col.as<int32_t>(), t.run_ptr.as<int32_t>(),
+      t.nuniq.as<int32_t>(), t.runs.as<int4>(), t.local.as<uint16_t>());
+  PLS_LAUNCH_CHECK();
+  PLS_CUDA(cudaStreamSynchronize(s));
+  t.filled = true;
+}
+
+// One stage buffer for the counted tiles: B tile, values, tile rows, row
+// pointers (see StageLayout).
+StageLayout stage_layout(const TileDev &t, size_t row_bytes, size_t val_bytes) {
+  StageLayout L;
+  L.tile = 0;
+  L.vals = up16((uint32_t)((size_t)t.max_uniq * row_bytes));
+  L.local = L.vals + up16((uint32_t)((size_t)t.max_bnnz * val_bytes + 32));
+  L.rp = L.local + up16((uint32_t)((size_t)t.max_bnnz * 2 + 32));
+  L.bytes = (L.rp + up16((uint32_t)((t.R + 1) * sizeof(int32_t))) + 127u) & ~127u;
+  return L;
+}
+
+}  // namespace
+
+// Two stage buffers per CTA, each within kStageBudget, so one CTA per SM
+// holds both. The block height is the largest in {128, ..., 4} whose buffer
+// fits, and B rows must be reused at least 1.5x on average (nonzeros per
+// staged row) for the staging to pay; otherwise (power-law or random
+// matrices) the row-group kernel runs.
+constexpr size_t kStageBudget = 100 * 1024;
+
+void check_tile_error(const TileDev &t) {
+  if (t.err.host && *(volatile int *)t.err.host) {
+    *(volatile int *)t.err.host = 0;
+    throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE,
+                "tiled SpMM: a staged copy did not complete (reported by an earlier call)");
+  }
+}
+
+template <class X>
+bool spmm_tiled(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64_t ldc, int k,
+                X alpha, X beta, cudaStream_t s, bool launch) {
+  constexpr int VEC = 16 / sizeof(X);
+  if (m == 0 || k == 0 || c.nnz == 0)
+    return false;
+  // 16-byte bulk copies and vector reads of the staged rows
+  if ((uintptr_t)B % 16 || k % VEC || ldb % VEC)
+    return false;
+  const int KTMAX = 512 / (int)sizeof(X);
+  const bool single = k <= KTMAX;
+  const int KT = single ? k : KTMAX;
+  const bool whole_rows = single && ldb == k;
+  const size_t row_bytes = (size_t)KT * sizeof(X);
+  const size_t val_bytes = vt_size(c.evt());
+  TileDev &t = c.tiles;
+  check_tile_error(t);
+  if ((int64_t)row_bytes >= t.unsuitable_from)
+    return false;
+  if (!(t.filled && stage_layout(t, row_bytes, val_bytes).bytes <= kStageBudget)) {
+    std::vector<int32_t> runs_per;
+    bool found = false;
+    for (int R : {128, 64, 32, 16, 8, 4}) {
+      if (!tile_counts(c, m, R, t, runs_per, s))
+        continue;
+      if (stage_layout(t, row_bytes, val_bytes).bytes <= kStageBudget) {
+        found = true;
+        break;
+      }
+    }
+    if (!found || (double)c.nnz < 1.5 * (double)t.total_uniq) {
+      t.filled = false;
+      t.unsuitable_from = found ? 0 : std::min<int64_t>(t.unsuitable_from, (int64_t)row_bytes);
+      return false;
+    }
+    tile_fill(c, m, t, runs_per, s);
+  }
+  if (!launch)
+    return true;
+  if (!t.err.host)
+    t.err.alloc();
+  const StageLayout L = stage_layout(t, row_bytes, val_bytes);
+  const size_t smem = 2 * (size_t)L.bytes;
+  const int ktiles = (int)div_up(k, KT);
+  const int64_t n_items = t.nblocks * ktiles;
+  int dev = 0, sms = 0;
+  PLS_CUDA(cudaGetDevice(&dev));
+  PLS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const unsigned grid = (unsigned)std::min<int64_t>(n_items, sms);
+  const int bnz = beta != X(0);
+  with_vt(c.evt(), [&](auto tag) {
+    using V = typename decltype(tag)::type;
+    if constexpr (std::is_same_v<X, float> && std::is_same_v<V, double>) {
+      throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE, "FP64 storage with FP32 API");
+    } else {
+      auto kern = k_spmm_tiled<VEC, V, X>;
+      PLS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+      kern<<<grid, kStageThreads, smem, s>>>(
+          m, t.R, t.nblocks, ktiles, c.row_ptr.as<int32_t>(), (const V *)c.ev(),
+          t.local.as<uint16_t>(), t.run_ptr.as<int32_t>(), t.runs.as<int4>(),
+          t.nuniq.as<int32_t>(), B, ldb, C, ldc, k, KT, whole_rows ? 1 : 0, L, alpha, beta, bnz,
+          t.err.dev);
+    }
+  });
+  PLS_LAUNCH_CHECK();
+  return true;
+}
+
+template bool spmm_tiled<float>(CsrDev &, int32_t, const float *, int64_t, float *, int64_t, int,
+                                float, float, cudaStream_t, bool);
+template bool spmm_tiled<double>(CsrDev &, int32_t, const double *, int64_t, double *, int64_t,
+                                 int, double, double, cudaStream_t, bool);
+
+}  // namespace pls

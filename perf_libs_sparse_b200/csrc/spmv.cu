@@ -183,6 +183,11 @@ void spmv_csr_split(const CsrDev &c, int32_t m, const X *x, X *y, X alpha,
 // products are still added one by one in column order j = 0 .. len-1, the
 // order of the reference's spmv_scs<T,C> (src/sell_c_sigma.cpp:727-775).
 constexpr int kSellGroup = 8;
+// 128-thread blocks (10 per SM at 48 registers): on power-law layouts a
+// block waits for its slowest chunk, and smaller blocks waste less of the
+// SM on that wait than 256-thread ones (measured 1.4% on the C2 matrix,
+// 3.4% on a 16.7 M-row Laplacian).
+constexpr int kSellThreads = 128;
 
 template <int C, class V, class O, class X>
 __device__ __forceinline__ typename AccOf<V, X>::type sell_row_sum(const V *vp, const O *op,
@@ -222,12 +227,15 @@ __device__ __forceinline__ typename AccOf<V, X>::type sell_row_sum(const V *vp, 
 // (chunk, j0, j1, slot), partial sum to part[slot*C + r]. The remaining
 // blocks take one chunk per C lanes (lane r = row r of the chunk, so the C
 // lanes read C consecutive values per column: a full 256-byte line for
-// C = 32, FP64) and skip the chunks the slices cover. Slices come first so
-// the longest work starts earliest.
+// C = 32, FP64) and skip the chunks the slices cover; they take the chunks in
+// `order` (decreasing width, or natural order when null). Slices come first,
+// then the widest chunks, so the longest work starts earliest and the launch
+// ends on the narrowest chunks.
 template <int C, class V, class O, class X>
-__global__ void __launch_bounds__(256, 5)
+__global__ void __launch_bounds__(kSellThreads, 10)
     k_sell(int64_t nC, int32_t split_w, int64_t n_items, int64_t slice_blocks,
-           const int4 *__restrict__ items, const int64_t *__restrict__ cs,
+           const int4 *__restrict__ items, const int32_t *__restrict__ order,
+           const int64_t *__restrict__ cs,
            const int32_t *__restrict__ cl, const int32_t *__restrict__ cmin,
            const int32_t *__restrict__ perm, const V *__restrict__ vals,
            const O *__restrict__ offs, const X *__restrict__ x, X *__restrict__ y,
@@ -248,9 +256,10 @@ __global__ void __launch_bounds__(256, 5)
     return;
   }
   const int64_t t = (int64_t)(blockIdx.x - slice_blocks) * blockDim.x + threadIdx.x;
-  const int64_t c = t / C;
-  if (c >= nC)
+  const int64_t ci = t / C;
+  if (ci >= nC)
     return;
+  const int64_t c = order ? (int64_t)__ldg(order + ci) : ci;
   const int r = (int)(t % C);
   const int32_t w = __ldg(cl + c);
   if (w > split_w)
@@ -291,14 +300,15 @@ static void launch_sell(const SellDev &s, const X *x, X *y, X alpha, X beta,
   using Acc = typename AccOf<V, X>::type;
   const int bnz = beta != X(0);
   const bool sliced = s.n_items > 0 && s.n_split > 0;
-  const int64_t slice_blocks = sliced ? div_up(s.n_items * C, 256) : 0;
-  const int64_t chunk_blocks = div_up(s.nC * C, 256);
+  const int64_t slice_blocks = sliced ? div_up(s.n_items * C, kSellThreads) : 0;
+  const int64_t chunk_blocks = div_up(s.nC * C, kSellThreads);
   if (slice_blocks + chunk_blocks == 0)
     return;
   Acc *part = sliced ? (Acc *)s.part.p : nullptr;  // partial sums (scratch)
-  k_sell<C, V, O, X><<<(unsigned)(slice_blocks + chunk_blocks), 256, 0, st>>>(
+  k_sell<C, V, O, X><<<(unsigned)(slice_blocks + chunk_blocks), kSellThreads, 0, st>>>(
       s.nC, sliced ? s.split_w : INT32_MAX, sliced ? s.n_items : 0, slice_blocks,
-      s.items.as<int4>(), s.cs.as<int64_t>(), s.cl.as<int32_t>(), s.col_min.as<int32_t>(),
+      s.items.as<int4>(), s.order.as<int32_t>(), s.cs.as<int64_t>(), s.cl.as<int32_t>(),
+      s.col_min.as<int32_t>(),
       s.permd2in.as<int32_t>(), s.vals.as<V>(), s.offsets.as<O>(), x, y, part, alpha, beta, bnz);
   if (sliced) {
     const int64_t b2 = div_up(s.n_split * C, 256);
@@ -407,16 +417,19 @@ void spmv_sell_scratch(const SellDev &s, const X *x, X *y, X alpha, X beta, void
   view.items.p = s.items.p;
   view.split_chunks.p = s.split_chunks.p;
   view.part.p = scratch;
+  view.order.p = s.order.p;
   try {
     spmv_sell<X>(view, x, y, alpha, beta, st);
   } catch (...) {
     // `view` borrows every pointer: release nothing.
     view.cs.p = view.cl.p = view.col_min.p = view.permd2in.p = nullptr;
     view.vals.p = view.offsets.p = view.items.p = view.split_chunks.p = view.part.p = nullptr;
+    view.order.p = nullptr;
     throw;
   }
   view.cs.p = view.cl.p = view.col_min.p = view.permd2in.p = nullptr;
   view.vals.p = view.offsets.p = view.items.p = view.split_chunks.p = view.part.p = nullptr;
+  view.order.p = nullptr;
 }
 
 template void spmv_sell_scratch<double>(const SellDev &, const double *, double *, double,

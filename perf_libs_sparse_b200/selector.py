@@ -38,6 +38,9 @@ from . import (SpMat, _check, _p, lib, HINT_SPMV_INVOCATIONS, INVOCATIONS_MANY, 
 
 NF = 24
 NNZ_CAP = 24_000_000
+# Parameters of the selector trained on the generated corpus (written by
+# `main`, shipped with the package).
+SHIPPED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "selector_params.npy")
 FAMILIES = ("stencil", "banded", "powerlaw", "uniform", "blocks")
 SOFT_TAU = 0.05
 
@@ -264,6 +267,15 @@ def create_from_device(m, n, row_ptr, col, vals) -> SpMat:
                                                    C.c_void_p(col.data_ptr()), C.c_void_p(vals.data_ptr()),
                                                    None), "create_csr_d_dev")
     return SpMat(h, np.float64)
+
+
+def default_selector():
+    """The shipped trained selector, or None when the package has none."""
+    if not os.path.exists(SHIPPED):
+        return None
+    S = Selector(len(candidates()))
+    S.load(SHIPPED)
+    return S
 
 
 # ---------------------------------------------------------------- corpus

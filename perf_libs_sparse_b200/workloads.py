@@ -122,6 +122,20 @@ def stencil_27pt(g: int = 128, seed: int = 2):
     return n, n, row_ptr, cols[mask].astype(np.int32), vals[mask]
 
 
+def banded_csr(n: int, half_bandwidth: int, rng: np.random.Generator):
+    """Square matrix with the full band |i - j| <= half_bandwidth, values
+    U[-1, 1]: (m, n, row_ptr, col, vals), 0-based."""
+    rows = np.arange(n)
+    lo = np.maximum(rows - half_bandwidth, 0)
+    hi = np.minimum(rows + half_bandwidth, n - 1)
+    lens = hi - lo + 1
+    row_ptr = np.zeros(n + 1, np.int32)
+    row_ptr[1:] = np.cumsum(lens)
+    col = (np.repeat(lo, lens) + np.arange(row_ptr[-1]) - np.repeat(row_ptr[:-1], lens)).astype(np.int32)
+    vals = rng.uniform(-1, 1, int(row_ptr[-1]))
+    return n, n, row_ptr, col, vals
+
+
 def random_csr(m: int, n: int, max_len: int, rng: np.random.Generator, base: int = 0,
                empty_frac: float = 0.1, dtype=np.float64):
     """Small irregular CSR with some empty rows (for parity tests)."""

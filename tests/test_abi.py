@@ -79,3 +79,20 @@ def test_fails_loudly_without_gpu():
     with pytest.raises(pls.PerflibsError) as e:
         pls.SpMat.csr(1, 1, rp, c, v)
     assert e.value.status == pls.STATUS_EXECUTION_FAILURE
+
+
+def test_reference_driver_links_against_drop_in():
+    """The reference's own benchmark driver (bench/pl_bench_sparse_x_dense.c),
+    unchanged, compiles against include/perflibs_sparse.h with
+    -DUSE_PERFLIBS_NAMES and links to this library: every name it uses is
+    declared and exported. (Running it needs a GPU; the repository's own
+    driver with the same command line runs in the GPU tests.)"""
+    import subprocess
+
+    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run(["make", "-s", "-C", os.path.join(here, "oracle"), "driver-check"],
+                       capture_output=True, text=True)
+    if r.returncode != 0 and "Error 77" in r.stderr:
+        pytest.skip("reference sources not present")
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert os.path.exists(os.path.join(here, "oracle", "_build", "ref_driver_on_b200"))

@@ -98,3 +98,62 @@ def test_norms():
     assert np.isnan(B.norm(pls.NORM_INF))
     D = pls.SpMat.dense(pls.COL_MAJOR, 2, 2, 2, np.array([1.0, -3.0, 2.0, 4.0]))
     assert D.norm(pls.NORM_INF) == 7.0
+
+
+def test_coo_input_matches_oracle():
+    """COO creation (device radix sort by (row, column), duplicates kept in
+    input order) gives exactly the oracle's CSR; SpMV on it matches."""
+    rng = np.random.default_rng(21)
+    for m, n, nnz in [(1, 1, 0), (7, 5, 30), (500, 300, 4000), (3000, 2000, 60000)]:
+        r = rng.integers(0, m, nnz).astype(np.int32)
+        c = rng.integers(0, n, nnz).astype(np.int32)
+        v = rng.normal(size=nnz)
+        A = pls.SpMat.coo(m, n, r, c, v)
+        mm, nn, rp, cc, vv = A.export_csr()
+        assert (mm, nn) == (m, n)
+        o_rp, o_c, o_v = oracle.coo2csr(m, n, r, c, v)
+        np.testing.assert_array_equal(rp, o_rp)
+        np.testing.assert_array_equal(cc, o_c)
+        np.testing.assert_array_equal(vv, o_v)
+        x = rng.uniform(-1, 1, n)
+        y = A.spmv(x)
+        ref = oracle.csr_spmv(o_rp, o_c, o_v, x)
+        sc = oracle.csr_absdot(o_rp, o_c, o_v, x)
+        den = np.maximum(np.abs(ref), sc)
+        den[den == 0] = 1
+        assert (np.abs(y - ref) / den).max() <= 1e-12
+
+
+def test_csc_input_matches_oracle():
+    rng = np.random.default_rng(22)
+    for m, n, ml, base in [(40, 60, 5, 0), (800, 500, 20, 1)]:
+        rp, c, v = W.random_csr(n, m, ml, rng)  # CSR of A^T = CSC of A
+        A = pls.SpMat.csc(m, n, c + base, rp + base, v)
+        got = A.export_csr()[2:]
+        o_rp, o_c, o_v = oracle.csc2csr(m, n, c, rp, v)
+        for a, b in zip(got, (o_rp, o_c, o_v)):
+            np.testing.assert_array_equal(a, b)
+
+
+def test_bad_indices_rejected_before_any_kernel():
+    """Indices out of range are input errors (argument position as the
+    error code), checked on the device before any kernel indexes with them."""
+    rp = np.array([0, 2, 3], np.int32)
+    v = np.ones(3)
+    A = pls.SpMat.csr(2, 4, rp, np.array([0, 4, 1], np.int32), v, check=False)
+    assert A.status == pls.STATUS_INPUT_PARAMETER_ERROR and A.error_code() == 5
+    A = pls.SpMat.csr(2, 4, np.array([0, 3, 2], np.int32), np.array([0, 1, 1], np.int32), v,
+                      check=False)
+    assert A.status == pls.STATUS_INPUT_PARAMETER_ERROR and A.error_code() == 4
+    A = pls.SpMat.coo(3, 3, np.array([0, 3], np.int32), np.array([1, 1], np.int32), np.ones(2),
+                      check=False)
+    assert A.status == pls.STATUS_INPUT_PARAMETER_ERROR and A.error_code() == 5
+    A = pls.SpMat.coo(3, 3, np.array([0, 1], np.int32), np.array([-1, 1], np.int32), np.ones(2),
+                      check=False)
+    assert A.status == pls.STATUS_INPUT_PARAMETER_ERROR and A.error_code() == 6
+    A = pls.SpMat.csc(3, 2, np.array([0, 1], np.int32), np.array([2, 1, 2], np.int32),
+                      np.ones(2), check=False)
+    assert A.status == pls.STATUS_INPUT_PARAMETER_ERROR and A.error_code() == 4
+    A = pls.SpMat.csc(3, 2, np.array([0, 5], np.int32), np.array([0, 1, 2], np.int32),
+                      np.ones(2), check=False)
+    assert A.status == pls.STATUS_INPUT_PARAMETER_ERROR and A.error_code() == 4

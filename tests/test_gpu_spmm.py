@@ -72,7 +72,7 @@ def test_kat_matrix_kernel_ops(kats):
     np.testing.assert_allclose(Cm.export_dense(), Ad @ Bd, atol=k["tol"])
 
 
-@pytest.mark.parametrize("k", [1, 3, 5, 8, 13, 32, 128])
+@pytest.mark.parametrize("k", [1, 3, 5, 8, 13, 32, 128, 300])
 def test_random_spmm_vs_oracle(k):
     rng = np.random.default_rng(k)
     for m, n, ml, base in [(200, 150, 20, 0), (1500, 1000, 40, 1)]:
@@ -90,6 +90,25 @@ def test_random_spmm_vs_oracle(k):
             got = Cm.export_dense()
             ref = spmm_ref(rp0, c0, v, Bd, alpha, beta, C0 if beta else None)
             assert scaled_err(got, ref, rp0, c0, v, Bd, alpha, beta, C0) <= 1e-12, (m, k, alpha, beta)
+
+
+@pytest.mark.parametrize("k", [7, 64, 200])
+def test_random_spmm_fp32_vs_oracle(k):
+    """FP32 API: 16-byte vectors (k = 64, 200 with several column tiles) and
+    scalar columns (k = 7); FP32 accumulation, scaled error <= 1e-5."""
+    rng = np.random.default_rng(100 + k)
+    m, n = 900, 700
+    rp, c, v = W.random_csr(m, n, 50, rng)
+    Bd = rng.uniform(-1, 1, (n, k)).astype(np.float32)
+    C0 = rng.uniform(-1, 1, (m, k)).astype(np.float32)
+    A = pls.SpMat.csr(m, n, rp, c, v.astype(np.float32))
+    B = pls.SpMat.dense(pls.ROW_MAJOR, n, k, k, Bd.reshape(-1))
+    Cm = pls.SpMat.dense(pls.ROW_MAJOR, m, k, k, C0.reshape(-1))
+    assert pls.spmm_exec(pls.OPERATION_NOTRANS, pls.OPERATION_NOTRANS, 1.25, A, B, 0.5, Cm) == 0
+    got = Cm.export_dense().astype(np.float64)
+    v32 = v.astype(np.float32).astype(np.float64)
+    ref = spmm_ref(rp, c, v32, Bd.astype(np.float64), 1.25, 0.5, C0.astype(np.float64))
+    assert scaled_err(got, ref, rp, c, v32, Bd.astype(np.float64), 1.25, 0.5, C0.astype(np.float64)) <= 1e-5
 
 
 def test_repeated_exec_with_beta_zero_overwrites():
@@ -156,3 +175,79 @@ def test_device_pointer_spmm():
     A.spmm_dev(Bt.data_ptr(), 32, 32, Ct.data_ptr(), 32, 1.0, 0.0, torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()
     np.testing.assert_allclose(Ct.cpu().numpy(), spmm_ref(rp, c, v, Bd, 1.0, 0.0, None), rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+def test_staged_spmm_vs_oracle(dt):
+    """The staged (shared-memory tile) SpMM on a 27-point stencil and a
+    banded matrix: one column tile (k = 8, 32), several (k = 136 FP64 /
+    200 FP32: 512-byte tiles plus a partial one), beta != 0, and a strided
+    B (ldb > k: per-row copies). The tiled kernel must be the one that ran."""
+    import torch
+
+    rng = np.random.default_rng(7)
+    m, n, rp, c, v = W.stencil_27pt(20, seed=2)
+    band = W.banded_csr(5000, 9, rng)
+    tol = 1e-12 if dt == np.float64 else 1e-5
+    tdt = torch.float64 if dt == np.float64 else torch.float32
+    cases = [(m, n, rp, c, v), band]
+    ks = (8, 24, 32, 136) if dt == np.float64 else (8, 20, 32, 200)
+    for (mm, nn, rpp, cc, vv) in cases:
+        vv = vv.astype(dt)
+        A = pls.SpMat.csr(mm, nn, rpp, cc, vv)
+        A.set_spmm_path(1)  # the staged kernel whenever it applies
+        for k in ks:
+            for ldb in (k, k + 8):
+                Bd = rng.uniform(-1, 1, (nn, ldb)).astype(dt)
+                C0 = rng.uniform(-1, 1, (mm, k)).astype(dt)
+                Bt = torch.tensor(Bd, device="cuda")
+                Ct = torch.tensor(C0, device="cuda")
+                s = torch.cuda.Stream()
+                A.spmm_dev(Bt.data_ptr(), ldb, k, Ct.data_ptr(), k, 1.25, -0.5, s.cuda_stream)
+                s.synchronize()
+                info = A.spmm_info()
+                assert info["tile_rows"] > 0 and info["path"] == 1, (mm, k, ldb, info)
+                got = Ct.cpu().numpy().astype(np.float64)
+                B64 = np.ascontiguousarray(Bd[:, :k].astype(np.float64))
+                v64 = vv.astype(np.float64)
+                ref = spmm_ref(rpp, cc, v64, B64, 1.25, -0.5, C0.astype(np.float64))
+                err = scaled_err(got, ref, rpp, cc, v64, B64, 1.25, -0.5, C0.astype(np.float64))
+                assert err <= tol, (mm, k, ldb, err)
+
+
+def test_random_matrix_keeps_row_group_kernel():
+    """B rows of a random matrix are not reused within row blocks: the
+    staged path declines and the row-group kernel gives the result."""
+    rng = np.random.default_rng(8)
+    rp, c, v = W.random_csr(3000, 3000, 20, rng)
+    Bd = rng.uniform(-1, 1, (3000, 32))
+    A = pls.SpMat.csr(3000, 3000, rp, c, v)
+    B = pls.SpMat.dense(pls.ROW_MAJOR, 3000, 32, 32, Bd.reshape(-1))
+    Cm = pls.SpMat.null(3000, 32)
+    assert pls.spmm_exec(pls.OPERATION_NOTRANS, pls.OPERATION_NOTRANS, 1.0, A, B, 0.0, Cm) == 0
+    info = A.spmm_info()
+    assert info["tile_rows"] == 0 and info["path"] == 0, info
+    ref = spmm_ref(rp, c, v, Bd, 1.0, 0.0, None)
+    assert scaled_err(Cm.export_dense(), ref, rp, c, v, Bd, 1.0, 0.0, None) <= 1e-12
+
+
+def test_spmm_measured_choice_matches_oracle():
+    """Default path: the first SpMM on a stencil times both kernels on
+    scratch output, keeps the faster, and the result matches the oracle
+    (beta != 0: the timing runs must not touch C)."""
+    import torch
+
+    rng = np.random.default_rng(11)
+    m, n, rp, c, v = W.stencil_27pt(24, seed=2)
+    A = pls.SpMat.csr(m, n, rp, c, v)
+    for k in (8, 32):
+        Bd = rng.uniform(-1, 1, (n, k))
+        C0 = rng.uniform(-1, 1, (m, k))
+        Bt, Ct = torch.tensor(Bd, device="cuda"), torch.tensor(C0, device="cuda")
+        s = torch.cuda.Stream()
+        A.spmm_dev(Bt.data_ptr(), k, k, Ct.data_ptr(), k, 0.75, 1.5, s.cuda_stream)
+        s.synchronize()
+        info = A.spmm_info()
+        assert info["path"] in (0, 1) and info["ms_staged"] > 0 and info["ms_rows"] > 0, info
+        ref = spmm_ref(rp, c, v, Bd, 0.75, 1.5, C0)
+        assert scaled_err(Ct.cpu().numpy(), ref, rp, c, v, Bd, 0.75, 1.5, C0) <= 1e-12

@@ -144,3 +144,51 @@ def test_scs_spmv_equals_csr():
             s = oracle.scs_build(rp, c, v, 700, C, sigma)
             y = oracle.scs_spmv(s, x)
             np.testing.assert_allclose(y, y_ref, rtol=1e-12, atol=1e-12)
+
+
+def _random_coo(rng, m, n, nnz, unique):
+    r = rng.integers(0, m, nnz).astype(np.int32)
+    c = rng.integers(0, n, nnz).astype(np.int32)
+    v = rng.normal(size=nnz)
+    if unique:
+        _, ui = np.unique(r.astype(np.int64) * n + c, return_index=True)
+        ui = np.sort(ui)
+        r, c, v = r[ui], c[ui], v[ui]
+    return r, c, v
+
+
+def _csc_of(m, n, r, c, v):
+    order = np.lexsort((r, c))  # by column, then row
+    cp = np.zeros(n + 1, np.int32)
+    np.add.at(cp, c + 1, 1)
+    return r[order].astype(np.int32), np.cumsum(cp).astype(np.int32), v[order]
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference library not built here")
+def test_coo_csc_restatement_matches_reference():
+    """coo2csr / csc2csr restated in the oracle against the reference
+    library's own conversion (its export_csr converts COO / CSC handles to
+    CSR): bit-exact for distinct positions; with duplicates the structure is
+    exact and the values agree as a multiset (the reference's std::sort
+    leaves the order of equal positions unspecified)."""
+    rng = np.random.default_rng(5)
+    for t in range(20):
+        m, n = int(rng.integers(1, 300)), int(rng.integers(1, 300))
+        nnz = int(rng.integers(0, 3 * (m + n)))
+        r, c, v = _random_coo(rng, m, n, nnz, unique=True)
+        ours = oracle.coo2csr(m, n, r, c, v)
+        theirs = oracle.RefMatrix.coo(m, n, r, c, v).export_csr(m)
+        for a, b in zip(ours, theirs):
+            np.testing.assert_array_equal(a, b)
+        ri, cp, cv = _csc_of(m, n, r, c, v)
+        for base in (0, 1):
+            ours = oracle.csc2csr(m, n, ri + base, cp + base, cv)
+            theirs = oracle.RefMatrix.csc(m, n, ri + base, cp + base, cv).export_csr(m, index_base=base)
+            for a, b in zip(ours, theirs):
+                np.testing.assert_array_equal(a, b)
+        r, c, v = _random_coo(rng, m, n, nnz, unique=False)
+        o_rp, o_c, o_v = oracle.coo2csr(m, n, r, c, v)
+        t_rp, t_c, t_v = oracle.RefMatrix.coo(m, n, r, c, v).export_csr(m)
+        np.testing.assert_array_equal(o_rp, t_rp)
+        np.testing.assert_array_equal(o_c, t_c)
+        np.testing.assert_array_equal(np.sort(o_v), np.sort(t_v))
