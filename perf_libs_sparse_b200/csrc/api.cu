@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <mutex>
 
 #include "common.cuh"
@@ -629,6 +630,23 @@ int spmm_check(int transA, int transB, int alpha_h, Mat *A, Mat *B, int beta_h, 
   return PERFLIBS_STATUS_SUCCESS;
 }
 
+// C(i, j) = T(j, i) + beta * C(i, j) for an m x n C and an n x m T, any
+// layout and leading dimension of either (beta == 0: C is not read).
+template <class X>
+__global__ void k_add_transposed(int32_t m, int32_t n, const X *__restrict__ T, int64_t ldt,
+                                 int t_rowmajor, X *__restrict__ C, int64_t ldc, int c_rowmajor,
+                                 X beta, int beta_nz) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)m * n)
+    return;
+  // walk C in its storage order
+  const int64_t i = c_rowmajor ? idx / n : idx % m;
+  const int64_t j = c_rowmajor ? idx % n : idx / m;
+  const X t = t_rowmajor ? T[j * ldt + i] : T[i * ldt + j];
+  X *c = C + (c_rowmajor ? i * ldc + j : j * ldc + i);
+  *c = beta_nz ? t + beta * *c : t;
+}
+
 // The sparse x dense branch of the reference's spmm_exec_checked
 // (src/matmul.cpp:343-652), on the device. exec == false is the optimize
 // call: it prepares layouts and tunes without computing.
@@ -661,10 +679,49 @@ perflibs_status_t spmm_impl(int transA, int transB, X alpha, Mat *A, Mat *B, X b
     }
     return PERFLIBS_STATUS_SUCCESS;
   }
+  // Dense x sparse (src/matmul.cpp:654-740): (op(A) op(B))^T = op'(B) op'(A)
+  // with each operation flipped, so the sparse x dense path computes
+  // T = alpha * op'(B) op'(A) (n x m) and C = T^T + beta * C.
+  if (A->fmt == Fmt::DENSE && is_sparse(B->fmt) && (C->fmt == Fmt::DENSE || c_null) && A != C &&
+      B != C) {
+    if (A->dt != dt || B->dt != dt)
+      return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+    auto flip = [](int t) {
+      return t == PERFLIBS_SPARSE_OPERATION_NOTRANS ? PERFLIBS_SPARSE_OPERATION_TRANS
+                                                    : PERFLIBS_SPARSE_OPERATION_NOTRANS;
+    };
+    std::unique_ptr<Mat> T(new_mat(dt, Fmt::NUL));
+    T->m = n;
+    T->n = m;
+    T->stream = A->stream;
+    const perflibs_status_t st =
+        spmm_impl<X>(flip(transB), flip(transA), alpha, B, A, X(0), T.get(), exec);
+    if (st != PERFLIBS_STATUS_SUCCESS)
+      return st;
+    if (c_null)
+      make_dense_zero<X>(C, dt, m, n, PERFLIBS_ROW_MAJOR);
+    if (!exec)
+      return PERFLIBS_STATUS_SUCCESS;
+    if (T->fmt == Fmt::DENSE) {
+      const int64_t total = (int64_t)m * n;
+      k_add_transposed<X><<<(unsigned)div_up(total, 256), 256, 0, s>>>(
+          m, n, T->dense.vals.as<X>(), T->dense.lda, T->dense.layout == PERFLIBS_ROW_MAJOR,
+          C->dense.vals.as<X>(), C->dense.lda, C->dense.layout == PERFLIBS_ROW_MAJOR, beta,
+          beta != X(0));
+      PLS_LAUNCH_CHECK();
+    } else if (beta != X(0)) {  // T is the null matrix: C = beta * C
+      scal<X>((int64_t)C->m * C->n, beta, C->dense.vals.as<X>(), s);
+    } else {
+      PLS_CUDA(cudaMemsetAsync(C->dense.vals.p, 0, sizeof(X) * (size_t)C->m * C->n, s));
+    }
+    PLS_CUDA(cudaStreamSynchronize(s));
+    C->dense.is_zero = false;
+    return PERFLIBS_STATUS_SUCCESS;
+  }
   if (!(is_sparse(A->fmt) && B->fmt == Fmt::DENSE && (C->fmt == Fmt::DENSE || c_null) && A != C &&
         B != C))
     throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE,
-                "only sparse x dense products are provided by the B200 execute path");
+                "sparse x sparse and identity products are not provided by the B200 execute path");
   if (A->dt != dt || B->dt != dt)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
 

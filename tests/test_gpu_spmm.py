@@ -251,3 +251,60 @@ def test_spmm_measured_choice_matches_oracle():
         assert info["path"] in (0, 1) and info["ms_staged"] > 0 and info["ms_rows"] > 0, info
         ref = spmm_ref(rp, c, v, Bd, 0.75, 1.5, C0)
         assert scaled_err(Ct.cpu().numpy(), ref, rp, c, v, Bd, 0.75, 1.5, C0) <= 1e-12
+
+
+@pytest.mark.parametrize("ta", [pls.OPERATION_NOTRANS, pls.OPERATION_TRANS])
+@pytest.mark.parametrize("tb", [pls.OPERATION_NOTRANS, pls.OPERATION_TRANS])
+def test_dense_times_sparse_vs_numpy(ta, tb):
+    """Dense x sparse through the (AB)^T = B^T A^T identity of the reference
+    (src/matmul.cpp:654-740): C = alpha op(A) op(B) + beta C with A dense
+    (row- or column-major), B sparse CSR, C null or dense of either layout;
+    m = 3 takes the narrow (one SpMV per column) path inside."""
+    rng = np.random.default_rng(31 + 2 * ta + tb)
+    for m, kk, n in [(40, 60, 50), (3, 30, 20)]:
+        bm, bn = (kk, n) if tb == pls.OPERATION_NOTRANS else (n, kk)
+        brp, bc, bv = W.random_csr(bm, bn, 8, rng)
+        Bsp = np.zeros((bm, bn))
+        for i in range(bm):
+            Bsp[i, bc[brp[i]:brp[i + 1]]] = bv[brp[i]:brp[i + 1]]
+        opB = Bsp if tb == pls.OPERATION_NOTRANS else Bsp.T
+        am, an = (m, kk) if ta == pls.OPERATION_NOTRANS else (kk, m)
+        Ad = rng.uniform(-1, 1, (am, an))
+        opA = Ad if ta == pls.OPERATION_NOTRANS else Ad.T
+        for a_layout in (pls.ROW_MAJOR, pls.COL_MAJOR):
+            for c_kind in ("null", pls.ROW_MAJOR, pls.COL_MAJOR):
+                C0 = rng.uniform(-1, 1, (m, n))
+                beta = 0.0 if c_kind == "null" else -0.75
+                A = pls.SpMat.dense(a_layout, am, an, an if a_layout == pls.ROW_MAJOR else am,
+                                    (Ad if a_layout == pls.ROW_MAJOR else Ad.T).reshape(-1))
+                B = pls.SpMat.csr(bm, bn, brp, bc, bv)
+                if c_kind == "null":
+                    Cm = pls.SpMat.null(m, n)
+                else:
+                    Cm = pls.SpMat.dense(c_kind, m, n, n if c_kind == pls.ROW_MAJOR else m,
+                                         (C0 if c_kind == pls.ROW_MAJOR else C0.T).reshape(-1))
+                st = pls.spmm_exec(ta, tb, 1.25, A, B, beta, Cm)
+                assert st == 0, (m, a_layout, c_kind)
+                got = Cm.export_dense()
+                ref = 1.25 * opA @ opB + beta * C0
+                scale = 1.25 * np.abs(opA) @ np.abs(opB) + abs(beta) * np.abs(C0)
+                assert (np.abs(got - ref) / np.maximum(scale, 1e-300)).max() <= 1e-12, (m, a_layout, c_kind)
+
+
+def test_dense_times_sparse_fp32():
+    rng = np.random.default_rng(41)
+    m, kk, n = 64, 80, 48
+    brp, bc, bv = W.random_csr(kk, n, 6, rng)
+    bv = bv.astype(np.float32)
+    Bsp = np.zeros((kk, n))
+    for i in range(kk):
+        Bsp[i, bc[brp[i]:brp[i + 1]]] = bv[brp[i]:brp[i + 1]]
+    Ad = rng.uniform(-1, 1, (m, kk)).astype(np.float32)
+    A = pls.SpMat.dense(pls.ROW_MAJOR, m, kk, kk, Ad.reshape(-1))
+    B = pls.SpMat.csr(kk, n, brp, bc, bv)
+    Cm = pls.SpMat.null(m, n, dtype=np.float32)
+    assert pls.spmm_exec(pls.OPERATION_NOTRANS, pls.OPERATION_NOTRANS, 1.0, A, B, 0.0, Cm) == 0
+    got = Cm.export_dense().astype(np.float64)
+    ref = Ad.astype(np.float64) @ Bsp
+    scale = np.abs(Ad.astype(np.float64)) @ np.abs(Bsp)
+    assert (np.abs(got - ref) / np.maximum(scale, 1e-300)).max() <= 1e-5
