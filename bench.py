@@ -1,8 +1,9 @@
 """Benchmark of the sparse x dense execute path on B200.
 
 Default workload (N=1): FP64 SELL-C-sigma SpMV on the power-law matrix
-(n = 4,194,304 rows, Zipf(2) row lengths clipped to [1, 4096] with mean 16,
-uniform unique columns, N(0,1) values, x ~ U[-1,1], seed 1), C and sigma
+(n = 4,194,304 rows, row lengths Zipf-Mandelbrot p(k) ~ (k + q)^-2 on
+[1, 4096] with q solved for mean 16, uniform unique columns, N(0,1) values,
+x ~ U[-1,1], seed 1), C and sigma
 picked by the exhaustive autotuner, compared with the plain CSR kernel on
 the same matrix. A step is one y = A*x over the whole matrix with inputs
 resident in HBM (889 MB of algorithmic traffic: larger than the 126 MB L2,
@@ -55,6 +56,25 @@ def peaks():
 def dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
         os.environ.get("LOCAL_RANK", "0"))
+
+
+def max_over_ranks(value: float, device="cpu") -> float:
+    """The maximum of a per-rank float over the default process group (the
+    value itself without one). Every rank must call it at the same point."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_gbs(bytes_per_step: float, seconds_per_step: float, world: int) -> float:
+    """Whole-job GB/s of `world` independent replicas, each moving
+    bytes_per_step, timed by the slowest rank's seconds per step."""
+    return bytes_per_step / seconds_per_step / 1e9 * world
 
 
 class ClockSampler:
@@ -212,7 +232,7 @@ def run_b200(args):
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
 
@@ -262,11 +282,7 @@ def run_b200(args):
             torch.cuda.synchronize()
             torch.cuda.nvtx.range_pop()
             ms = e0.elapsed_time(e1)
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms / K
+        return max_over_ranks(ms, dev) / K
 
     K, Wm = args.steps, max(args.warmup, 3)
     # Keep the GPU busy ~0.5 s before the timed region so that the clock
@@ -351,20 +367,16 @@ def run_b200(args):
     for _ in range(Ke):
         st = lib.perflibs_spmv_exec_d(pls.OPERATION_NOTRANS, 1.0, A.h, xp, 0.0, yp)
         assert st == 0
-    e2e_s = (time.perf_counter() - t0) / Ke
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / Ke, dev)
 
     hbm, peak_kind = peaks()
-    achieved = bytes_step / (ms_tuned * 1e-3) / 1e9
+    achieved = replica_gbs(bytes_step, ms_tuned * 1e-3, 1)  # per GPU
     info = A.exec_info()
     kernels_per_step = info["kernels_per_spmv"]
     workload = f"C2 power-law SpMV n={m} nnz={nnz}"
     line = {
         "metric": "SpMV GB/s (algorithmic bytes) vs B200 HBM roofline, FP64, tuned vs plain CSR",
-        "value": achieved * world,
+        "value": replica_gbs(bytes_step, ms_tuned * 1e-3, world),
         "unit": "GB/s",
         "n_gpus": world,
         "steps": K,
@@ -385,13 +397,13 @@ def run_b200(args):
             "optimize_s": t_opt,
             "parallelism": f"replicas x{world}",
         },
-        "plain_csr": {"value": bytes_step / (ms_plain * 1e-3) / 1e9 * world, "ms_per_step": ms_plain},
+        "plain_csr": {"value": replica_gbs(bytes_step, ms_plain * 1e-3, world), "ms_per_step": ms_plain},
         "speedup_vs_plain_csr": ms_plain / ms_tuned,
         "max_rel_err": max_rel,
         "inf_norm_check": inf_check(y_gpu),
         "gflops": 2.0 * nnz / (ms_tuned * 1e-3) / 1e9 * world,
         "selector": selector_arms or None,
-        "e2e": {"value": bytes_step / e2e_s / 1e9 * world, "unit": "GB/s",
+        "e2e": {"value": replica_gbs(bytes_step, e2e_s, world), "unit": "GB/s",
                 "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": m * 8, "ms_per_step": e2e_s * 1e3},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_source": peak_kind,
