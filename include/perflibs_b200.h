@@ -308,6 +308,16 @@ perflibs_status_t perflibs_b200_read_mtx(const char *path, int32_t *m, int32_t *
                                          int64_t *nnz, int32_t **row_ptr,
                                          int32_t **col_indx, double **vals);
 
+/* ---- failure-path testing ---------------------------------------------
+ * For tests of the failure path only. The staged SpMM kernel waits on a
+ * shared-memory barrier for its bulk copies with a poll limit; on expiry it
+ * flags the failure (reported as EXECUTION_FAILURE by the handle's next
+ * SpMM) and stops without touching C. This makes every later staged launch
+ * post `shortfall_bytes` (0-4096) more than it copies, so the wait runs out
+ * after `wait_polls` polls with no copy in flight. (0, 0) restores the
+ * defaults: no shortfall, about a second of polling. */
+perflibs_status_t perflibs_b200_testing_stage_fault(int32_t shortfall_bytes, int32_t wait_polls);
+
 /* The handle's error record (what perflibs_spmat_print_err prints): the
  * status of the last failed call (0 when none), the 1-based argument
  * position for input errors, and the message (NUL-terminated, truncated to

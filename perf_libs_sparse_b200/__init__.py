@@ -112,6 +112,7 @@ def lib():
             "perflibs_b200_spmat_spmm_info": [vp, vp, vp, vp, vp, vp, vp],
             "perflibs_b200_spmat_set_spmm_path": [vp, i32],
             "perflibs_b200_read_mtx": [C.c_char_p, vp, vp, vp, vp, vp, vp],
+            "perflibs_b200_testing_stage_fault": [i32, i32],
             "perflibs_b200_spmv_exec_d_dev": [i, d, vp, vp, d, vp, vp],
             "perflibs_b200_spmv_exec_s_dev": [i, f, vp, vp, f, vp, vp],
             "perflibs_b200_spmm_exec_d_dev": [d, vp, vp, i64, i32, d, vp, i64, vp],

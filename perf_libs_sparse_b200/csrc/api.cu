@@ -504,6 +504,7 @@ template <class X> bool matches(const Mat *A) {
 
 template <class X>
 perflibs_status_t spmv_exec_host(int trans, X alpha, Mat *A, const X *x, X beta, X *y) {
+  TraceRange trace("perflibs_spmv_exec");
   if (!A)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
   return guarded(A, [&]() -> perflibs_status_t {
@@ -832,6 +833,7 @@ perflibs_status_t spmm_impl(int transA, int transB, X alpha, Mat *A, Mat *B, X b
 template <class X>
 perflibs_status_t spmm_exec_entry(int transA, int transB, X alpha, Mat *A, Mat *B, X beta,
                                   Mat *C) {
+  TraceRange trace("perflibs_spmm_exec");
   const int st = spmm_check(transA, transB, PERFLIBS_SPARSE_SCALAR_ANY, A, B,
                             PERFLIBS_SPARSE_SCALAR_ANY, C);
   if (st != PERFLIBS_STATUS_SUCCESS)
@@ -1354,6 +1356,7 @@ perflibs_status_t perflibs_spmat_hint(perflibs_spmat_t A, enum perflibs_sparse_h
 
 // src/matvec.cpp:583-630 (spmv_optimize).
 perflibs_status_t perflibs_spmv_optimize(perflibs_spmat_t A) {
+  TraceRange trace("perflibs_spmv_optimize");
   if (!A)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
   return guarded(A, [&]() -> perflibs_status_t {
@@ -1423,6 +1426,7 @@ perflibs_status_t perflibs_spmm_optimize(enum perflibs_sparse_hint_value transA,
                                          perflibs_spmat_t A, perflibs_spmat_t B,
                                          enum perflibs_sparse_hint_value beta,
                                          perflibs_spmat_t C) {
+  TraceRange trace("perflibs_spmm_optimize");
   const int st = spmm_check(transA, transB, alpha, A, B, beta, C);
   if (st != PERFLIBS_STATUS_SUCCESS)
     return (perflibs_status_t)st;

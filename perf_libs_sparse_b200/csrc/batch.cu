@@ -262,6 +262,7 @@ perflibs_status_t perflibs_b200_batch_set_tile(perflibs_b200_batch_t B, int32_t 
 
 perflibs_status_t perflibs_b200_batch_tune(perflibs_b200_batch_t B, int32_t *best_tile,
                                            float *best_ms) {
+  TraceRange trace("perflibs_b200_batch_tune");
   if (!B)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
   try {

@@ -28,6 +28,8 @@
 #include <utility>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/perflibs_b200.h"
 #include "../../include/perflibs_sparse.h"
 
@@ -52,6 +54,17 @@ struct Error : std::runtime_error {
   } while (0)
 
 #define PLS_LAUNCH_CHECK() PLS_CUDA(cudaGetLastError())
+
+// An NVTX range over a library call (optimize, host-pointer exec, SpMM,
+// batch tuning), visible in Nsight timelines; free when no tool listens.
+// The device-pointer SpMV entry points, the per-iteration hot path, carry
+// none, so callers' own ranges around them stay the innermost.
+struct TraceRange {
+  explicit TraceRange(const char *name) { nvtxRangePushA(name); }
+  ~TraceRange() { nvtxRangePop(); }
+  TraceRange(const TraceRange &) = delete;
+  TraceRange &operator=(const TraceRange &) = delete;
+};
 
 // ------------------------------------------------------------ device buffer
 

@@ -41,6 +41,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <atomic>
 
 #include "common.cuh"
 #include "pls_internal.hpp"
@@ -221,9 +222,9 @@ __device__ __forceinline__ bool bar_try_wait(uint64_t *bar, uint32_t parity) {
 
 // Bounded wait for the phase with `parity`: polls back to back first (the
 // copies usually land within a few microseconds), then with short sleeps;
-// gives up after about a second.
-__device__ __forceinline__ bool bar_wait_bounded(uint64_t *bar, uint32_t parity) {
-  for (int it = 0; it < (1 << 22); ++it) {
+// gives up after `limit` polls (the default 2^22 is about a second).
+__device__ __forceinline__ bool bar_wait_bounded(uint64_t *bar, uint32_t parity, int limit) {
+  for (int it = 0; it < limit; ++it) {
     if (bar_try_wait(bar, parity))
       return true;
     if (it >= 1024)
@@ -285,7 +286,7 @@ __device__ __forceinline__ void stage_item(int lane, unsigned char *sb, const St
                                            const int32_t *__restrict__ run_ptr,
                                            const int4 *__restrict__ runs,
                                            const int32_t *__restrict__ nuniq,
-                                           const X *__restrict__ B, int64_t ldb) {
+                                           const X *__restrict__ B, int64_t ldb, int tx_extra) {
   const int64_t r0 = blk * R;
   const int64_t r1 = r0 + R < (int64_t)m ? r0 + R : (int64_t)m;
   const int64_t p0 = rp[r0], p1 = rp[r1];
@@ -294,7 +295,7 @@ __device__ __forceinline__ void stage_item(int lane, unsigned char *sb, const St
     interior(p0, p1, sizeof(V), va0, va1);
     interior(p0, p1, 2, la0, la1);
     const uint64_t tx = (uint64_t)nuniq[blk] * (uint64_t)kw * sizeof(X) + (uint64_t)(va1 - va0) +
-                        (uint64_t)(la1 - la0);
+                        (uint64_t)(la1 - la0) + (uint64_t)tx_extra;
     // the buffer's previous contents were read through the generic proxy
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
@@ -333,7 +334,8 @@ __global__ void __launch_bounds__(kStageThreads, 1)
                  const int32_t *__restrict__ run_ptr, const int4 *__restrict__ runs,
                  const int32_t *__restrict__ nuniq, const X *__restrict__ B, int64_t ldb,
                  X *__restrict__ C, int64_t ldc, int k, int KT, int whole_rows, StageLayout L,
-                 X alpha, X beta, int beta_nz, int *__restrict__ err) {
+                 X alpha, X beta, int beta_nz, int *__restrict__ err, int tx_extra,
+                 int wait_limit) {
   using Acc = typename AccOf<V, X>::type;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t bars[2];
@@ -355,7 +357,7 @@ __global__ void __launch_bounds__(kStageThreads, 1)
     const int k0 = (int)(it / nblocks) * KT;
     const int kw = min(KT, k - k0);
     stage_item<V, X>(lane, sbuf[b], L, &bars[b], m, R, blk, k0, kw, stride, whole_rows, k, rp, val,
-                     local, run_ptr, runs, nuniq, B, ldb);
+                     local, run_ptr, runs, nuniq, B, ldb, tx_extra);
   };
   if (warp == 0)
     issue(blockIdx.x, 0);
@@ -373,7 +375,7 @@ __global__ void __launch_bounds__(kStageThreads, 1)
   int b = 0;
   for (int64_t it = blockIdx.x; it < n_items; it += gridDim.x) {
     if (threadIdx.x == 0)
-      ok_s = bar_wait_bounded(&bars[b], phase[b]);
+      ok_s = bar_wait_bounded(&bars[b], phase[b], wait_limit);
     __syncthreads();
     if (!ok_s) {
       // The copies did not land in time: record it, give the copies in
@@ -382,7 +384,7 @@ __global__ void __launch_bounds__(kStageThreads, 1)
       if (threadIdx.x == 0) {
         *(volatile int *)err = 1;
         __threadfence_system();
-        bar_wait_bounded(&bars[b], phase[b]);
+        bar_wait_bounded(&bars[b], phase[b], wait_limit);
       }
       __syncthreads();
       return;
@@ -530,6 +532,11 @@ StageLayout stage_layout(const TileDev &t, size_t row_bytes, size_t val_bytes) {
 // matrices) the row-group kernel runs.
 constexpr size_t kStageBudget = 100 * 1024;
 
+// Failure-path test hook (perflibs_b200_testing_stage_fault): bytes the
+// stage barrier expects beyond what is copied, and the wait's poll limit.
+std::atomic<int> g_stage_shortfall{0};
+std::atomic<int> g_stage_wait_limit{1 << 22};
+
 void check_tile_error(const TileDev &t) {
   if (t.err.host && *(volatile int *)t.err.host) {
     *(volatile int *)t.err.host = 0;
@@ -600,7 +607,7 @@ bool spmm_tiled(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64_t ldc
           m, t.R, t.nblocks, ktiles, c.row_ptr.as<int32_t>(), (const V *)c.ev(),
           t.local.as<uint16_t>(), t.run_ptr.as<int32_t>(), t.runs.as<int4>(),
           t.nuniq.as<int32_t>(), B, ldb, C, ldc, k, KT, whole_rows ? 1 : 0, L, alpha, beta, bnz,
-          t.err.dev);
+          t.err.dev, g_stage_shortfall.load(), g_stage_wait_limit.load());
     }
   });
   PLS_LAUNCH_CHECK();
@@ -613,3 +620,12 @@ template bool spmm_tiled<double>(CsrDev &, int32_t, const double *, int64_t, dou
                                  int, double, double, cudaStream_t, bool);
 
 }  // namespace pls
+
+extern "C" perflibs_status_t perflibs_b200_testing_stage_fault(int32_t shortfall_bytes,
+                                                             int32_t wait_polls) {
+  if (shortfall_bytes < 0 || shortfall_bytes > 4096 || wait_polls < 0)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  pls::g_stage_shortfall.store(shortfall_bytes);
+  pls::g_stage_wait_limit.store(wait_polls > 0 ? wait_polls : (1 << 22));
+  return PERFLIBS_STATUS_SUCCESS;
+}

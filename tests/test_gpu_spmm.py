@@ -308,3 +308,40 @@ def test_dense_times_sparse_fp32():
     ref = Ad.astype(np.float64) @ Bsp
     scale = np.abs(Ad.astype(np.float64)) @ np.abs(Bsp)
     assert (np.abs(got - ref) / np.maximum(scale, 1e-300)).max() <= 1e-5
+
+
+def test_staged_wait_timeout_is_reported_and_recoverable():
+    """Failure path without a fault: the test hook makes the staged kernel's
+    barrier expect 16 bytes more than it copies, so its bounded wait runs out
+    (20,000 polls, several milliseconds; every copy has landed by then). The
+    kernel flags the failure and leaves C untouched; the handle's next SpMM
+    reports EXECUTION_FAILURE; after the hook is cleared the same handle and
+    context compute correctly again."""
+    import torch
+
+    m, n, rp, c, v = W.stencil_27pt(16, seed=2)
+    k = 8
+    rng = np.random.default_rng(12)
+    Bd = rng.uniform(-1, 1, (n, k))
+    A = pls.SpMat.csr(m, n, rp, c, v)
+    A.set_spmm_path(1)
+    Bt = torch.tensor(Bd, device="cuda")
+    Ct = torch.full((m, k), 7.0, dtype=torch.float64, device="cuda")
+    s = torch.cuda.Stream()
+    L = pls.lib()
+    assert L.perflibs_b200_testing_stage_fault(16, 20000) == 0
+    try:
+        A.spmm_dev(Bt.data_ptr(), k, k, Ct.data_ptr(), k, 1.0, 0.0, s.cuda_stream)
+        s.synchronize()
+        assert A.spmm_info()["path"] == 1
+        assert torch.all(Ct == 7.0)  # C untouched by the failed launch
+        with pytest.raises(pls.PerflibsError) as e:
+            A.spmm_dev(Bt.data_ptr(), k, k, Ct.data_ptr(), k, 1.0, 0.0, s.cuda_stream)
+        assert e.value.status == pls.STATUS_EXECUTION_FAILURE
+    finally:
+        assert L.perflibs_b200_testing_stage_fault(0, 0) == 0
+    s.synchronize()
+    A.spmm_dev(Bt.data_ptr(), k, k, Ct.data_ptr(), k, 1.0, 0.0, s.cuda_stream)
+    s.synchronize()
+    ref = spmm_ref(rp, c, v, Bd, 1.0, 0.0, None)
+    assert scaled_err(Ct.cpu().numpy(), ref, rp, c, v, Bd, 1.0, 0.0, None) <= 1e-12
