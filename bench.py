@@ -473,7 +473,39 @@ def run_extra(args):
 
     line = {"n_gpus": 1, "steps": K, "warmup": Wm, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "data": "synthetic", "unit": "GB/s"}
-    if args.workload == "c1":
+    if args.workload == "c3spmv":
+        # FP64 SpMV (tuned) on C3's matrix: the structured counterpart of C2,
+        # where x gathers are neighbours instead of uniformly random.
+        m, n, rp, c, v = W.stencil_27pt(128, seed=2)
+        x = W.uniform_vector(n, 2)
+        A = pls.SpMat.csr(m, n, rp, c, v)
+        A.set_stream(sp)
+        A.hint(pls.HINT_SPMV_INVOCATIONS, pls.INVOCATIONS_MANY)
+        assert A.optimize() == 0
+        P = pls.SpMat.csr(m, n, rp, c, v)
+        P.set_stream(sp)
+        P.hint(pls.HINT_SPMV_INVOCATIONS, pls.INVOCATIONS_SINGLE)
+        assert P.optimize() == 0
+        xd = torch.tensor(x, device="cuda")
+        yd = torch.zeros(m, dtype=torch.float64, device="cuda")
+        ms_plain = timed(lambda: P.spmv_dev(xd.data_ptr(), yd.data_ptr(), 1.0, 0.0, sp))
+        ms = timed(lambda: A.spmv_dev(xd.data_ptr(), yd.data_ptr(), 1.0, 0.0, sp))
+        torch.cuda.synchronize()
+        y = yd.cpu().numpy()
+        y_ref = oracle.csr_spmv(rp, c, v, x)
+        sc = oracle.csr_absdot(rp, c, v, x)
+        err = float((np.abs(y - y_ref) / np.maximum(np.maximum(np.abs(y_ref), sc), 1e-300)).max())
+        b = W.algorithmic_bytes_spmv(m, n, int(rp[-1]), 8, 8, False)
+        cfg = A.config()
+        line.update(metric="SpMV GB/s (algorithmic bytes), FP64, 27-point stencil 128^3, tuned vs plain CSR",
+                    dtype="f64", value=b / ms / 1e6, ms_per_step=ms, max_rel_err=err,
+                    plain_csr={"value": b / ms_plain / 1e6, "ms_per_step": ms_plain},
+                    speedup_vs_plain_csr=ms_plain / ms,
+                    config={"workload": "27-point stencil 128^3 n=2097152 nnz=55742968 (C3's matrix)",
+                            "format": {0: "CSR", 1: "SELL-C-sigma", 2: "CSR-split"}[cfg["kind"]],
+                            "C": cfg["C"], "sigma": cfg["sigma"], "tpr": cfg["tpr"],
+                            "l2": "inputs (711 MB) exceed L2; no flush"})
+    elif args.workload == "c1":
         m, n, rp, c, v = W.laplacian_2d(512)
         x = W.uniform_vector(n, 0)
         A = pls.SpMat.csr(m, n, rp, c, v)
@@ -559,7 +591,7 @@ def run_extra(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4"],
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c3spmv", "c4"],
                     help="c2 (default, the headline) or one of the other configurations")
     ap.add_argument("--k", type=int, default=32, help="right-hand sides for --workload c3")
     ap.add_argument("--storage", default="native", choices=["native", "fp32", "bf16"])
