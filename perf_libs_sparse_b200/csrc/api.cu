@@ -227,6 +227,7 @@ perflibs_status_t create_csr(Mat **out, int32_t m, int32_t n, const int32_t *row
     cudaStream_t s = stream_of(A);
     CsrDev &c = A->csr;
     c.nnz = A->nnz;
+    c.ncols = n;
     c.vt = native_vt(A->dt);
     upload_index(c.row_ptr, row_ptr, (int64_t)m + 1, A->index_base, s);
     upload_index(c.col, col, A->nnz, A->index_base, s);
@@ -288,6 +289,7 @@ perflibs_status_t create_coo(Mat **out, int32_t m, int32_t n, int32_t nnz, const
     if (bad >= 0)
       return param_error(A, row[bad] < 0 || row[bad] >= m ? 5 : 6,
                          "entry " + std::to_string(bad) + " is outside the matrix");
+    A->csr.ncols = n;
     A->cfg = default_config(A);
     return PERFLIBS_STATUS_SUCCESS;
   });
@@ -340,6 +342,7 @@ perflibs_status_t create_csc(Mat **out, int32_t m, int32_t n, const int32_t *row
     if (bad.second >= 0)
       return param_error(A, 4, "row_indx[" + std::to_string(bad.second) + "] is outside [0, m)");
     build_csr_transpose(t, n, m, A->csr, s);
+    A->csr.ncols = n;
     PLS_CUDA(cudaStreamSynchronize(s));
     A->cfg = default_config(A);
     return PERFLIBS_STATUS_SUCCESS;
@@ -1938,6 +1941,7 @@ perflibs_status_t perflibs_b200_spmat_create_csr_d_dev(perflibs_spmat_t *out, in
       return param_error(A, 4, "row_ptr[m] is below row_ptr[0]");
     CsrDev &c = A->csr;
     c.nnz = A->nnz;
+    c.ncols = n;
     c.vt = Vt::F64;
     c.row_ptr.reserve(4 * ((size_t)m + 1));
     c.col.reserve(std::max<size_t>(4 * A->nnz, 16));

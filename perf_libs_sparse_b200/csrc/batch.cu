@@ -41,6 +41,29 @@ struct Item {
   int32_t inst, row0, row1, pad;
 };
 
+// One item's rows with the instance's row kind (CSR or BSR, resolved at
+// compile time) and vector shape.
+template <class Rows, bool OFF32>
+__device__ __forceinline__ void batch_rows(const Rows &A, const InstDesc &d, const Item &w,
+                                           int lane, float alpha, float beta, int beta_nz,
+                                           const L2Policy &pol) {
+  const int lg_g = d.lg_tk + d.lg_tn;
+  for (int32_t r0 = w.row0; r0 < w.row1; r0 += (32 >> lg_g)) {
+    const int32_t row = r0 + (lane >> lg_g);
+    const bool live = row < w.row1;
+    if (d.path == 0)
+      spmm_row_group<4, 1, float, float, Rows, OFF32>(A, row, live, d.lg_tk, d.lg_tn, d.B, d.ldb,
+                                                      d.C, d.ldc, d.k, alpha, beta, beta_nz, pol);
+    else if (d.path == 1)
+      spmm_row_group<1, 1, float, float, Rows, OFF32>(A, row, live, d.lg_tk, d.lg_tn, d.B, d.ldb,
+                                                      d.C, d.ldc, d.k, alpha, beta, beta_nz, pol);
+    else
+      spmm_row_group<1, 2, float, float, Rows, OFF32>(A, row, live, d.lg_tk, d.lg_tn, d.B, d.ldb,
+                                                      d.C, d.ldc, d.k, alpha, beta, beta_nz, pol);
+  }
+}
+
+template <bool OFF32>
 __global__ void __launch_bounds__(256)
     k_batch_spmm(const InstDesc *__restrict__ inst, const Item *__restrict__ items,
                  int64_t n_items, unsigned long long *__restrict__ counter, float alpha,
@@ -58,20 +81,16 @@ __global__ void __launch_bounds__(256)
       next = atomicAdd(counter, 1ull);
     const Item w = items[it];
     const InstDesc d = inst[w.inst];
-    const MixedRows A{d.rp, d.col, d.val, d.bs, d.layout == PERFLIBS_ROW_MAJOR, d.is_bsr};
-    const int lg_g = d.lg_tk + d.lg_tn;
-    for (int32_t r0 = w.row0; r0 < w.row1; r0 += (32 >> lg_g)) {
-      const int32_t row = r0 + (lane >> lg_g);
-      const bool live = row < w.row1;
-      if (d.path == 0)
-        spmm_row_group<4, 1, float, float>(A, row, live, d.lg_tk, d.lg_tn, d.B, d.ldb, d.C,
-                                           d.ldc, d.k, alpha, beta, beta_nz, pol);
-      else if (d.path == 1)
-        spmm_row_group<1, 1, float, float>(A, row, live, d.lg_tk, d.lg_tn, d.B, d.ldb, d.C,
-                                           d.ldc, d.k, alpha, beta, beta_nz, pol);
-      else
-        spmm_row_group<1, 2, float, float>(A, row, live, d.lg_tk, d.lg_tn, d.B, d.ldb, d.C,
-                                           d.ldc, d.k, alpha, beta, beta_nz, pol);
+    if (d.is_bsr) {
+      int lg = 0;
+      while ((1 << lg) < d.bs)
+        ++lg;
+      const BsrRows A{d.rp, d.col, d.val, d.bs, (1 << lg) == d.bs ? lg : -1,
+                      d.layout == PERFLIBS_ROW_MAJOR};
+      batch_rows<BsrRows, OFF32>(A, d, w, lane, alpha, beta, beta_nz, pol);
+    } else {
+      const CsrRows<float> A{d.rp, d.col, d.val};
+      batch_rows<CsrRows<float>, OFF32>(A, d, w, lane, alpha, beta, beta_nz, pol);
     }
     it = __shfl_sync(0xffffffffu, next, 0);
   }
@@ -94,6 +113,7 @@ struct perflibs_b200_batch_s {
   float g_alpha = 0.f, g_beta = 0.f;
   bool graph_valid = false;
   bool own_stream = false;
+  bool off32 = true;  // every B / C offset of every instance fits in 32 bits
   ~perflibs_b200_batch_s() {
     if (graph)
       cudaGraphExecDestroy(graph);
@@ -144,9 +164,11 @@ void capture(Batch *B, float alpha, float beta) {
   PLS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   cudaMemsetAsync(B->counter.p, 0, 8, s);
   if (B->n_items > 0)
-    k_batch_spmm<<<B->grid, 256, 0, s>>>(B->inst.as<InstDesc>(), B->items.as<Item>(), B->n_items,
-                                         B->counter.as<unsigned long long>(), alpha, beta,
-                                         beta != 0.f);
+  {
+    auto kern = B->off32 ? k_batch_spmm<true> : k_batch_spmm<false>;
+    kern<<<B->grid, 256, 0, s>>>(B->inst.as<InstDesc>(), B->items.as<Item>(), B->n_items,
+                                 B->counter.as<unsigned long long>(), alpha, beta, beta != 0.f);
+  }
   PLS_CUDA(cudaStreamEndCapture(s, &g));
   PLS_CUDA(cudaGraphInstantiate(&B->graph, g, 0));
   cudaGraphDestroy(g);
@@ -228,6 +250,9 @@ perflibs_status_t perflibs_b200_batch_create(perflibs_b200_batch_t *out, int32_t
       d.lg_tk = sh.lg_tk;
       d.lg_tn = sh.lg_tn;
       d.path = v4 ? 0 : (sh.nv == 2 ? 2 : 1);
+      // B has A->n rows of ldb, C has A->m rows of ldc
+      if ((int64_t)A->n * ldb[i] >= INT32_MAX || (int64_t)A->m * ldc[i] >= INT32_MAX)
+        B->off32 = false;
       B->host.push_back(d);
       B->work_per_row.push_back(((double)A->nnz / std::max(A->m, 1) + 1.0) * std::max(k[i], 1));
     }
@@ -237,7 +262,8 @@ perflibs_status_t perflibs_b200_batch_create(perflibs_b200_batch_t *out, int32_t
     B->counter.reserve(8);
     int sms = 0, per_sm = 0;
     PLS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, B->device));
-    PLS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_spmm, 256, 0));
+    PLS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, B->off32 ? k_batch_spmm<true> : k_batch_spmm<false>, 256, 0));
     B->grid = sms * std::max(per_sm, 1);
     build_items(B, 64);
     *out = B;

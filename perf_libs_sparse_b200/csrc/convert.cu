@@ -369,6 +369,7 @@ void build_csr_transpose(const CsrDev &c, int32_t m, int32_t n, CsrDev &out,
   CsrDev T;
   T.vt = c.vt;
   T.nnz = c.nnz;
+  T.ncols = m;
   T.row_ptr.reserve(sizeof(int32_t) * (n + 1));
   T.col.reserve(sizeof(int32_t) * std::max<int64_t>(c.nnz, 1));
   T.vals.reserve(vt_size(c.vt) * std::max<int64_t>(c.nnz, 1));
@@ -567,6 +568,7 @@ void bsr_to_csr(const BsrDev &b, int32_t m, bool drop_zeros, CsrDev &out,
                 cudaStream_t s) {
   CsrDev R;
   R.vt = b.vt;
+  R.ncols = b.nb * b.bs;
   R.row_ptr.reserve(sizeof(int32_t) * (m + 1));
   DevBuf cnt;
   cnt.reserve(sizeof(int32_t) * (m + 1));

@@ -205,6 +205,7 @@ struct TileDev {
 struct CsrDev {
   DevBuf row_ptr, col, vals;  // vals in the API type (authoritative)
   int64_t nnz = 0;
+  int32_t ncols = 0;  // columns (bound of col); 0 when not recorded
   Vt vt = Vt::F64;
   // Reduced-precision copy of the values used by the kernels when the
   // handle's storage mode asks for one.

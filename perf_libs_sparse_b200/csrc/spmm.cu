@@ -10,13 +10,15 @@
 //
 // BSR: a warp per block row, lanes over C's columns; each lane keeps bs
 // accumulators (one per scalar row of the block row).
+#include <type_traits>
+
 #include "common.cuh"
 #include "pls_internal.hpp"
 #include "spmm_rows.cuh"
 
 namespace pls {
 
-template <int VEC, int NV, class V, class X>
+template <int VEC, int NV, class V, class X, bool OFF32>
 __global__ void __launch_bounds__(256)
     k_spmm_csr(int32_t m, int lg_tk, int lg_tn, const int32_t *__restrict__ rp,
                const int32_t *__restrict__ col, const V *__restrict__ val,
@@ -28,59 +30,98 @@ __global__ void __launch_bounds__(256)
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t row = (warp << (5 - lg_g)) + ((threadIdx.x & 31) >> lg_g);
   const CsrRows<V> A{rp, col, val};
-  spmm_row_group<VEC, NV, Acc, X>(A, row, row < m, lg_tk, lg_tn, B, ldb, C, ldc, k, alpha, beta,
-                                  beta_nz, pol);
+  spmm_row_group<VEC, NV, Acc, X, CsrRows<V>, OFF32>(A, row, row < m, lg_tk, lg_tn, B, ldb, C,
+                                                      ldc, k, alpha, beta, beta_nz, pol);
+}
+
+// 32-bit address arithmetic is possible when every offset into B (rows
+// 0 .. ncols-1 of ldb) and C (rows 0 .. m-1 of ldc) fits; ncols 0 means the
+// column count was not recorded.
+static bool rows_off32_fits(const CsrDev &c, int32_t m, int64_t ldb, int64_t ldc) {
+  return c.ncols > 0 && (int64_t)c.ncols * ldb < INT32_MAX && (int64_t)m * ldc < INT32_MAX;
 }
 
 template <int VEC, class V, class X>
 static void launch_spmm_csr(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
-                            int64_t ldc, int k, X alpha, X beta, cudaStream_t s) {
+                            int64_t ldc, int k, X alpha, X beta, bool off32, cudaStream_t s) {
   const RowsShape sh = rows_shape(k, VEC, (double)c.nnz / std::max<int32_t>(m, 1));
   const int64_t rows_per_block = (int64_t)8 << (5 - (sh.lg_tk + sh.lg_tn));
   const unsigned blocks = (unsigned)div_up(m, rows_per_block);
   const int bnz = beta != X(0);
+  off32 = off32 && rows_off32_fits(c, m, ldb, ldc);
+  auto go = [&](auto nv_tag, auto off_tag) {
+    constexpr int NV = decltype(nv_tag)::value;
+    constexpr bool OFF = decltype(off_tag)::value;
+    k_spmm_csr<VEC, NV, V, X, OFF><<<blocks, 256, 0, s>>>(m, sh.lg_tk, sh.lg_tn,
+        c.row_ptr.as<int32_t>(), c.col.as<int32_t>(), (const V *)c.ev(), B, ldb, C, ldc, k,
+        alpha, beta, bnz);
+  };
+  using I1 = std::integral_constant<int, 1>;
+  using I2 = std::integral_constant<int, 2>;
+  using T = std::true_type;
+  using F = std::false_type;
   if (sh.nv == 2)
-    k_spmm_csr<VEC, 2, V, X><<<blocks, 256, 0, s>>>(m, sh.lg_tk, sh.lg_tn, c.row_ptr.as<int32_t>(),
-        c.col.as<int32_t>(), (const V *)c.ev(), B, ldb, C, ldc, k, alpha, beta, bnz);
+    off32 ? go(I2{}, T{}) : go(I2{}, F{});
   else
-    k_spmm_csr<VEC, 1, V, X><<<blocks, 256, 0, s>>>(m, sh.lg_tk, sh.lg_tn, c.row_ptr.as<int32_t>(),
-        c.col.as<int32_t>(), (const V *)c.ev(), B, ldb, C, ldc, k, alpha, beta, bnz);
+    off32 ? go(I1{}, T{}) : go(I1{}, F{});
 }
 
-// Row-group SpMM (the launch half of spmm_csr).
+// Row-group SpMM (the launch half of spmm_csr), with 32-bit address
+// arithmetic when `off32` and the offsets fit.
 template <class X>
 static void spmm_rows(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64_t ldc,
-                      int k, X alpha, X beta, cudaStream_t s);
+                      int k, X alpha, X beta, bool off32, cudaStream_t s) {
+  constexpr int VMAX = 16 / sizeof(X);
+  const bool aligned = k >= VMAX && ((uintptr_t)B % 16 == 0) && ((uintptr_t)C % 16 == 0) &&
+                       (ldb % VMAX == 0) && (ldc % VMAX == 0);
+  with_vt(c.evt(), [&](auto tag) {
+    using V = typename decltype(tag)::type;
+    if constexpr (std::is_same_v<X, float> && std::is_same_v<V, double>) {
+      throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE, "FP64 storage with FP32 API");
+    } else {
+      if (aligned)
+        launch_spmm_csr<VMAX, V, X>(c, m, B, ldb, C, ldc, k, alpha, beta, off32, s);
+      else
+        launch_spmm_csr<1, V, X>(c, m, B, ldb, C, ldc, k, alpha, beta, off32, s);
+    }
+  });
+  PLS_LAUNCH_CHECK();
+}
 
-// The first SpMM of a call signature on a matrix the staged kernel applies
-// to runs both kernels on a scratch C (beta = 0, CUDA events, one warm-up
-// and two timed runs each) and keeps the faster; later calls with that
-// signature use the kept choice. Matrices it does not apply to (B rows not
-// reused inside row blocks, B not 16-byte aligned) always take the
-// row-group kernel.
+// Kernel choice for a CSR SpMM, measured once per call signature (k, ldb,
+// value and API types): the row-group kernel with 64-bit and, when the
+// offsets fit, 32-bit address arithmetic (the better of the two differs
+// with k and the value type), and the staged kernel when it applies. With
+// more than one candidate, the first SpMM of the signature runs each on a
+// scratch C (beta = 0, CUDA events, one warm-up and two timed runs) and
+// keeps the fastest; later calls use the kept one. choice: 0 row group
+// 64-bit, 2 row group 32-bit, 1 staged.
 template <class X>
 void spmm_csr(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
               int64_t ldc, int k, X alpha, X beta, cudaStream_t s) {
   if (m == 0 || k == 0)
     return;
-  const int64_t sig = ((int64_t)k << 32) ^ (ldb << 8) ^ ((int64_t)sizeof(X) << 4) ^
-                      (int64_t)c.evt();
+  const int64_t sig = ((int64_t)k << 32) ^ (ldb << 8) ^ (ldc << 20) ^
+                      ((int64_t)sizeof(X) << 4) ^ (int64_t)c.evt();
   TileDev &t = c.tiles;
+  const bool fits32 = rows_off32_fits(c, m, ldb, ldc);
   if (t.forced == 0) {
-    spmm_rows<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s);
+    spmm_rows<X>(c, m, B, ldb, C, ldc, k, alpha, beta, fits32, s);
     t.last_path = 0;
     return;
   }
   if (t.forced == 1) {
     const bool staged = spmm_tiled<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s, true);
     if (!staged)
-      spmm_rows<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s);
+      spmm_rows<X>(c, m, B, ldb, C, ldc, k, alpha, beta, fits32, s);
     t.last_path = staged ? 1 : 0;
     return;
   }
   if (t.choice_sig != sig) {
+    const bool staged_ok = spmm_tiled<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s, false);
     t.choice = 0;
-    if (spmm_tiled<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s, false)) {
+    t.ms_rows = t.ms_staged = 0.f;
+    if (staged_ok || fits32) {
       DevBuf scratch;
       scratch.reserve(sizeof(X) * (size_t)m * k);
       X *sc = scratch.as<X>();
@@ -98,12 +139,26 @@ void spmm_csr(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
         PLS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
         return ms / 2;
       };
-      t.ms_rows = time2([&] { spmm_rows<X>(c, m, B, ldb, sc, (int64_t)k, k, X(1), X(0), s); });
-      t.ms_staged =
-          time2([&] { spmm_tiled<X>(c, m, B, ldb, sc, (int64_t)k, k, X(1), X(0), s, true); });
+      const float ms64 =
+          time2([&] { spmm_rows<X>(c, m, B, ldb, sc, (int64_t)k, k, X(1), X(0), false, s); });
+      float best = ms64;
+      if (fits32 && rows_off32_fits(c, m, ldb, k)) {
+        const float ms32 =
+            time2([&] { spmm_rows<X>(c, m, B, ldb, sc, (int64_t)k, k, X(1), X(0), true, s); });
+        if (ms32 < best) {
+          best = ms32;
+          t.choice = 2;
+        }
+      }
+      t.ms_rows = best;
+      if (staged_ok) {
+        t.ms_staged =
+            time2([&] { spmm_tiled<X>(c, m, B, ldb, sc, (int64_t)k, k, X(1), X(0), s, true); });
+        if (t.ms_staged < best)
+          t.choice = 1;
+      }
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
-      t.choice = t.ms_staged < t.ms_rows ? 1 : 0;
     }
     t.choice_sig = sig;
   }
@@ -111,28 +166,8 @@ void spmm_csr(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
     t.last_path = 1;
     return;
   }
-  spmm_rows<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s);
+  spmm_rows<X>(c, m, B, ldb, C, ldc, k, alpha, beta, t.choice == 2, s);
   t.last_path = 0;
-}
-
-template <class X>
-static void spmm_rows(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64_t ldc,
-                      int k, X alpha, X beta, cudaStream_t s) {
-  constexpr int VMAX = 16 / sizeof(X);
-  const bool aligned = k >= VMAX && ((uintptr_t)B % 16 == 0) && ((uintptr_t)C % 16 == 0) &&
-                       (ldb % VMAX == 0) && (ldc % VMAX == 0);
-  with_vt(c.evt(), [&](auto tag) {
-    using V = typename decltype(tag)::type;
-    if constexpr (std::is_same_v<X, float> && std::is_same_v<V, double>) {
-      throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE, "FP64 storage with FP32 API");
-    } else {
-      if (aligned)
-        launch_spmm_csr<VMAX, V, X>(c, m, B, ldb, C, ldc, k, alpha, beta, s);
-      else
-        launch_spmm_csr<1, V, X>(c, m, B, ldb, C, ldc, k, alpha, beta, s);
-    }
-  });
-  PLS_LAUNCH_CHECK();
 }
 
 // ---------------------------------------------------------------- BSR

@@ -130,13 +130,41 @@ struct MixedRows {
   }
 };
 
+// FP32 BSR seen as scalar rows (the batched kernel's BSR instances), with
+// the block size's log2 when it is a power of two (shifts instead of
+// divisions), else -1.
+struct BsrRows {
+  using V = float;
+  const int32_t *rp, *col;
+  const float *val;
+  int32_t bs, lg_bs, rowmajor;
+  __device__ __forceinline__ int32_t div_bs(int32_t q) const {
+    return lg_bs >= 0 ? q >> lg_bs : q / bs;
+  }
+  __device__ __forceinline__ void range(int64_t r, int32_t &s, int32_t &e, int32_t &aux) const {
+    const int32_t br = div_bs((int32_t)r);
+    aux = (int32_t)r - br * bs;
+    s = __ldg(rp + br) * bs;
+    e = __ldg(rp + br + 1) * bs;
+  }
+  __device__ __forceinline__ void entry(int32_t q, int32_t aux, int32_t &c, float &a,
+                                        const L2Policy &pol) const {
+    const int32_t b = div_bs(q), jj = q - b * bs;
+    c = __ldg(col + b) * bs + jj;
+    a = ld_stream(val + (int64_t)b * bs * bs + (rowmajor ? aux * bs + jj : jj * bs + aux),
+                  pol.stream);
+  }
+};
+
 constexpr int kSpmmInFlight = 4;  // U: nonzeros in flight per lane
 
 // One group's row. Every lane of the warp must call this together (the
 // reduction shuffles over the whole warp); lanes whose row is past the end
 // pass live = false and only take part in the shuffles. TK, TN (as log2)
 // and k are uniform across the warp.
-template <int VEC, int NV, class Acc, class X, class Rows>
+// OFF32: every offset into B and C (row * ld + column) fits in 32 bits, so
+// the address arithmetic stays 32-bit.
+template <int VEC, int NV, class Acc, class X, class Rows, bool OFF32 = false>
 __device__ __forceinline__ void spmm_row_group(const Rows &A, int64_t row, bool live, int lg_tk,
                                                int lg_tn, const X *__restrict__ B, int64_t ldb,
                                                X *__restrict__ C, int64_t ldc, int k, X alpha,
@@ -178,7 +206,8 @@ __device__ __forceinline__ void spmm_row_group(const Rows &A, int64_t row, bool 
 #pragma unroll
         for (int nv = 0; nv < NV; ++nv) {
           const int kk = k0 + (nv * TK + tk) * VEC;
-          const X *bp = B + (int64_t)(c[u] < 0 ? 0 : c[u]) * ldb + kk;
+          const X *bp = OFF32 ? B + ((c[u] < 0 ? 0 : c[u]) * (int32_t)ldb + kk)
+                              : B + (int64_t)(c[u] < 0 ? 0 : c[u]) * ldb + kk;
           if (c[u] >= 0 && kk + VEC <= k) {
             ld_vec<X, VEC>(bp, b[u][nv]);
           } else {
@@ -203,7 +232,7 @@ __device__ __forceinline__ void spmm_row_group(const Rows &A, int64_t row, bool 
         for (int v = 0; v < VEC; ++v)
           acc[nv][v] += __shfl_xor_sync(0xffffffffu, acc[nv][v], o);
     if (live && tn == 0) {
-      X *crow = C + row * ldc;
+      X *crow = OFF32 ? C + (int32_t)row * (int32_t)ldc : C + row * ldc;
 #pragma unroll
       for (int nv = 0; nv < NV; ++nv) {
         const int kk = k0 + (nv * TK + tk) * VEC;
