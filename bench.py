@@ -14,7 +14,8 @@ Reported:
              counted once, SELL padding not counted), summed over ranks;
   e2e        the same metric through the drop-in C call
              perflibs_spmv_exec_d with host (pinned) x and y: H2D of x and
-             D2H of y inside every timed step;
+             D2H of y inside every timed step (y comes back in row bands,
+             each band's copy overlapping the next band's kernels);
   roofline   the dominant kernel's achieved GB/s vs the measured HBM peak;
   cpu_baseline  the reference library (compiled from its own sources,
              OpenMP on all host cores) on the same matrix, same metric.
@@ -368,6 +369,7 @@ def run_b200(args):
         st = lib.perflibs_spmv_exec_d(pls.OPERATION_NOTRANS, 1.0, A.h, xp, 0.0, yp)
         assert st == 0
     e2e_s = max_over_ranks((time.perf_counter() - t0) / Ke, dev)
+    e2e_bands = A.host_bands_used()
 
     hbm, peak_kind = peaks()
     achieved = replica_gbs(bytes_step, ms_tuned * 1e-3, 1)  # per GPU
@@ -404,7 +406,8 @@ def run_b200(args):
         "gflops": 2.0 * nnz / (ms_tuned * 1e-3) / 1e9 * world,
         "selector": selector_arms or None,
         "e2e": {"value": replica_gbs(bytes_step, e2e_s, world), "unit": "GB/s",
-                "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": m * 8, "ms_per_step": e2e_s * 1e3},
+                "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": m * 8, "ms_per_step": e2e_s * 1e3,
+                "row_bands": e2e_bands},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_source": peak_kind,
                      "traffic": load_traffic("c2_spmv_fp64")},

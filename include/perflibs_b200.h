@@ -136,6 +136,20 @@ perflibs_status_t perflibs_b200_spmat_exec_info(perflibs_spmat_t A,
  * 0 row-group kernel, 1 staged kernel whenever it applies. */
 perflibs_status_t perflibs_b200_spmat_set_spmm_path(perflibs_spmat_t A, int32_t path);
 
+/* Host-buffer SpMV (perflibs_spmv_exec_{s,d}) in row bands: the kernels of
+ * band b write rows [r0_b, r1_b) of y, and those rows go back to the host on
+ * a second stream while the later bands compute, so the kernels of all but
+ * the first band hide under the device-to-host copy. Applies to NOTRANS
+ * with CSR or SELL-C-sigma kernels; every row is summed exactly as in one
+ * launch. n_bands = 0 (default) splits results of 8 MB and more into bands
+ * of at least 4 MB, up to 8; 1 turns banding off; 2..64 asks for that many
+ * (SELL bands are whole sort windows, so there may be fewer). */
+perflibs_status_t perflibs_b200_spmat_set_host_bands(perflibs_spmat_t A, int32_t n_bands);
+
+/* Bands the handle's last host-buffer SpMV ran in; 0 when it ran as one
+ * launch. */
+perflibs_status_t perflibs_b200_spmat_host_bands_used(perflibs_spmat_t A, int32_t *n_bands);
+
 /* SpMM plan of the handle: the staged tiles' block height R (0 when none
  * were built: the staged kernel does not apply), the B rows staged per
  * column tile over all blocks and the copy runs; the path the last SpMM

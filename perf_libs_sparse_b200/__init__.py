@@ -111,6 +111,8 @@ def lib():
             "perflibs_b200_spmat_get_error": [vp, vp, vp, vp, i32],
             "perflibs_b200_spmat_spmm_info": [vp, vp, vp, vp, vp, vp, vp],
             "perflibs_b200_spmat_set_spmm_path": [vp, i32],
+            "perflibs_b200_spmat_set_host_bands": [vp, i32],
+            "perflibs_b200_spmat_host_bands_used": [vp, vp],
             "perflibs_b200_read_mtx": [C.c_char_p, vp, vp, vp, vp, vp, vp],
             "perflibs_b200_testing_stage_fault": [i32, i32],
             "perflibs_b200_spmv_exec_d_dev": [i, d, vp, vp, d, vp, vp],
@@ -452,6 +454,16 @@ class SpMat:
         """-1 measured choice (default), 0 row-group kernel, 1 staged kernel."""
         _check(lib().perflibs_b200_spmat_set_spmm_path(self.h, path), "set_spmm_path")
 
+    def set_host_bands(self, n_bands):
+        """Row bands of host-buffer SpMV: 0 by size (default), 1 none, 2..64 that many."""
+        _check(lib().perflibs_b200_spmat_set_host_bands(self.h, n_bands), "set_host_bands")
+
+    def host_bands_used(self):
+        """Bands the last host-buffer SpMV ran in (0 = one launch)."""
+        r = C.c_int32()
+        _check(lib().perflibs_b200_spmat_host_bands_used(self.h, C.byref(r)), "host_bands_used")
+        return r.value
+
     def destroy(self):
         if self.h is not None and self.h.value:
             lib().perflibs_spmat_destroy(self.h)
@@ -507,6 +519,16 @@ class Batch:
         n, l, t = C.c_int64(), C.c_int32(), C.c_int32()
         _check(lib().perflibs_b200_batch_info(self.h, C.byref(n), C.byref(l), C.byref(t)), "batch_info")
         return {"n_items": n.value, "launches": l.value, "tile": t.value}
+
+    def set_host_bands(self, n_bands):
+        """Row bands of host-buffer SpMV: 0 by size (default), 1 none, 2..64 that many."""
+        _check(lib().perflibs_b200_spmat_set_host_bands(self.h, n_bands), "set_host_bands")
+
+    def host_bands_used(self):
+        """Bands the last host-buffer SpMV ran in (0 = one launch)."""
+        r = C.c_int32()
+        _check(lib().perflibs_b200_spmat_host_bands_used(self.h, C.byref(r)), "host_bands_used")
+        return r.value
 
     def destroy(self):
         if self.h is not None and self.h.value:

@@ -744,6 +744,7 @@ int64_t count_blocks(const CsrDev &c, int32_t m, int32_t n, int bs, cudaStream_t
 }
 
 void csr_build_long_rows(CsrDev &c, int32_t m, int threshold, cudaStream_t s) {
+  c.bands.clear();
   c.long_threshold = threshold;
   c.n_long = 0;
   c.long_rows.reserve(sizeof(int32_t) * std::max(m, 1));

@@ -141,6 +141,72 @@ struct SpmvConfig {
 
 // ------------------------------------------------------------ formats
 
+// Rows [r0, r1) of an SpMV run as one band of a host-buffer call: the band's
+// kernels write exactly these rows of y, so the copy of one band's rows to
+// the host overlaps the kernels of the next band. For SELL, [c0, c1) are the
+// band's chunks (whole sort windows), [i0, i1) its column slices and
+// [s0, s1) its sliced chunks in the plan's arrays; for CSR, [i0, i1) are its
+// long rows.
+struct RowBand {
+  int64_t r0 = 0, r1 = 0;
+  int64_t c0 = 0, c1 = 0;
+  int64_t i0 = 0, i1 = 0;
+  int64_t s0 = 0, s1 = 0;
+};
+
+// Bands of one layout, built on the first host-buffer call that uses them.
+// SELL: `order` holds each band's chunks in the layout's processing order
+// (empty when the layout has none); `items` / `splits` the column slices
+// and sliced chunks of the band plan's own, finer slicing (chunks wider than
+// split_w), grouped by band, with their partial sums in `part`. CSR: `order`
+// holds the long rows in increasing order.
+struct BandPlan {
+  int planned = 0;  // band count asked for when built; 0 = not built
+  std::vector<RowBand> bands;
+  DevBuf order, items, splits, part;
+  int32_t split_w = INT32_MAX;
+  void clear() {
+    planned = 0;
+    bands.clear();
+    order.release();
+    items.release();
+    splits.release();
+    part.release();
+    split_w = INT32_MAX;
+  }
+};
+
+// The copy stream and events of banded host-buffer calls, created on first
+// use on the handle's GPU: event i marks the end of band i's kernels on the
+// handle's stream, and the copy stream waits for it before copying the
+// band's rows of y to the host.
+struct BandLanes {
+  cudaStream_t copy = nullptr;
+  std::vector<cudaEvent_t> ev;
+  BandLanes() = default;
+  BandLanes(const BandLanes &) = delete;
+  BandLanes &operator=(const BandLanes &) = delete;
+  ~BandLanes() {
+    for (cudaEvent_t e : ev)
+      cudaEventDestroy(e);
+    if (copy)
+      cudaStreamDestroy(copy);
+  }
+  cudaStream_t copy_stream() {
+    if (!copy)
+      PLS_CUDA(cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking));
+    return copy;
+  }
+  cudaEvent_t event(size_t i) {
+    while (ev.size() <= i) {
+      cudaEvent_t e;
+      PLS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      ev.push_back(e);
+    }
+    return ev[i];
+  }
+};
+
 // A 4-byte flag in mapped pinned host memory: kernels write it through the
 // device pointer, the host reads it without synchronising.
 struct HostFlag {
@@ -221,6 +287,7 @@ struct CsrDev {
   int long_threshold = 0;
   // Staged-SpMM tiles (built on the first suitable SpMM).
   TileDev tiles;
+  BandPlan bands;
 };
 
 struct SellDev {
@@ -243,6 +310,7 @@ struct SellDev {
   // Chunk indices by decreasing width (stable); the SpMV kernel takes chunks
   // in this order. Empty when all chunks have the same width.
   DevBuf order;
+  BandPlan bands;
 };
 
 struct BsrDev {
@@ -332,6 +400,9 @@ struct perflibs_spmat_top_t {
 
   // Staging for host-pointer execution.
   pls::DevBuf xbuf, ybuf;
+  pls::BandLanes lanes;
+  int host_bands = 0;       // row bands of host-buffer SpMV: 0 = by size, 1 = none
+  int last_host_bands = 0;  // bands the last host-buffer SpMV ran in (0 = one launch)
 };
 
 namespace pls {
@@ -362,6 +433,17 @@ void *noalloc_scratch_address(int device);
 template <class X>
 void spmv_sell_scratch(const SellDev &s, const X *x, X *y, X alpha, X beta,
                        void *scratch, int64_t capacity, cudaStream_t st);
+// Row bands for host-buffer SpMV: plan about n_bands bands of equal row
+// count (kept when already planned for n_bands), then run one band.
+void sell_plan_bands(SellDev &s, int64_t m, int n_bands);
+void csr_plan_bands(CsrDev &c, int32_t m, int n_bands);
+template <class X>
+void spmv_sell_band(const SellDev &s, const RowBand &b, const X *x, X *y, X alpha, X beta,
+                    cudaStream_t st);
+// tpr = 0 runs the long-row split kernels (threshold c.long_threshold).
+template <class X>
+void spmv_csr_band(const CsrDev &c, const RowBand &b, int tpr, const X *x, X *y, X alpha,
+                   X beta, cudaStream_t s);
 template <class X>
 void spmv_csr_trans(const CsrDev &c, int32_t m, int32_t n, const X *x, X *y,
                     X alpha, X beta, cudaStream_t s);

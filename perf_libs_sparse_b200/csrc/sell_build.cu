@@ -408,6 +408,7 @@ int64_t sell_padded_size(const CsrDev &c, int32_t m, int C, int sigma, cudaStrea
 // groups; the other chunks stay one lane group each. Slices are ordered by
 // decreasing chunk width so the longest work starts first.
 void sell_build_work_list(SellDev &S, int slice_w, cudaStream_t st) {
+  S.bands.clear();
   S.items.release();
   S.split_chunks.release();
   S.part.release();

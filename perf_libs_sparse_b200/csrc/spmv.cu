@@ -9,6 +9,7 @@
 //     result depends only on that row (no atomics on the NOTRANS path);
 //   * grids launch one thread group per row / chunk and let the block
 //     scheduler balance uneven rows across the 148 SMs.
+#include <algorithm>
 #include <mutex>
 
 #include "common.cuh"
@@ -107,28 +108,42 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Rows [r0, r0 + m): row_ptr holds absolute offsets, so the kernel sees the
+// row pointers and y from r0 on.
 template <int TPR, class V, class X>
-static void launch_csr_vector(const CsrDev &c, int32_t m, const X *x, X *y,
+static void launch_csr_vector(const CsrDev &c, int64_t r0, int32_t m, const X *x, X *y,
                               X alpha, X beta, int32_t skip, cudaStream_t s) {
   const int64_t threads = (int64_t)m * TPR;
   const int64_t blocks = div_up(threads, 256);
   k_csr_vector<TPR, V, X><<<(unsigned)blocks, 256, 0, s>>>(
-      m, c.row_ptr.as<int32_t>(), c.col.as<int32_t>(), (const V *)c.ev(), x, y,
+      m, c.row_ptr.as<int32_t>() + r0, c.col.as<int32_t>(), (const V *)c.ev(), x, y + r0,
       alpha, beta, beta != X(0), skip);
 }
 
 template <class V, class X>
-static void csr_vector_dispatch(const CsrDev &c, int32_t m, int tpr,
+static void csr_vector_dispatch(const CsrDev &c, int64_t r0, int32_t m, int tpr,
                                 const X *x, X *y, X alpha, X beta,
                                 int32_t skip, cudaStream_t s) {
   switch (tpr) {
-  case 1: launch_csr_vector<1, V>(c, m, x, y, alpha, beta, skip, s); break;
-  case 2: launch_csr_vector<2, V>(c, m, x, y, alpha, beta, skip, s); break;
-  case 4: launch_csr_vector<4, V>(c, m, x, y, alpha, beta, skip, s); break;
-  case 8: launch_csr_vector<8, V>(c, m, x, y, alpha, beta, skip, s); break;
-  case 16: launch_csr_vector<16, V>(c, m, x, y, alpha, beta, skip, s); break;
-  default: launch_csr_vector<32, V>(c, m, x, y, alpha, beta, skip, s); break;
+  case 1: launch_csr_vector<1, V>(c, r0, m, x, y, alpha, beta, skip, s); break;
+  case 2: launch_csr_vector<2, V>(c, r0, m, x, y, alpha, beta, skip, s); break;
+  case 4: launch_csr_vector<4, V>(c, r0, m, x, y, alpha, beta, skip, s); break;
+  case 8: launch_csr_vector<8, V>(c, r0, m, x, y, alpha, beta, skip, s); break;
+  case 16: launch_csr_vector<16, V>(c, r0, m, x, y, alpha, beta, skip, s); break;
+  default: launch_csr_vector<32, V>(c, r0, m, x, y, alpha, beta, skip, s); break;
   }
+}
+
+// Lanes per row of the vector kernel beside the long-row kernel: rows up to
+// the threshold take 4 lanes up to 64 entries, then 8, 16 and 32.
+static int split_tpr(int32_t threshold) {
+  if (threshold <= 64)
+    return 4;
+  if (threshold <= 256)
+    return 8;
+  if (threshold <= 1024)
+    return 16;
+  return 32;
 }
 
 template <class X>
@@ -141,7 +156,7 @@ void spmv_csr(const CsrDev &c, int32_t m, int tpr, const X *x, X *y, X alpha,
     if constexpr (std::is_same_v<X, float> && std::is_same_v<V, double>)
       throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE, "FP64 storage with FP32 API");
     else
-      csr_vector_dispatch<V, X>(c, m, tpr, x, y, alpha, beta, 0, s);
+      csr_vector_dispatch<V, X>(c, 0, m, tpr, x, y, alpha, beta, 0, s);
   });
   PLS_LAUNCH_CHECK();
 }
@@ -157,12 +172,8 @@ void spmv_csr_split(const CsrDev &c, int32_t m, const X *x, X *y, X alpha,
     if constexpr (std::is_same_v<X, float> && std::is_same_v<V, double>) {
       throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE, "FP64 storage with FP32 API");
     } else {
-      int tpr = 32;
-      int32_t thr = c.long_threshold;
-      if (thr <= 64) tpr = 4;
-      else if (thr <= 256) tpr = 8;
-      else if (thr <= 1024) tpr = 16;
-      csr_vector_dispatch<V, X>(c, m, tpr, x, y, alpha, beta, thr, s);
+      const int32_t thr = c.long_threshold;
+      csr_vector_dispatch<V, X>(c, 0, m, split_tpr(thr), x, y, alpha, beta, thr, s);
       if (c.n_long > 0)
         k_csr_long<V, X><<<c.n_long, 256, 0, s>>>(
             c.long_rows.as<int32_t>(), c.row_ptr.as<int32_t>(),
@@ -228,12 +239,12 @@ __device__ __forceinline__ typename AccOf<V, X>::type sell_row_sum(const V *vp, 
 // blocks take one chunk per C lanes (lane r = row r of the chunk, so the C
 // lanes read C consecutive values per column: a full 256-byte line for
 // C = 32, FP64) and skip the chunks the slices cover; they take the chunks in
-// `order` (decreasing width, or natural order when null). Slices come first,
+// `order` (decreasing width, or c_base onwards when null). Slices come first,
 // then the widest chunks, so the longest work starts earliest and the launch
 // ends on the narrowest chunks.
 template <int C, class V, class O, class X>
 __global__ void __launch_bounds__(kSellThreads, 10)
-    k_sell(int64_t nC, int32_t split_w, int64_t n_items, int64_t slice_blocks,
+    k_sell(int64_t nC, int64_t c_base, int32_t split_w, int64_t n_items, int64_t slice_blocks,
            const int4 *__restrict__ items, const int32_t *__restrict__ order,
            const int64_t *__restrict__ cs,
            const int32_t *__restrict__ cl, const int32_t *__restrict__ cmin,
@@ -259,7 +270,7 @@ __global__ void __launch_bounds__(kSellThreads, 10)
   const int64_t ci = t / C;
   if (ci >= nC)
     return;
-  const int64_t c = order ? (int64_t)__ldg(order + ci) : ci;
+  const int64_t c = order ? (int64_t)__ldg(order + ci) : c_base + ci;
   const int r = (int)(t % C);
   const int32_t w = __ldg(cl + c);
   if (w > split_w)
@@ -294,44 +305,72 @@ __global__ void k_sell_combine(int64_t n_split, const int4 *__restrict__ split,
     store_y(y, dst, acc, alpha, beta, beta_nz);
 }
 
+// What one k_sell launch covers: n_chunks chunks (order[0, n_chunks), or
+// c_base onwards when order is null), n_items column slices and n_split
+// sliced chunks.
+struct SellWork {
+  int64_t n_chunks = 0, c_base = 0;
+  int32_t split_w = INT32_MAX;  // wider chunks are covered by the slices
+  const int32_t *order = nullptr;
+  int64_t n_items = 0;
+  const int4 *items = nullptr;
+  int64_t n_split = 0;
+  const int4 *splits = nullptr;
+  void *part = nullptr;  // partial sums of the slices (scratch)
+};
+
+static SellWork whole_work(const SellDev &s) {
+  SellWork w;
+  w.n_chunks = s.nC;
+  w.order = s.order.as<int32_t>();
+  w.part = s.part.p;
+  if (s.n_split > 0)
+    w.split_w = s.split_w;
+  if (s.n_items > 0 && s.n_split > 0) {
+    w.n_items = s.n_items;
+    w.items = s.items.as<int4>();
+    w.n_split = s.n_split;
+    w.splits = s.split_chunks.as<int4>();
+  }
+  return w;
+}
+
 template <int C, class V, class O, class X>
-static void launch_sell(const SellDev &s, const X *x, X *y, X alpha, X beta,
-                        cudaStream_t st) {
+static void launch_sell(const SellDev &s, const SellWork &w, const X *x, X *y, X alpha,
+                        X beta, cudaStream_t st) {
   using Acc = typename AccOf<V, X>::type;
   const int bnz = beta != X(0);
-  const bool sliced = s.n_items > 0 && s.n_split > 0;
-  const int64_t slice_blocks = sliced ? div_up(s.n_items * C, kSellThreads) : 0;
-  const int64_t chunk_blocks = div_up(s.nC * C, kSellThreads);
+  const int64_t slice_blocks = w.n_items > 0 ? div_up(w.n_items * C, kSellThreads) : 0;
+  const int64_t chunk_blocks = div_up(w.n_chunks * C, kSellThreads);
   if (slice_blocks + chunk_blocks == 0)
     return;
-  Acc *part = sliced ? (Acc *)s.part.p : nullptr;  // partial sums (scratch)
+  Acc *part = (Acc *)w.part;
   k_sell<C, V, O, X><<<(unsigned)(slice_blocks + chunk_blocks), kSellThreads, 0, st>>>(
-      s.nC, sliced ? s.split_w : INT32_MAX, sliced ? s.n_items : 0, slice_blocks,
-      s.items.as<int4>(), s.order.as<int32_t>(), s.cs.as<int64_t>(), s.cl.as<int32_t>(),
-      s.col_min.as<int32_t>(),
+      w.n_chunks, w.c_base, w.split_w, w.n_items, slice_blocks,
+      w.items, w.order, s.cs.as<int64_t>(), s.cl.as<int32_t>(), s.col_min.as<int32_t>(),
       s.permd2in.as<int32_t>(), s.vals.as<V>(), s.offsets.as<O>(), x, y, part, alpha, beta, bnz);
-  if (sliced) {
-    const int64_t b2 = div_up(s.n_split * C, 256);
+  if (w.n_split > 0) {
+    const int64_t b2 = div_up(w.n_split * C, 256);
     k_sell_combine<C, Acc, X><<<(unsigned)b2, 256, 0, st>>>(
-        s.n_split, s.split_chunks.as<int4>(), s.permd2in.as<int32_t>(), part, y, alpha, beta, bnz);
+        w.n_split, w.splits, s.permd2in.as<int32_t>(), part, y, alpha, beta, bnz);
   }
 }
 
 template <int C, class V, class X>
-static void sell_by_width(const SellDev &s, const X *x, X *y, X alpha, X beta,
-                          cudaStream_t st) {
+static void sell_by_width(const SellDev &s, const SellWork &w, const X *x, X *y, X alpha,
+                          X beta, cudaStream_t st) {
   switch (s.col_bytes) {
-  case 1: launch_sell<C, V, uint8_t, X>(s, x, y, alpha, beta, st); break;
-  case 2: launch_sell<C, V, uint16_t, X>(s, x, y, alpha, beta, st); break;
-  case 4: launch_sell<C, V, uint32_t, X>(s, x, y, alpha, beta, st); break;
+  case 1: launch_sell<C, V, uint8_t, X>(s, w, x, y, alpha, beta, st); break;
+  case 2: launch_sell<C, V, uint16_t, X>(s, w, x, y, alpha, beta, st); break;
+  case 4: launch_sell<C, V, uint32_t, X>(s, w, x, y, alpha, beta, st); break;
   default:
     throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE, "unsupported SELL offset width");
   }
 }
 
 template <class X>
-void spmv_sell(const SellDev &s, const X *x, X *y, X alpha, X beta,
-               cudaStream_t st) {
+static void run_sell(const SellDev &s, const SellWork &w, const X *x, X *y, X alpha, X beta,
+                     cudaStream_t st) {
   if (s.nC == 0)
     return;
   with_vt(s.vt, [&](auto tag) {
@@ -340,12 +379,192 @@ void spmv_sell(const SellDev &s, const X *x, X *y, X alpha, X beta,
       throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE, "FP64 storage with FP32 API");
     } else {
       switch (s.C) {
-      case 8: sell_by_width<8, V, X>(s, x, y, alpha, beta, st); break;
-      case 16: sell_by_width<16, V, X>(s, x, y, alpha, beta, st); break;
-      case 32: sell_by_width<32, V, X>(s, x, y, alpha, beta, st); break;
+      case 8: sell_by_width<8, V, X>(s, w, x, y, alpha, beta, st); break;
+      case 16: sell_by_width<16, V, X>(s, w, x, y, alpha, beta, st); break;
+      case 32: sell_by_width<32, V, X>(s, w, x, y, alpha, beta, st); break;
       default:
         throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE, "SELL chunk height must be 8, 16 or 32");
       }
+    }
+  });
+  PLS_LAUNCH_CHECK();
+}
+
+template <class X>
+void spmv_sell(const SellDev &s, const X *x, X *y, X alpha, X beta,
+               cudaStream_t st) {
+  run_sell<X>(s, whole_work(s), x, y, alpha, beta, st);
+}
+
+// ------------------------------------------ row bands (host-buffer calls)
+
+template <class T>
+static std::vector<T> to_host(const DevBuf &b, int64_t n) {
+  std::vector<T> h((size_t)n);
+  if (n > 0)
+    PLS_CUDA(cudaMemcpy(h.data(), b.p, sizeof(T) * (size_t)n, cudaMemcpyDeviceToHost));
+  return h;
+}
+
+template <class T>
+static void to_device(DevBuf &b, const std::vector<T> &h) {
+  b.reserve(sizeof(T) * std::max<size_t>(h.size(), 1));
+  if (!h.empty())
+    PLS_CUDA(cudaMemcpy(b.p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+}
+
+// Stable grouping of `v` by band: band b's elements keep their order and
+// land in [first[b], first[b + 1]).
+template <class T, class F>
+static std::vector<T> group_by_band(const std::vector<T> &v, size_t n_bands, F band_of,
+                                    std::vector<int64_t> &first) {
+  first.assign(n_bands + 1, 0);
+  for (const T &e : v)
+    first[band_of(e) + 1]++;
+  for (size_t b = 0; b < n_bands; ++b)
+    first[b + 1] += first[b];
+  std::vector<int64_t> at(first.begin(), first.end() - 1);
+  std::vector<T> out(v.size());
+  for (const T &e : v)
+    out[(size_t)at[band_of(e)]++] = e;
+  return out;
+}
+
+// A band is a run of whole sort windows (sigma rows; C rows without
+// sorting), so the permutation keeps its rows inside it and its chunks
+// [c0, c1) write exactly the rows [c0*C, c1*C) of y. Inside a band the
+// chunks keep the layout's processing order (widest first for power-law
+// layouts). A band's launch lasts at least as long as one lane group's walk
+// along its widest unsliced chunk, a floor that a whole-matrix launch hides
+// under other work but a band of a few tens of microseconds does not; so the
+// plan slices every chunk wider than 2 * kBandSliceW columns into slices of
+// kBandSliceW, widest chunks first within each band.
+constexpr int32_t kBandSliceW = 32;
+
+void sell_plan_bands(SellDev &s, int64_t m, int n_bands) {
+  if (s.bands.planned == n_bands)
+    return;
+  s.bands.clear();
+  s.bands.planned = n_bands;
+  if (s.nC == 0 || n_bands < 1)
+    return;
+  const int64_t window = (s.sigma > 0 ? s.sigma : s.C) / s.C;  // chunks
+  const int64_t per = div_up(div_up(s.nC, window), (int64_t)n_bands) * window;
+  std::vector<RowBand> bands;
+  for (int64_t c0 = 0; c0 < s.nC; c0 += per) {
+    RowBand b;
+    b.c0 = c0;
+    b.c1 = std::min(s.nC, c0 + per);
+    b.r0 = c0 * s.C;
+    b.r1 = std::min(m, b.c1 * s.C);
+    bands.push_back(b);
+  }
+  const size_t nb = bands.size();
+  const auto band_of = [&](int64_t c) { return (size_t)(c / per); };
+  std::vector<int64_t> first;
+  if (s.order.p) {
+    const auto ord = group_by_band(to_host<int32_t>(s.order, s.nC), nb,
+                                   [&](int32_t c) { return band_of(c); }, first);
+    to_device(s.bands.order, ord);
+  }
+  const std::vector<int32_t> cl = to_host<int32_t>(s.cl, s.nC);
+  std::vector<int32_t> wide;
+  for (int64_t c = 0; c < s.nC; ++c)
+    if (cl[c] > 2 * kBandSliceW)
+      wide.push_back((int32_t)c);
+  if (!wide.empty()) {
+    std::stable_sort(wide.begin(), wide.end(),
+                     [&](int32_t a, int32_t b) { return cl[a] > cl[b]; });
+    wide = group_by_band(wide, nb, [&](int32_t c) { return band_of(c); }, first);
+    std::vector<int4> items, splits;
+    int32_t slot = 0;
+    for (size_t b = 0; b < nb; ++b) {
+      bands[b].i0 = (int64_t)items.size();
+      bands[b].s0 = (int64_t)splits.size();
+      for (int64_t k = first[b]; k < first[b + 1]; ++k) {
+        const int32_t c = wide[(size_t)k];
+        const int32_t ns = (int32_t)div_up(cl[c], kBandSliceW);
+        splits.push_back(make_int4(c, slot, ns, 0));
+        for (int32_t q = 0; q < ns; ++q)
+          items.push_back(make_int4(c, q * kBandSliceW,
+                                    std::min(cl[c], (q + 1) * kBandSliceW), slot + q));
+        slot += ns;
+      }
+      bands[b].i1 = (int64_t)items.size();
+      bands[b].s1 = (int64_t)splits.size();
+    }
+    to_device(s.bands.items, items);
+    to_device(s.bands.splits, splits);
+    s.bands.part.reserve(sizeof(double) * (size_t)slot * s.C);  // FP64 covers both accumulators
+    s.bands.split_w = 2 * kBandSliceW;
+  }
+  s.bands.bands = std::move(bands);
+}
+
+template <class X>
+void spmv_sell_band(const SellDev &s, const RowBand &b, const X *x, X *y, X alpha, X beta,
+                    cudaStream_t st) {
+  SellWork w;
+  w.n_chunks = b.c1 - b.c0;
+  w.c_base = b.c0;
+  w.split_w = s.bands.split_w;
+  w.order = s.bands.order.p ? s.bands.order.as<int32_t>() + b.c0 : nullptr;
+  w.n_items = b.i1 - b.i0;
+  w.items = s.bands.items.p ? s.bands.items.as<int4>() + b.i0 : nullptr;
+  w.n_split = b.s1 - b.s0;
+  w.splits = s.bands.splits.p ? s.bands.splits.as<int4>() + b.s0 : nullptr;
+  w.part = s.bands.part.p;
+  run_sell<X>(s, w, x, y, alpha, beta, st);
+}
+
+// CSR bands: equal row counts; the long rows (when the split kernels are
+// configured) sorted so that each band's are a contiguous run.
+void csr_plan_bands(CsrDev &c, int32_t m, int n_bands) {
+  if (c.bands.planned == n_bands)
+    return;
+  c.bands.clear();
+  c.bands.planned = n_bands;
+  if (m == 0 || n_bands < 1)
+    return;
+  const int64_t per = div_up((int64_t)m, (int64_t)n_bands);
+  std::vector<RowBand> bands;
+  for (int64_t r0 = 0; r0 < m; r0 += per) {
+    RowBand b;
+    b.r0 = r0;
+    b.r1 = std::min<int64_t>(m, r0 + per);
+    bands.push_back(b);
+  }
+  if (c.n_long > 0) {
+    std::vector<int32_t> rows = to_host<int32_t>(c.long_rows, c.n_long);
+    std::sort(rows.begin(), rows.end());
+    for (RowBand &b : bands) {
+      b.i0 = std::lower_bound(rows.begin(), rows.end(), (int32_t)b.r0) - rows.begin();
+      b.i1 = std::lower_bound(rows.begin(), rows.end(), (int32_t)b.r1) - rows.begin();
+    }
+    to_device(c.bands.order, rows);
+  }
+  c.bands.bands = std::move(bands);
+}
+
+template <class X>
+void spmv_csr_band(const CsrDev &c, const RowBand &b, int tpr, const X *x, X *y, X alpha,
+                   X beta, cudaStream_t s) {
+  const int32_t mb = (int32_t)(b.r1 - b.r0);
+  if (mb == 0)
+    return;
+  with_vt(c.evt(), [&](auto tag) {
+    using V = typename decltype(tag)::type;
+    if constexpr (std::is_same_v<X, float> && std::is_same_v<V, double>) {
+      throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE, "FP64 storage with FP32 API");
+    } else if (tpr > 0) {
+      csr_vector_dispatch<V, X>(c, b.r0, mb, tpr, x, y, alpha, beta, 0, s);
+    } else {
+      const int32_t thr = c.long_threshold;
+      csr_vector_dispatch<V, X>(c, b.r0, mb, split_tpr(thr), x, y, alpha, beta, thr, s);
+      if (b.i1 > b.i0)
+        k_csr_long<V, X><<<(unsigned)(b.i1 - b.i0), 256, 0, s>>>(
+            c.bands.order.as<int32_t>() + b.i0, c.row_ptr.as<int32_t>(), c.col.as<int32_t>(),
+            (const V *)c.ev(), x, y, alpha, beta, beta != X(0));
     }
   });
   PLS_LAUNCH_CHECK();
@@ -400,36 +619,9 @@ void spmv_sell_scratch(const SellDev &s, const X *x, X *y, X alpha, X beta, void
     throw Error(PERFLIBS_STATUS_INPUT_PARAMETER_ERROR,
                 "this matrix needs " + std::to_string(slots * s.C) +
                     " scratch elements; the fixed scratch holds " + std::to_string(capacity));
-  SellDev view;  // the handle's layout, partial sums redirected to `scratch`
-  view.C = s.C;
-  view.nC = s.nC;
-  view.col_bytes = s.col_bytes;
-  view.vt = s.vt;
-  view.n_items = s.n_items;
-  view.n_split = s.n_split;
-  view.split_w = s.split_w;
-  view.cs.p = s.cs.p;
-  view.cl.p = s.cl.p;
-  view.col_min.p = s.col_min.p;
-  view.permd2in.p = s.permd2in.p;
-  view.vals.p = s.vals.p;
-  view.offsets.p = s.offsets.p;
-  view.items.p = s.items.p;
-  view.split_chunks.p = s.split_chunks.p;
-  view.part.p = scratch;
-  view.order.p = s.order.p;
-  try {
-    spmv_sell<X>(view, x, y, alpha, beta, st);
-  } catch (...) {
-    // `view` borrows every pointer: release nothing.
-    view.cs.p = view.cl.p = view.col_min.p = view.permd2in.p = nullptr;
-    view.vals.p = view.offsets.p = view.items.p = view.split_chunks.p = view.part.p = nullptr;
-    view.order.p = nullptr;
-    throw;
-  }
-  view.cs.p = view.cl.p = view.col_min.p = view.permd2in.p = nullptr;
-  view.vals.p = view.offsets.p = view.items.p = view.split_chunks.p = view.part.p = nullptr;
-  view.order.p = nullptr;
+  SellWork w = whole_work(s);
+  w.part = scratch;
+  run_sell<X>(s, w, x, y, alpha, beta, st);
 }
 
 template void spmv_sell_scratch<double>(const SellDev &, const double *, double *, double,
@@ -659,6 +851,10 @@ void spmv_bsr(const BsrDev &b, const X *x, X *y, X alpha, X beta,
                                   X, cudaStream_t);                            \
   template void spmv_sell<X>(const SellDev &, const X *, X *, X, X,           \
                              cudaStream_t);                                    \
+  template void spmv_sell_band<X>(const SellDev &, const RowBand &, const X *, \
+                                  X *, X, X, cudaStream_t);                    \
+  template void spmv_csr_band<X>(const CsrDev &, const RowBand &, int,         \
+                                 const X *, X *, X, X, cudaStream_t);          \
   template void spmv_bsr<X>(const BsrDev &, const X *, X *, X, X,             \
                             cudaStream_t);                                     \
   template void spmv_csr_trans<X>(const CsrDev &, int32_t, int32_t,           \

@@ -293,6 +293,64 @@ def test_device_pointer_exec_on_torch_stream():
     assert rel_err_rows(yd.cpu().numpy(), yref, scale_of(rp, c, v, x, 1, 0, None)).max() <= FP64_TOL
 
 
+@pytest.fixture(scope="module")
+def zipf_large():
+    m, n, rp, c, v = W.zipf_rows(2_500_011, seed=21)
+    rng = np.random.default_rng(22)
+    return m, n, rp, c, v, W.uniform_vector(n, 23), rng.uniform(-1, 1, m)
+
+
+@pytest.mark.parametrize("cfg", [(pls.KIND_SELL, 32, 4096, 0), (pls.KIND_SELL, 16, 48, 0),
+                                 (pls.KIND_SELL, 8, 0, 0), (pls.KIND_CSR, 0, 0, 4),
+                                 (pls.KIND_CSR_SPLIT, 0, 0, 256)])
+def test_host_exec_in_row_bands(zipf_large, cfg):
+    """Host-buffer calls with a y of 20 MB run in row bands, each band's rows
+    copied back while the next computes. Without bands the host call is the
+    device path bit for bit; with them, rows of chunks the band plan slices
+    more finely are summed in another order, within the FP64 tolerance."""
+    import torch
+
+    m, n, rp, c, v, x, y0 = zipf_large
+    A = pls.SpMat.csr(m, n, rp, c, v)
+    assert A.force_config(*cfg) == 0
+    assert A.optimize() == 0
+    for alpha, beta in ((1.0, 0.0), (-0.75, 1.5)):
+        yref = oracle.csr_spmv(rp, c, v, x, y=y0, alpha=alpha, beta=beta)
+        sc = scale_of(rp, c, v, x, alpha, beta, y0)
+        A.set_host_bands(0)
+        yb = A.spmv(x, y0.copy(), alpha=alpha, beta=beta)
+        assert A.host_bands_used() == 4, cfg
+        assert rel_err_rows(yb, yref, sc).max() <= FP64_TOL
+        A.set_host_bands(1)
+        y1 = A.spmv(x, y0.copy(), alpha=alpha, beta=beta)
+        assert A.host_bands_used() == 0
+        xd = torch.tensor(x, device="cuda")
+        yd = torch.tensor(y0, device="cuda")
+        torch.cuda.synchronize()
+        A.spmv_dev(xd.data_ptr(), yd.data_ptr(), alpha, beta)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(y1, yd.cpu().numpy())
+        for nb in (2, 7, 64):
+            A.set_host_bands(nb)
+            y = A.spmv(x, y0.copy(), alpha=alpha, beta=beta)
+            assert 2 <= A.host_bands_used() <= nb
+            assert rel_err_rows(y, yref, sc).max() <= FP64_TOL, (cfg, nb)
+    A.destroy()
+
+
+def test_host_exec_in_row_bands_fp32():
+    m, n, rp, c, v = W.zipf_rows(2_200_003, seed=24)
+    x = W.uniform_vector(n, 25).astype(np.float32)
+    A = pls.SpMat.csr(m, n, rp, c, v.astype(np.float32))
+    assert A.force_config(pls.KIND_SELL, 32, 1024, 0) == 0
+    assert A.optimize() == 0
+    y = A.spmv(x)
+    yref = oracle.csr_spmv(rp, c, v, x.astype(np.float64))
+    sc = scale_of(rp, c, v, x.astype(np.float64), 1.0, 0.0, None)
+    assert rel_err_rows(y.astype(np.float64), yref, sc).max() <= 1e-5
+    A.destroy()
+
+
 # ------------------------------------------------------- reduced precision
 
 
