@@ -1700,8 +1700,7 @@ perflibs_status_t perflibs_b200_spmv_exec_d_noalloc(double alpha, perflibs_spmat
       scal<double>(A->m, beta, y, s);
       return PERFLIBS_STATUS_SUCCESS;
     }
-    spmv_sell_scratch<double>(A->sell, x, y, alpha, beta, noalloc_scratch_address(A->device),
-                              noalloc_scratch_capacity(), s);
+    spmv_sell_noalloc(A->sell, x, y, alpha, beta, A->device, s);
     return PERFLIBS_STATUS_SUCCESS;
   });
 }
@@ -1814,9 +1813,7 @@ perflibs_status_t perflibs_b200_spmat_exec_info(perflibs_spmat_t A, int32_t *ker
   if (!A)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
   int32_t k = 1;
-  if (A->fmt == Fmt::SELL)
-    k = (A->sell.n_items > 0 && A->sell.n_split > 0) ? 2 : 1;
-  else if (A->fmt == Fmt::CSR && A->cfg.kind == Kind::CSR_SPLIT)
+  if (A->fmt == Fmt::CSR && A->cfg.kind == Kind::CSR_SPLIT)
     k = A->csr.n_long > 0 ? 2 : 1;
   if (kernels_per_spmv)
     *kernels_per_spmv = k;

@@ -144,34 +144,32 @@ struct SpmvConfig {
 // Rows [r0, r1) of an SpMV run as one band of a host-buffer call: the band's
 // kernels write exactly these rows of y, so the copy of one band's rows to
 // the host overlaps the kernels of the next band. For SELL, [c0, c1) are the
-// band's chunks (whole sort windows), [i0, i1) its column slices and
-// [s0, s1) its sliced chunks in the plan's arrays; for CSR, [i0, i1) are its
-// long rows.
+// band's chunks (whole sort windows) and [i0, i1) its column slices in the
+// plan's arrays; for CSR, [i0, i1) are its long rows.
 struct RowBand {
   int64_t r0 = 0, r1 = 0;
   int64_t c0 = 0, c1 = 0;
   int64_t i0 = 0, i1 = 0;
-  int64_t s0 = 0, s1 = 0;
 };
 
 // Bands of one layout, built on the first host-buffer call that uses them.
 // SELL: `order` holds each band's chunks in the layout's processing order
-// (empty when the layout has none); `items` / `splits` the column slices
-// and sliced chunks of the band plan's own, finer slicing (chunks wider than
-// split_w), grouped by band, with their partial sums in `part`. CSR: `order`
-// holds the long rows in increasing order.
+// (empty when the layout has none); `items` the column slices of the band
+// plan's own, finer slicing (chunks wider than split_w), grouped by band,
+// with their partial sums in `part` and completion counts in `done`. CSR:
+// `order` holds the long rows in increasing order.
 struct BandPlan {
   int planned = 0;  // band count asked for when built; 0 = not built
   std::vector<RowBand> bands;
-  DevBuf order, items, splits, part;
+  DevBuf order, items, part, done;
   int32_t split_w = INT32_MAX;
   void clear() {
     planned = 0;
     bands.clear();
     order.release();
     items.release();
-    splits.release();
     part.release();
+    done.release();
     split_w = INT32_MAX;
   }
 };
@@ -304,9 +302,9 @@ struct SellDev {
   int64_t n_items = 0;
   int slice_w = 0;
   int32_t split_w = INT32_MAX;
-  DevBuf split_chunks;  // (chunk, first slot, slice count) per split chunk
-  int64_t n_split = 0;
+  int64_t n_split = 0;  // chunks split into slices
   DevBuf part;          // partial sums of the split chunks' slices (scratch)
+  DevBuf done;          // per slot: slices of its chunk finished (0 between launches)
   // Chunk indices by decreasing width (stable); the SpMV kernel takes chunks
   // in this order. Empty when all chunks have the same width.
   DevBuf order;
@@ -426,13 +424,10 @@ void spmv_sell(const SellDev &s, const X *x, X *y, X alpha, X beta,
 template <class X>
 void spmv_bsr(const BsrDev &b, const X *x, X *y, X alpha, X beta,
               cudaStream_t s);
-// Allocation-free variant of spmv_sell: partial sums in a fixed device
-// array (see spmv.cu).
-int64_t noalloc_scratch_capacity();
-void *noalloc_scratch_address(int device);
-template <class X>
-void spmv_sell_scratch(const SellDev &s, const X *x, X *y, X alpha, X beta,
-                       void *scratch, int64_t capacity, cudaStream_t st);
+// Allocation-free FP64 variant of spmv_sell: the slices' partial sums and
+// completion counts in fixed device arrays (see spmv.cu).
+void spmv_sell_noalloc(const SellDev &s, const double *x, double *y, double alpha, double beta,
+                       int device, cudaStream_t st);
 // Row bands for host-buffer SpMV: plan about n_bands bands of equal row
 // count (kept when already planned for n_bands), then run one band.
 void sell_plan_bands(SellDev &s, int64_t m, int n_bands);

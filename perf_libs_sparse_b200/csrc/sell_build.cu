@@ -410,8 +410,8 @@ int64_t sell_padded_size(const CsrDev &c, int32_t m, int C, int sigma, cudaStrea
 void sell_build_work_list(SellDev &S, int slice_w, cudaStream_t st) {
   S.bands.clear();
   S.items.release();
-  S.split_chunks.release();
   S.part.release();
+  S.done.release();
   S.n_items = 0;
   S.n_split = 0;
   S.slice_w = 0;
@@ -426,29 +426,28 @@ void sell_build_work_list(SellDev &S, int slice_w, cudaStream_t st) {
       wide.push_back(c);
   std::stable_sort(wide.begin(), wide.end(),
                    [&](int64_t a, int64_t b) { return cl[a] > cl[b]; });
-  std::vector<int4> items, splits;
+  std::vector<int4> items;
   int32_t slot = 0;
   for (int64_t c : wide) {
     const int32_t w = cl[c];
     const int32_t ns = (int32_t)div_up(w, slice_w);
-    splits.push_back(make_int4((int)c, slot, ns, 0));
     for (int32_t q = 0; q < ns; ++q)
       items.push_back(make_int4((int)c, q * slice_w, std::min(w, (q + 1) * slice_w), slot + q));
     slot += ns;
   }
   S.n_items = (int64_t)items.size();
-  S.n_split = (int64_t)splits.size();
+  S.n_split = (int64_t)wide.size();
   S.slice_w = slice_w;
   S.split_w = 2 * slice_w;
   S.items.reserve(sizeof(int4) * items.size());
   PLS_CUDA(cudaMemcpyAsync(S.items.p, items.data(), sizeof(int4) * items.size(),
                            cudaMemcpyHostToDevice, st));
-  S.split_chunks.reserve(sizeof(int4) * splits.size());
-  PLS_CUDA(cudaMemcpyAsync(S.split_chunks.p, splits.data(), sizeof(int4) * splits.size(),
-                           cudaMemcpyHostToDevice, st));
   // Partial sums: one accumulator per (slot, row); FP64 covers both
-  // accumulator types.
+  // accumulator types. Completion counts: one per slot (the chunk's first
+  // slot counts its slices), zero between launches.
   S.part.reserve(sizeof(double) * (size_t)slot * S.C);
+  S.done.reserve(sizeof(int32_t) * (size_t)slot);
+  PLS_CUDA(cudaMemsetAsync(S.done.p, 0, sizeof(int32_t) * (size_t)slot, st));
   PLS_CUDA(cudaStreamSynchronize(st));
 }
 

@@ -235,35 +235,71 @@ __device__ __forceinline__ typename AccOf<V, X>::type sell_row_sum(const V *vp, 
 
 // One launch, two kinds of blocks. Blocks [0, slice_blocks) take column
 // slices of the few chunks wider than split_w (power-law tails): item =
-// (chunk, j0, j1, slot), partial sum to part[slot*C + r]. The remaining
+// (chunk, j0, j1, slot), slices of slice_w columns, the slices of one chunk
+// in consecutive slots from first = slot - j0 / slice_w. The remaining
 // blocks take one chunk per C lanes (lane r = row r of the chunk, so the C
 // lanes read C consecutive values per column: a full 256-byte line for
 // C = 32, FP64) and skip the chunks the slices cover; they take the chunks in
 // `order` (decreasing width, or c_base onwards when null). Slices come first,
 // then the widest chunks, so the longest work starts earliest and the launch
 // ends on the narrowest chunks.
+//
+// A slice writes its partial sums to part[slot*C + r] and counts itself in
+// done[first]; the chunk's last slice to finish adds the chunk's partial
+// sums in slice order and writes y. The writes are fenced before the count
+// and the finisher fences before it reads them through L2, the pattern of
+// the CUDA programming guide's last-block reduction. The finisher puts the
+// count back to zero, so done[] is all zero between launches.
 template <int C, class V, class O, class X>
 __global__ void __launch_bounds__(kSellThreads, 10)
-    k_sell(int64_t nC, int64_t c_base, int32_t split_w, int64_t n_items, int64_t slice_blocks,
-           const int4 *__restrict__ items, const int32_t *__restrict__ order,
-           const int64_t *__restrict__ cs,
+    k_sell(int64_t nC, int64_t c_base, int32_t split_w, int32_t slice_w, int64_t n_items,
+           int64_t slice_blocks, const int4 *__restrict__ items,
+           const int32_t *__restrict__ order, const int64_t *__restrict__ cs,
            const int32_t *__restrict__ cl, const int32_t *__restrict__ cmin,
            const int32_t *__restrict__ perm, const V *__restrict__ vals,
            const O *__restrict__ offs, const X *__restrict__ x, X *__restrict__ y,
-           typename AccOf<V, X>::type *__restrict__ part, X alpha, X beta, int beta_nz) {
+           typename AccOf<V, X>::type *__restrict__ part, int32_t *__restrict__ done, X alpha,
+           X beta, int beta_nz) {
   using Acc = typename AccOf<V, X>::type;
   const L2Policy pol = make_l2_policy();
   if (blockIdx.x < slice_blocks) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t it = t / C;
     if (it >= n_items)
-      return;
+      return;  // whole lane groups: C divides 32
     const int r = (int)(t % C);
-    const int4 w = items[it];  // chunk, j0, j1, slot
-    const int64_t base = __ldg(cs + w.x) + (int64_t)w.y * C + r;
-    const X *xb = x + __ldg(cmin + w.x);
-    part[(int64_t)w.w * C + r] =
-        sell_row_sum<C, V, O, X>(vals + base, offs + base, xb, w.z - w.y, pol);
+    Acc v;
+    {
+      const int4 w = __ldg(items + it);  // chunk, j0, j1, slot
+      const int64_t base = __ldg(cs + w.x) + (int64_t)w.y * C + r;
+      const X *xb = x + __ldg(cmin + w.x);
+      v = sell_row_sum<C, V, O, X>(vals + base, offs + base, xb, w.z - w.y, pol);
+    }
+    // The item is read again rather than kept in registers over the sum.
+    const int4 w = __ldg(items + it);
+    const int lane = threadIdx.x & 31;
+    const unsigned group = C == 32 ? 0xffffffffu : ((1u << (C & 31)) - 1) << (lane & ~(C - 1));
+    __stcg(part + (int64_t)w.w * C + r, v);
+    __threadfence();
+    __syncwarp(group);
+    const int32_t first = w.w - w.y / slice_w;
+    const int32_t ns = (__ldg(cl + w.x) + slice_w - 1) / slice_w;
+    int last = 0;
+    if (r == 0) {
+      last = atomicAdd(done + first, 1) == ns - 1;
+      if (last)
+        done[first] = 0;
+    }
+    last = __shfl_sync(group, last, lane & ~(C - 1));
+    if (!last)
+      return;
+    __threadfence();
+    Acc acc = 0;
+    for (int32_t q = 0; q < ns; ++q)
+      acc += __ldcg(part + (int64_t)(first + q) * C + r);
+    const int32_t dst = __ldg(perm + (int64_t)w.x * C + r);
+    if (dst >= 0)
+      store_y(y, dst, acc, alpha, beta, beta_nz);
     return;
   }
   const int64_t t = (int64_t)(blockIdx.x - slice_blocks) * blockDim.x + threadIdx.x;
@@ -274,7 +310,7 @@ __global__ void __launch_bounds__(kSellThreads, 10)
   const int r = (int)(t % C);
   const int32_t w = __ldg(cl + c);
   if (w > split_w)
-    return;  // sliced chunk: written by k_sell_combine
+    return;  // sliced chunk: written by its last slice
   const int64_t base = __ldg(cs + c) + r;
   const int32_t cm = __ldg(cmin + c);
   const int32_t dst = __ldg(perm + c * C + r);
@@ -284,53 +320,32 @@ __global__ void __launch_bounds__(kSellThreads, 10)
     store_y(y, dst, acc, alpha, beta, beta_nz);
 }
 
-// split: (chunk, first slot, slice count) per sliced chunk; the slices'
-// partial sums are added in slice order.
-template <int C, class Acc, class X>
-__global__ void k_sell_combine(int64_t n_split, const int4 *__restrict__ split,
-                               const int32_t *__restrict__ perm,
-                               const Acc *__restrict__ part, X *__restrict__ y,
-                               X alpha, X beta, int beta_nz) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t sidx = t / C;
-  if (sidx >= n_split)
-    return;
-  const int r = (int)(t % C);
-  const int4 sp = split[sidx];
-  Acc acc = 0;
-  for (int q = 0; q < sp.z; ++q)
-    acc += part[(int64_t)(sp.y + q) * C + r];
-  const int32_t dst = __ldg(perm + (int64_t)sp.x * C + r);
-  if (dst >= 0)
-    store_y(y, dst, acc, alpha, beta, beta_nz);
-}
-
 // What one k_sell launch covers: n_chunks chunks (order[0, n_chunks), or
-// c_base onwards when order is null), n_items column slices and n_split
-// sliced chunks.
+// c_base onwards when order is null) and n_items column slices of slice_w
+// columns, with their partial sums in `part` and completion counts in `done`
+// (one per slot, zero between launches).
 struct SellWork {
   int64_t n_chunks = 0, c_base = 0;
   int32_t split_w = INT32_MAX;  // wider chunks are covered by the slices
+  int32_t slice_w = 0;
   const int32_t *order = nullptr;
   int64_t n_items = 0;
   const int4 *items = nullptr;
-  int64_t n_split = 0;
-  const int4 *splits = nullptr;
-  void *part = nullptr;  // partial sums of the slices (scratch)
+  void *part = nullptr;
+  int32_t *done = nullptr;
 };
 
 static SellWork whole_work(const SellDev &s) {
   SellWork w;
   w.n_chunks = s.nC;
   w.order = s.order.as<int32_t>();
-  w.part = s.part.p;
-  if (s.n_split > 0)
+  if (s.n_items > 0) {
     w.split_w = s.split_w;
-  if (s.n_items > 0 && s.n_split > 0) {
+    w.slice_w = s.slice_w;
     w.n_items = s.n_items;
     w.items = s.items.as<int4>();
-    w.n_split = s.n_split;
-    w.splits = s.split_chunks.as<int4>();
+    w.part = s.part.p;
+    w.done = s.done.as<int32_t>();
   }
   return w;
 }
@@ -344,16 +359,10 @@ static void launch_sell(const SellDev &s, const SellWork &w, const X *x, X *y, X
   const int64_t chunk_blocks = div_up(w.n_chunks * C, kSellThreads);
   if (slice_blocks + chunk_blocks == 0)
     return;
-  Acc *part = (Acc *)w.part;
   k_sell<C, V, O, X><<<(unsigned)(slice_blocks + chunk_blocks), kSellThreads, 0, st>>>(
-      w.n_chunks, w.c_base, w.split_w, w.n_items, slice_blocks,
-      w.items, w.order, s.cs.as<int64_t>(), s.cl.as<int32_t>(), s.col_min.as<int32_t>(),
-      s.permd2in.as<int32_t>(), s.vals.as<V>(), s.offsets.as<O>(), x, y, part, alpha, beta, bnz);
-  if (w.n_split > 0) {
-    const int64_t b2 = div_up(w.n_split * C, 256);
-    k_sell_combine<C, Acc, X><<<(unsigned)b2, 256, 0, st>>>(
-        w.n_split, w.splits, s.permd2in.as<int32_t>(), part, y, alpha, beta, bnz);
-  }
+      w.n_chunks, w.c_base, w.split_w, w.slice_w, w.n_items, slice_blocks, w.items, w.order,
+      s.cs.as<int64_t>(), s.cl.as<int32_t>(), s.col_min.as<int32_t>(), s.permd2in.as<int32_t>(),
+      s.vals.as<V>(), s.offsets.as<O>(), x, y, (Acc *)w.part, w.done, alpha, beta, bnz);
 }
 
 template <int C, class V, class X>
@@ -476,26 +485,24 @@ void sell_plan_bands(SellDev &s, int64_t m, int n_bands) {
     std::stable_sort(wide.begin(), wide.end(),
                      [&](int32_t a, int32_t b) { return cl[a] > cl[b]; });
     wide = group_by_band(wide, nb, [&](int32_t c) { return band_of(c); }, first);
-    std::vector<int4> items, splits;
+    std::vector<int4> items;
     int32_t slot = 0;
     for (size_t b = 0; b < nb; ++b) {
       bands[b].i0 = (int64_t)items.size();
-      bands[b].s0 = (int64_t)splits.size();
       for (int64_t k = first[b]; k < first[b + 1]; ++k) {
         const int32_t c = wide[(size_t)k];
         const int32_t ns = (int32_t)div_up(cl[c], kBandSliceW);
-        splits.push_back(make_int4(c, slot, ns, 0));
         for (int32_t q = 0; q < ns; ++q)
           items.push_back(make_int4(c, q * kBandSliceW,
                                     std::min(cl[c], (q + 1) * kBandSliceW), slot + q));
         slot += ns;
       }
       bands[b].i1 = (int64_t)items.size();
-      bands[b].s1 = (int64_t)splits.size();
     }
     to_device(s.bands.items, items);
-    to_device(s.bands.splits, splits);
     s.bands.part.reserve(sizeof(double) * (size_t)slot * s.C);  // FP64 covers both accumulators
+    s.bands.done.reserve(sizeof(int32_t) * (size_t)slot);
+    PLS_CUDA(cudaMemset(s.bands.done.p, 0, sizeof(int32_t) * (size_t)slot));
     s.bands.split_w = 2 * kBandSliceW;
   }
   s.bands.bands = std::move(bands);
@@ -508,12 +515,12 @@ void spmv_sell_band(const SellDev &s, const RowBand &b, const X *x, X *y, X alph
   w.n_chunks = b.c1 - b.c0;
   w.c_base = b.c0;
   w.split_w = s.bands.split_w;
+  w.slice_w = kBandSliceW;
   w.order = s.bands.order.p ? s.bands.order.as<int32_t>() + b.c0 : nullptr;
   w.n_items = b.i1 - b.i0;
   w.items = s.bands.items.p ? s.bands.items.as<int4>() + b.i0 : nullptr;
-  w.n_split = b.s1 - b.s0;
-  w.splits = s.bands.splits.p ? s.bands.splits.as<int4>() + b.s0 : nullptr;
   w.part = s.bands.part.p;
+  w.done = s.bands.done.as<int32_t>();
   run_sell<X>(s, w, x, y, alpha, beta, st);
 }
 
@@ -572,60 +579,63 @@ void spmv_csr_band(const CsrDev &c, const RowBand &b, int tpr, const X *x, X *y,
 
 // -------------------------------------- SELL SpMV without allocation
 
-// Scratch of the allocation-free SELL entry point: the partial sums of the
-// column slices of wide chunks, in a fixed device array instead of a
-// per-handle cudaMalloc buffer. Every GPU that loads the library holds these
-// 16 MiB until the process exits. All calls share it, so calls that overlap
-// on the GPU (different streams, or different host threads) race on it.
-constexpr int64_t kNoAllocScratchElems = int64_t(1) << 21;  // FP64 elements
+// Fixed device arrays of the allocation-free SELL entry point, instead of
+// per-handle cudaMalloc buffers: the partial sums of the column slices of
+// wide chunks (2^21 FP64 elements) and their completion counts (one per
+// slot; C >= 8, so 2^18 of them). Every GPU that loads the library holds
+// these 17 MiB until the process exits. All calls share them, so calls that
+// overlap on the GPU (different streams, or different host threads) race on
+// them.
+constexpr int64_t kNoAllocScratchElems = int64_t(1) << 21;
+constexpr int64_t kNoAllocSlots = kNoAllocScratchElems / 8;
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchElems];
+static __device__ int32_t g_noalloc_done[kNoAllocSlots];  // zero at load
 
 namespace {
 std::mutex g_noalloc_mu;
-void *g_noalloc_addr[64] = {};
+void *g_noalloc_part[64] = {};
+void *g_noalloc_count[64] = {};
+
+void *symbol_address(const void *sym, const char *what) {
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, sym);
+  if (e != cudaSuccess)
+    throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE,
+                std::string("cudaGetSymbolAddress(") + what + "): " + cudaGetErrorString(e));
+  return p;
+}
 }  // namespace
 
-int64_t noalloc_scratch_capacity() { return kNoAllocScratchElems; }
-
-// Device address of the scratch array for `device`. In host code the array's
-// name is only a host-side stand-in, so the address comes from
-// cudaGetSymbolAddress, once per device, with that device current (the
-// caller's DeviceGuard makes it current).
-void *noalloc_scratch_address(int device) {
-  std::lock_guard<std::mutex> g(g_noalloc_mu);
-  void *&a = g_noalloc_addr[device & 63];
-  if (!a) {
-    void *p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess)
-      throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE,
-                  std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
-    a = p;
-  }
-  return a;
-}
-
-// The sliced SELL SpMV (k_sell_items + k_sell_combine, or k_sell when no
-// chunk is sliced) with its partial sums in `scratch` (capacity in FP64
-// elements). Every slot a call reads was written earlier in the same call,
-// so nothing needs clearing between calls.
-template <class X>
-void spmv_sell_scratch(const SellDev &s, const X *x, X *y, X alpha, X beta, void *scratch,
-                       int64_t capacity, cudaStream_t st) {
+// The SELL SpMV with its slices' partial sums and counts in the fixed
+// arrays. Their device addresses come from cudaGetSymbolAddress (in host code
+// the arrays' names are only host-side stand-ins), once per device, with that
+// device current (the caller's DeviceGuard makes it current). Every slot a
+// call reads was written earlier in the same call, and the counts return to
+// zero by the end of every launch, so nothing needs clearing between calls.
+void spmv_sell_noalloc(const SellDev &s, const double *x, double *y, double alpha, double beta,
+                       int device, cudaStream_t st) {
   if (s.nC == 0)
     return;
-  const int64_t slots = s.n_split > 0 ? (int64_t)(s.part.bytes / (sizeof(double) * s.C)) : 0;
-  if (slots * s.C > capacity)
+  const int64_t slots = s.n_items > 0 ? (int64_t)(s.done.bytes / sizeof(int32_t)) : 0;
+  if (slots * s.C > kNoAllocScratchElems)
     throw Error(PERFLIBS_STATUS_INPUT_PARAMETER_ERROR,
                 "this matrix needs " + std::to_string(slots * s.C) +
-                    " scratch elements; the fixed scratch holds " + std::to_string(capacity));
+                    " scratch elements; the fixed scratch holds " +
+                    std::to_string(kNoAllocScratchElems));
   SellWork w = whole_work(s);
-  w.part = scratch;
-  run_sell<X>(s, w, x, y, alpha, beta, st);
+  {
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    void *&part = g_noalloc_part[device & 63];
+    void *&count = g_noalloc_count[device & 63];
+    if (!part) {
+      part = symbol_address(g_noalloc_scratch, "scratch");
+      count = symbol_address(g_noalloc_done, "counts");
+    }
+    w.part = part;
+    w.done = static_cast<int32_t *>(count);
+  }
+  run_sell<double>(s, w, x, y, alpha, beta, st);
 }
-
-template void spmv_sell_scratch<double>(const SellDev &, const double *, double *, double,
-                                        double, void *, int64_t, cudaStream_t);
 
 // ------------------------------------------------------------ transpose
 
