@@ -214,7 +214,7 @@ def run_reference(args):
         "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(line))
+    emit(line, args)
     return 0
 
 
@@ -421,7 +421,7 @@ def run_b200(args):
         line["cpu_baseline"] = {"value": gbs, "unit": "GB/s", "cores": threads, "kind": kind,
                                 "sample": sample, "optimize_s": t_opt_cpu, "ms_per_step": sec * 1e3}
     if rank == 0:
-        print(json.dumps(line))
+        emit(line, args)
     A.destroy()
     A_plain.destroy()
     if world > 1:
@@ -588,8 +588,18 @@ def run_extra(args):
                             **bt.info(), "rows_total": int(sum(d["m"] for d in inst))})
     line["roofline"] = {"bound": "hbm", "achieved": line["value"], "peak": hbm, "unit": "GB/s",
                         "frac": line["value"] / hbm, "peak_source": peak_kind}
-    print(json.dumps(line))
+    emit(line, args)
     return 0
+
+
+def emit(line, args):
+    """Print the result line; with --log, also append it to that JSON-lines
+    file (one object per run, so a series of runs is one log)."""
+    text = json.dumps(line)
+    print(text)
+    if args.log:
+        with open(args.log, "a") as f:
+            f.write(text + "\n")
 
 
 def main():
@@ -603,6 +613,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--log", default=None, help="append the result line to this JSON-lines file")
     ap.add_argument("--soak-seconds", type=float, default=0.5,
                     help="untimed load before the timed region, so the clock samples see the GPU busy")
     args = ap.parse_args()

@@ -160,6 +160,32 @@ perflibs_status_t perflibs_b200_spmat_spmm_info(perflibs_spmat_t A, int32_t *til
                                                 int64_t *staged_rows, int64_t *runs,
                                                 int32_t *path, float *ms_staged, float *ms_rows);
 
+/* How the handle's active SpMV configuration was chosen: 0 not chosen
+ * (default heuristic), 1 timed by the exhaustive tuner, 2 taken from the
+ * autotune cache, 3 predicted by the learned selector, 4 forced. */
+perflibs_status_t perflibs_b200_spmat_tune_source(perflibs_spmat_t A, int32_t *source);
+
+/* Autotune cache (checkpoint / resume of the exhaustive tuner). Every
+ * exhaustive tune is recorded under a key of the GPU model (compute
+ * capability and SM count), the matrix's dimensions and nonzero count, the
+ * API and storage value types and a 64-bit hash of its sparsity structure
+ * (values do not enter: they do not change a kernel's speed). A later
+ * exhaustive optimize with the same key applies the recorded configuration
+ * and timing table without timing anything (tune_source 2). save writes the
+ * process's cache to a text file; load merges a file into it (a malformed
+ * or truncated file changes nothing and is an input error); clear empties
+ * it; size counts its entries. */
+perflibs_status_t perflibs_b200_tune_cache_save(const char *path);
+perflibs_status_t perflibs_b200_tune_cache_load(const char *path);
+perflibs_status_t perflibs_b200_tune_cache_clear(void);
+int64_t perflibs_b200_tune_cache_size(void);
+
+/* Writes past the end of the library's device buffers seen so far in the
+ * guard build (libplsparse_b200_guard.so: every buffer followed by a guard
+ * of 0xFF bytes, checked when the buffer is freed); -1 in the regular
+ * build, which has no guards. */
+int64_t perflibs_b200_debug_guard_violations(void);
+
 /* Timings the last exhaustive tune measured: up to `cap` rows of
  * (kind, C, sigma, tpr) in cfg4, milliseconds in ms and the SELL padding
  * efficiency nnz / padded size in beta (1 for CSR rows); any output may be

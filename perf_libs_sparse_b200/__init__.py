@@ -19,7 +19,9 @@ from typing import Optional
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libplsparse_b200.so")
+# PERFLIBS_B200_LIBRARY selects another build of the library (the guard
+# build, libplsparse_b200_guard.so, for instance).
+LIB_PATH = os.environ.get("PERFLIBS_B200_LIBRARY") or os.path.join(HERE, "libplsparse_b200.so")
 ROOT = os.path.dirname(HERE)
 INCLUDE_DIR = os.path.join(ROOT, "include")
 
@@ -113,6 +115,10 @@ def lib():
             "perflibs_b200_spmat_set_spmm_path": [vp, i32],
             "perflibs_b200_spmat_set_host_bands": [vp, i32],
             "perflibs_b200_spmat_host_bands_used": [vp, vp],
+            "perflibs_b200_spmat_tune_source": [vp, vp],
+            "perflibs_b200_tune_cache_save": [C.c_char_p],
+            "perflibs_b200_tune_cache_load": [C.c_char_p],
+            "perflibs_b200_tune_cache_clear": [],
             "perflibs_b200_read_mtx": [C.c_char_p, vp, vp, vp, vp, vp, vp],
             "perflibs_b200_testing_stage_fault": [i32, i32],
             "perflibs_b200_spmv_exec_d_dev": [i, d, vp, vp, d, vp, vp],
@@ -140,6 +146,10 @@ def lib():
         L.perflibs_spmat_create_identity.restype = vp
         L.perflibs_spmat_print_err.restype = None
         L.perflibs_b200_version.restype = C.c_char_p
+        L.perflibs_b200_tune_cache_size.argtypes = []
+        L.perflibs_b200_tune_cache_size.restype = C.c_int64
+        L.perflibs_b200_debug_guard_violations.argtypes = []
+        L.perflibs_b200_debug_guard_violations.restype = C.c_int64
         _lib = L
     return _lib
 
@@ -458,6 +468,12 @@ class SpMat:
         """Row bands of host-buffer SpMV: 0 by size (default), 1 none, 2..64 that many."""
         _check(lib().perflibs_b200_spmat_set_host_bands(self.h, n_bands), "set_host_bands")
 
+    def tune_source(self):
+        """How the active SpMV configuration was chosen (TUNE_SOURCE_*)."""
+        r = C.c_int32()
+        _check(lib().perflibs_b200_spmat_tune_source(self.h, C.byref(r)), "tune_source")
+        return r.value
+
     def host_bands_used(self):
         """Bands the last host-buffer SpMV ran in (0 = one launch)."""
         r = C.c_int32()
@@ -524,6 +540,12 @@ class Batch:
         """Row bands of host-buffer SpMV: 0 by size (default), 1 none, 2..64 that many."""
         _check(lib().perflibs_b200_spmat_set_host_bands(self.h, n_bands), "set_host_bands")
 
+    def tune_source(self):
+        """How the active SpMV configuration was chosen (TUNE_SOURCE_*)."""
+        r = C.c_int32()
+        _check(lib().perflibs_b200_spmat_tune_source(self.h, C.byref(r)), "tune_source")
+        return r.value
+
     def host_bands_used(self):
         """Bands the last host-buffer SpMV ran in (0 = one launch)."""
         r = C.c_int32()
@@ -540,6 +562,32 @@ class Batch:
             self.destroy()
         except Exception:
             pass
+
+
+# Autotune cache (checkpoint / resume of the exhaustive tuner).
+TUNE_SOURCE_NONE, TUNE_SOURCE_TIMED, TUNE_SOURCE_CACHE, TUNE_SOURCE_SELECTOR, TUNE_SOURCE_FORCED = range(5)
+
+
+def tune_cache_save(path):
+    _check(lib().perflibs_b200_tune_cache_save(os.fsencode(path)), "tune_cache_save")
+
+
+def tune_cache_load(path):
+    _check(lib().perflibs_b200_tune_cache_load(os.fsencode(path)), "tune_cache_load")
+
+
+def tune_cache_clear():
+    _check(lib().perflibs_b200_tune_cache_clear(), "tune_cache_clear")
+
+
+def tune_cache_size():
+    return int(lib().perflibs_b200_tune_cache_size())
+
+
+def debug_guard_violations():
+    """Writes past device buffers' ends seen by the guard build (-1 in the
+    regular build)."""
+    return int(lib().perflibs_b200_debug_guard_violations())
 
 
 def spmm_optimize(transA, transB, alpha_hint, A: SpMat, B: SpMat, beta_hint, Cm: SpMat):

@@ -1462,6 +1462,7 @@ perflibs_status_t perflibs_spmv_optimize(perflibs_spmat_t A) {
     if (A->forced) {
       bsr_become_csr(A);
       apply_config(A, A->forced_cfg);
+      A->tune_source = TuneSource::FORCED;
       A->tuned = true;
       A->tuned_op = op;
       return PERFLIBS_STATUS_SUCCESS;
@@ -1482,6 +1483,7 @@ perflibs_status_t perflibs_spmv_optimize(perflibs_spmat_t A) {
           cls >= 0 && cls < (int32_t)cands.size()) {
         apply_config(A, cands[cls]);
         A->selector_class = cls;
+        A->tune_source = TuneSource::SELECTOR;
         A->tuned = true;
         A->tuned_op = op;
         return PERFLIBS_STATUS_SUCCESS;
@@ -1617,6 +1619,13 @@ perflibs_status_t perflibs_b200_spmat_set_host_bands(perflibs_spmat_t A, int32_t
   if (!A || n_bands < 0 || n_bands > kMaxHostBands)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
   A->host_bands = n_bands;
+  return PERFLIBS_STATUS_SUCCESS;
+}
+
+perflibs_status_t perflibs_b200_spmat_tune_source(perflibs_spmat_t A, int32_t *source) {
+  if (!A || !source)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  *source = (int32_t)A->tune_source;
   return PERFLIBS_STATUS_SUCCESS;
 }
 

@@ -25,6 +25,7 @@
 #include <cstdio>
 #include <stdexcept>
 #include <string>
+#include <tuple>
 #include <utility>
 #include <vector>
 
@@ -68,6 +69,19 @@ struct TraceRange {
 
 // ------------------------------------------------------------ device buffer
 
+#ifdef PLS_DEBUG_GUARDS
+// Guard build (libplsparse_b200_guard.so): every device buffer is followed
+// by kGuardBytes of 0xFF bytes, NaN as FP64 / FP32 words and -1 as indices.
+// A kernel that writes past a buffer's end changes them, and release()
+// counts that (perflibs_b200_debug_guard_violations); one that reads past
+// the end reads NaN into its result, which the comparison with the oracle
+// catches. compute-sanitizer is the tool for this, and it is not available
+// on every machine.
+constexpr size_t kGuardBytes = 4096;
+void guard_arm(void *end);                  // fill the guard (debug.cu)
+void guard_check(const void *end) noexcept;  // verify it, count a violation
+#endif
+
 struct DevBuf {
   void *p = nullptr;
   size_t bytes = 0;
@@ -90,8 +104,12 @@ struct DevBuf {
   }
   ~DevBuf() { release(); }
   void release() {
-    if (p)
+    if (p) {
+#ifdef PLS_DEBUG_GUARDS
+      guard_check(static_cast<char *>(p) + bytes);
+#endif
       cudaFree(p);
+    }
     p = nullptr;
     bytes = 0;
   }
@@ -102,7 +120,12 @@ struct DevBuf {
     release();
     if (b == 0)
       b = 16;
+#ifdef PLS_DEBUG_GUARDS
+    PLS_CUDA(cudaMalloc(&p, b + kGuardBytes));
+    guard_arm(static_cast<char *>(p) + b);
+#else
     PLS_CUDA(cudaMalloc(&p, b));
+#endif
     bytes = b;
   }
   template <class T> T *as() const { return static_cast<T *>(p); }
@@ -339,6 +362,23 @@ struct TuneEntry {
   double beta = 1.0;  // SELL padding efficiency (1 for CSR)
 };
 
+// Key of the autotune cache: GPU model, dimensions, value types and a hash
+// of the sparsity structure (tune_cache.cu).
+struct TuneKey {
+  std::string dev;
+  int32_t m = 0, n = 0;
+  int64_t nnz = 0;
+  uint64_t hash = 0;
+  int dt = 0, vt = 0;
+  bool operator<(const TuneKey &o) const {
+    return std::tie(dev, m, n, nnz, hash, dt, vt) <
+           std::tie(o.dev, o.m, o.n, o.nnz, o.hash, o.dt, o.vt);
+  }
+};
+
+// How the active SpMV configuration was chosen (perflibs_b200_spmat_tune_source).
+enum class TuneSource : int { NONE = 0, TIMED = 1, CACHE = 2, SELECTOR = 3, FORCED = 4 };
+
 }  // namespace pls
 
 // The opaque handle of the C interface.
@@ -385,6 +425,7 @@ struct perflibs_spmat_top_t {
   bool tuned = false;
   int tuned_op = PERFLIBS_SPARSE_OPERATION_NOTRANS;
   std::vector<pls::TuneEntry> tune_table;
+  pls::TuneSource tune_source = pls::TuneSource::NONE;
   cudaStream_t stream = nullptr;  // nullptr = library stream
 
   pls::CsrDev csr;
@@ -517,6 +558,12 @@ int64_t count_blocks(const CsrDev &c, int32_t m, int32_t n, int bs, cudaStream_t
 int64_t sell_padded_size(const CsrDev &c, int32_t m, int C, int sigma, cudaStream_t s);
 
 // Tuning.
+// Autotune cache: find computes the matrix's key (one device pass over its
+// structure) and looks it up; put records a finished tune under it.
+bool tune_cache_find(const Mat *A, SpmvConfig &best, std::vector<TuneEntry> &table,
+                     TuneKey &key);
+void tune_cache_put(const TuneKey &key, const SpmvConfig &best,
+                    const std::vector<TuneEntry> &table);
 std::vector<SpmvConfig> tune_candidates(const Mat *A);
 void tune_spmv(Mat *A);
 SpmvConfig default_config(const Mat *A);

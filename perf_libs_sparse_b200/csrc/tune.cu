@@ -175,8 +175,16 @@ std::vector<SpmvConfig> tune_candidates(const Mat *A) {
 
 void tune_spmv(Mat *A) {
   A->tune_table.clear();
+  A->tune_source = TuneSource::NONE;
   if (A->m == 0 || A->csr.nnz == 0) {
     apply_config(A, default_config(A));
+    return;
+  }
+  TuneKey key;
+  SpmvConfig cached;
+  if (tune_cache_find(A, cached, A->tune_table, key)) {
+    apply_config(A, cached);
+    A->tune_source = TuneSource::CACHE;
     return;
   }
   const auto cands = tune_candidates(A);
@@ -207,6 +215,8 @@ void tune_spmv(Mat *A) {
   if (best_cfg.kind == Kind::SELL)
     A->sell = std::move(best_sell);
   apply_config(A, best_cfg);
+  A->tune_source = TuneSource::TIMED;
+  tune_cache_put(key, best_cfg, A->tune_table);
 }
 
 }  // namespace pls

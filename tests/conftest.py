@@ -34,6 +34,22 @@ def pytest_collection_modifyitems(config, items):
             it.add_marker(skip)
 
 
+@pytest.fixture(scope="session", autouse=True)
+def guard_build_check():
+    """Under the guard build of the library (PERFLIBS_B200_LIBRARY naming
+    libplsparse_b200_guard.so), the session fails if any kernel wrote past a
+    device buffer's end. The handles still alive are freed first, since the
+    guards are checked when buffers are freed."""
+    yield
+    if os.environ.get("PERFLIBS_B200_LIBRARY", "").endswith("_guard.so"):
+        import gc
+
+        import perf_libs_sparse_b200 as pls
+
+        gc.collect()
+        assert pls.debug_guard_violations() == 0
+
+
 @pytest.fixture(scope="session")
 def kats():
     with open(os.path.join(GOLDEN, "reference_kats.json")) as f:

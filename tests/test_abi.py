@@ -41,6 +41,21 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_guard_build_exports_the_same_symbols():
+    import perf_libs_sparse_b200.build as b
+
+    if not os.path.exists(b.LIB_GUARD):
+        pytest.skip("guard build not present")
+    G = ctypes.CDLL(b.LIB_GUARD)
+    missing = [n for n in declared_functions() if not hasattr(G, n)]
+    assert not missing, missing
+    G.perflibs_b200_debug_guard_violations.restype = ctypes.c_int64
+    assert G.perflibs_b200_debug_guard_violations() == 0
+    L = ctypes.CDLL(pls.LIB_PATH)
+    L.perflibs_b200_debug_guard_violations.restype = ctypes.c_int64
+    assert L.perflibs_b200_debug_guard_violations() == -1
+
+
 def test_library_is_sm100a_only():
     # The fat binary carries sm_100a code only; cuobjdump is not used, the
     # build command line is the evidence.

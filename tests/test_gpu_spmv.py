@@ -203,6 +203,57 @@ def test_autotune_picks_a_valid_config_and_matches():
     assert rel_err_rows(y, yref, scale_of(rp, c, v, x, 1, 0, None)).max() <= FP64_TOL
 
 
+def test_autotune_cache_resumes_tuning(tmp_path):
+    """An exhaustive tune is recorded under the matrix's structure; the same
+    structure (any values) takes it from the cache without timing, across a
+    save / clear / load of the cache file; another storage mode is another
+    key."""
+    pls.tune_cache_clear()
+    m, n, rp, c, v = W.zipf_rows(60_000, seed=31)
+    x = W.uniform_vector(n, 32)
+    A = pls.SpMat.csr(m, n, rp, c, v)
+    assert A.optimize() == 0
+    assert A.tune_source() == pls.TUNE_SOURCE_TIMED
+    cfg0 = A.config()
+    tab_a, ms_a = A.tune_table()
+    B = pls.SpMat.csr(m, n, rp, c, 2.0 * v)
+    assert B.optimize() == 0
+    assert B.tune_source() == pls.TUNE_SOURCE_CACHE
+    assert B.config() == cfg0
+    tab_b, ms_b = B.tune_table()
+    np.testing.assert_array_equal(tab_a, tab_b)
+    np.testing.assert_array_equal(ms_a, ms_b)
+    yref = oracle.csr_spmv(rp, c, 2.0 * v, x)
+    assert rel_err_rows(B.spmv(x), yref, scale_of(rp, c, 2.0 * v, x, 1, 0, None)).max() <= FP64_TOL
+    F = pls.SpMat.csr(m, n, rp, c, v)
+    assert F.set_storage(pls.STORAGE_FP32) == 0
+    assert F.optimize() == 0
+    assert F.tune_source() == pls.TUNE_SOURCE_TIMED
+    path = tmp_path / "tune.cache"
+    pls.tune_cache_save(path)
+    assert pls.tune_cache_size() == 2
+    pls.tune_cache_clear()
+    D = pls.SpMat.csr(m, n, rp, c, v)
+    assert D.optimize() == 0
+    assert D.tune_source() == pls.TUNE_SOURCE_TIMED
+    pls.tune_cache_clear()
+    pls.tune_cache_load(path)
+    E = pls.SpMat.csr(m, n, rp, c, v)
+    assert E.optimize() == 0
+    assert E.tune_source() == pls.TUNE_SOURCE_CACHE
+    assert E.config() == cfg0
+    tab_e, ms_e = E.tune_table()
+    np.testing.assert_array_equal(tab_a, tab_e)
+    np.testing.assert_allclose(ms_a, ms_e, rtol=1e-6)
+    G = pls.SpMat.csr(m, n, rp, c, v)
+    assert G.force_config(pls.KIND_CSR, 0, 0, 4) == 0
+    assert G.optimize() == 0
+    assert G.tune_source() == pls.TUNE_SOURCE_FORCED
+    for h in (A, B, D, E, F, G):
+        h.destroy()
+    pls.tune_cache_clear()
+
+
 # ------------------------------------------------------- edge cases
 
 
