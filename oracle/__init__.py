@@ -22,7 +22,9 @@ from typing import Optional
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-PORT_SO = os.path.join(HERE, "_build", "liboracle.so")
+# PLSPARSE_ORACLE_LIB selects another build of the restatement (the
+# sanitized one, for instance).
+PORT_SO = os.environ.get("PLSPARSE_ORACLE_LIB") or os.path.join(HERE, "_build", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libplsparse_ref.so")
 
 _port = None
