@@ -129,11 +129,15 @@ perflibs_status_t perflibs_b200_spmat_exec_info(perflibs_spmat_t A,
 /* SpMM kernels for a CSR A. The staged kernel copies, for every block of R
  * rows of A, the rows of B the block needs into shared memory (TMA bulk
  * copies) and multiplies from there; the row-group kernel reads B through
- * the caches. When the staged kernel applies (B rows reused inside row
- * blocks, B 16-byte aligned, ldb and k multiples of 16 bytes), the first
- * SpMM of each (k, ldb, value type) times both on scratch output and keeps
- * the faster. set_spmm_path overrides that: -1 measured choice (default),
- * 0 row-group kernel, 1 staged kernel whenever it applies. */
+ * the caches, its lanes loading a row's entries one group at a time or (the
+ * shared-entries variant) a row's lanes loading consecutive entries together
+ * and passing them round. The first SpMM of each (k, ldb, value type) times
+ * the candidates that apply (the staged kernel needs B rows reused inside
+ * row blocks, B 16-byte aligned, ldb and k multiples of 16 bytes) on scratch
+ * output and keeps the fastest. set_spmm_path overrides that: -1 measured
+ * choice (default), 0 row-group kernel, 1 staged kernel whenever it
+ * applies, 2 row-group kernel with shared entries whenever the lane shape
+ * allows (at least 4 lanes per row of C). */
 perflibs_status_t perflibs_b200_spmat_set_spmm_path(perflibs_spmat_t A, int32_t path);
 
 /* Host-buffer SpMV (perflibs_spmv_exec_{s,d}) in row bands: the kernels of
@@ -153,7 +157,8 @@ perflibs_status_t perflibs_b200_spmat_host_bands_used(perflibs_spmat_t A, int32_
 /* SpMM plan of the handle: the staged tiles' block height R (0 when none
  * were built: the staged kernel does not apply), the B rows staged per
  * column tile over all blocks and the copy runs; the path the last SpMM
- * took (1 staged, 0 row-group, -1 none yet); and the two timings of the
+ * took (1 staged, 0 row-group, 2 row-group with shared entries, -1 none
+ * yet); and the two timings of the
  * measured choice in milliseconds (0 when not measured). Any output may be
  * NULL. */
 perflibs_status_t perflibs_b200_spmat_spmm_info(perflibs_spmat_t A, int32_t *tile_rows,

@@ -52,13 +52,13 @@ __device__ __forceinline__ void batch_rows(const Rows &A, const InstDesc &d, con
     const int32_t row = r0 + (lane >> lg_g);
     const bool live = row < w.row1;
     if (d.path == 0)
-      spmm_row_group<4, 1, float, float, Rows, OFF32, true>(
+      spmm_row_group<4, 1, float, float, Rows, OFF32, kEntriesAhead>(
           A, row, live, d.lg_tk, d.lg_tn, d.B, d.ldb, d.C, d.ldc, d.k, alpha, beta, beta_nz, pol);
     else if (d.path == 1)
-      spmm_row_group<1, 1, float, float, Rows, OFF32, true>(
+      spmm_row_group<1, 1, float, float, Rows, OFF32, kEntriesAhead>(
           A, row, live, d.lg_tk, d.lg_tn, d.B, d.ldb, d.C, d.ldc, d.k, alpha, beta, beta_nz, pol);
     else
-      spmm_row_group<1, 2, float, float, Rows, OFF32, true>(
+      spmm_row_group<1, 2, float, float, Rows, OFF32, kEntriesAhead>(
           A, row, live, d.lg_tk, d.lg_tn, d.B, d.ldb, d.C, d.ldc, d.k, alpha, beta, beta_nz, pol);
   }
 }

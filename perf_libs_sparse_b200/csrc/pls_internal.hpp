@@ -277,16 +277,20 @@ struct TileDev {
   int64_t unsuitable_from = INT64_MAX;
   DevBuf nuniq, run_ptr, runs, local;
   HostFlag err;
-  // Measured choice between the staged and the row-group SpMM for the call
-  // signature `choice_sig` (k, ldb, value and API types): 1 staged, 0 row
-  // group, -1 not measured; with both timings (ms).
+  // Measured choice between the SpMM kernels for the call signature
+  // `choice_sig` (k, ldb, value and API types): 0 row group 64-bit offsets,
+  // 2 row group 32-bit, 3 row group with shared entries, 1 staged, -1 not
+  // measured; with the staged and the best row-group timing (ms).
   int64_t choice_sig = -1;
   int choice = -1;
   float ms_staged = 0.f, ms_rows = 0.f;
   // Path forced by perflibs_b200_spmat_set_spmm_path: -1 measured choice,
-  // 0 row group, 1 staged (when it applies).
+  // 0 row group, 1 staged (when it applies), 2 row group with shared entries
+  // (when the lane shape allows them).
   int forced = -1;
-  int last_path = -1;  // path of the last SpMM: 1 staged, 0 row group
+  // Path of the last SpMM: 1 staged, 0 row group, 2 row group with shared
+  // entries.
+  int last_path = -1;
 };
 
 struct CsrDev {

@@ -18,20 +18,48 @@
 
 namespace pls {
 
-template <int VEC, int NV, class V, class X, bool OFF32>
-__global__ void __launch_bounds__(256)
-    k_spmm_csr(int32_t m, int lg_tk, int lg_tn, const int32_t *__restrict__ rp,
-               const int32_t *__restrict__ col, const V *__restrict__ val,
-               const X *__restrict__ B, int64_t ldb, X *__restrict__ C, int64_t ldc, int k,
-               X alpha, X beta, int beta_nz) {
+template <int VEC, int NV, class V, class X, bool OFF32, int ENTRIES>
+__device__ __forceinline__ void spmm_csr_rows(int32_t m, int lg_tk, int lg_tn,
+                                              const int32_t *__restrict__ rp,
+                                              const int32_t *__restrict__ col,
+                                              const V *__restrict__ val, const X *__restrict__ B,
+                                              int64_t ldb, X *__restrict__ C, int64_t ldc, int k,
+                                              X alpha, X beta, int beta_nz) {
   using Acc = typename AccOf<V, X>::type;
   const L2Policy pol = make_l2_policy();
   const int lg_g = lg_tk + lg_tn;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t row = (warp << (5 - lg_g)) + ((threadIdx.x & 31) >> lg_g);
   const CsrRows<V> A{rp, col, val};
-  spmm_row_group<VEC, NV, Acc, X, CsrRows<V>, OFF32>(A, row, row < m, lg_tk, lg_tn, B, ldb, C,
-                                                      ldc, k, alpha, beta, beta_nz, pol);
+  spmm_row_group<VEC, NV, Acc, X, CsrRows<V>, OFF32, ENTRIES>(
+      A, row, row < m, lg_tk, lg_tn, B, ldb, C, ldc, k, alpha, beta, beta_nz, pol);
+}
+
+template <int VEC, int NV, class V, class X, bool OFF32, int ENTRIES>
+__global__ void __launch_bounds__(256)
+    k_spmm_csr(int32_t m, int lg_tk, int lg_tn, const int32_t *__restrict__ rp,
+               const int32_t *__restrict__ col, const V *__restrict__ val,
+               const X *__restrict__ B, int64_t ldb, X *__restrict__ C, int64_t ldc, int k,
+               X alpha, X beta, int beta_nz) {
+  spmm_csr_rows<VEC, NV, V, X, OFF32, ENTRIES>(m, lg_tk, lg_tn, rp, col, val, B, ldb, C, ldc, k,
+                                               alpha, beta, beta_nz);
+}
+
+// Shared entries for FP32 results with one vector per lane, held to 48
+// registers (5 blocks of 256 per SM): the shared loads add about 10
+// registers, which would cost a resident block. Measured on the 27-point
+// stencil (plain row-group kernel / shared uncapped / shared capped): FP32
+// k = 32 0.598 / 0.628 / 0.591 ms, k = 128 2.141 / 2.180 / 2.019 ms. FP64
+// results spill at the cap and run uncapped (k = 8 0.494 / 0.388 / 0.505,
+// k = 32 1.39 / 1.18 / 1.26), as do two vectors per lane (NV = 2).
+template <int VEC, class V, class X, bool OFF32>
+__global__ void __launch_bounds__(256, 5)
+    k_spmm_csr_shared(int32_t m, int lg_tk, int lg_tn, const int32_t *__restrict__ rp,
+                      const int32_t *__restrict__ col, const V *__restrict__ val,
+                      const X *__restrict__ B, int64_t ldb, X *__restrict__ C, int64_t ldc,
+                      int k, X alpha, X beta, int beta_nz) {
+  spmm_csr_rows<VEC, 1, V, X, OFF32, kEntriesShared>(m, lg_tk, lg_tn, rp, col, val, B, ldb, C,
+                                                     ldc, k, alpha, beta, beta_nz);
 }
 
 // 32-bit address arithmetic is possible when every offset into B (rows
@@ -41,61 +69,86 @@ static bool rows_off32_fits(const CsrDev &c, int32_t m, int64_t ldb, int64_t ldc
   return c.ncols > 0 && (int64_t)c.ncols * ldb < INT32_MAX && (int64_t)m * ldc < INT32_MAX;
 }
 
+// Whether the shared-entries mode applies to this lane shape: one lane group
+// per row (TN = 1) of at least 4 lanes, so a shared load covers a group of
+// U = 4 entries.
+static bool shared_entries_fit(const RowsShape &sh) { return sh.lg_tn == 0 && sh.lg_tk >= 2; }
+
 template <int VEC, class V, class X>
-static void launch_spmm_csr(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
-                            int64_t ldc, int k, X alpha, X beta, bool off32, cudaStream_t s) {
+static bool launch_spmm_csr(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
+                            int64_t ldc, int k, X alpha, X beta, bool off32, bool shared,
+                            cudaStream_t s) {
   const RowsShape sh = rows_shape(k, VEC, (double)c.nnz / std::max<int32_t>(m, 1));
   const int64_t rows_per_block = (int64_t)8 << (5 - (sh.lg_tk + sh.lg_tn));
   const unsigned blocks = (unsigned)div_up(m, rows_per_block);
   const int bnz = beta != X(0);
   off32 = off32 && rows_off32_fits(c, m, ldb, ldc);
-  auto go = [&](auto nv_tag, auto off_tag) {
+  shared = shared && shared_entries_fit(sh);
+  auto go = [&](auto nv_tag, auto off_tag, auto entries_tag) {
     constexpr int NV = decltype(nv_tag)::value;
     constexpr bool OFF = decltype(off_tag)::value;
-    k_spmm_csr<VEC, NV, V, X, OFF><<<blocks, 256, 0, s>>>(m, sh.lg_tk, sh.lg_tn,
-        c.row_ptr.as<int32_t>(), c.col.as<int32_t>(), (const V *)c.ev(), B, ldb, C, ldc, k,
-        alpha, beta, bnz);
+    constexpr int EM = decltype(entries_tag)::value;
+    if constexpr (EM == kEntriesShared && NV == 1 && sizeof(X) == 4)
+      k_spmm_csr_shared<VEC, V, X, OFF><<<blocks, 256, 0, s>>>(m, sh.lg_tk, sh.lg_tn,
+          c.row_ptr.as<int32_t>(), c.col.as<int32_t>(), (const V *)c.ev(), B, ldb, C, ldc, k,
+          alpha, beta, bnz);
+    else
+      k_spmm_csr<VEC, NV, V, X, OFF, EM><<<blocks, 256, 0, s>>>(m, sh.lg_tk, sh.lg_tn,
+          c.row_ptr.as<int32_t>(), c.col.as<int32_t>(), (const V *)c.ev(), B, ldb, C, ldc, k,
+          alpha, beta, bnz);
   };
   using I1 = std::integral_constant<int, 1>;
   using I2 = std::integral_constant<int, 2>;
   using T = std::true_type;
   using F = std::false_type;
+  auto by_entries = [&](auto nv_tag, auto off_tag) {
+    if (shared)
+      go(nv_tag, off_tag, std::integral_constant<int, kEntriesShared>{});
+    else
+      go(nv_tag, off_tag, std::integral_constant<int, kEntriesLane>{});
+  };
   if (sh.nv == 2)
-    off32 ? go(I2{}, T{}) : go(I2{}, F{});
+    off32 ? by_entries(I2{}, T{}) : by_entries(I2{}, F{});
   else
-    off32 ? go(I1{}, T{}) : go(I1{}, F{});
+    off32 ? by_entries(I1{}, T{}) : by_entries(I1{}, F{});
+  return shared;
 }
 
 // Row-group SpMM (the launch half of spmm_csr), with 32-bit address
-// arithmetic when `off32` and the offsets fit.
+// arithmetic when `off32` and the offsets fit, and shared entry loads when
+// `shared` and the lane shape allows them (returns whether they ran).
 template <class X>
-static void spmm_rows(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64_t ldc,
-                      int k, X alpha, X beta, bool off32, cudaStream_t s) {
+static bool spmm_rows(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64_t ldc,
+                      int k, X alpha, X beta, bool off32, bool shared, cudaStream_t s) {
   constexpr int VMAX = 16 / sizeof(X);
   const bool aligned = k >= VMAX && ((uintptr_t)B % 16 == 0) && ((uintptr_t)C % 16 == 0) &&
                        (ldb % VMAX == 0) && (ldc % VMAX == 0);
+  bool ran = false;
   with_vt(c.evt(), [&](auto tag) {
     using V = typename decltype(tag)::type;
     if constexpr (std::is_same_v<X, float> && std::is_same_v<V, double>) {
       throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE, "FP64 storage with FP32 API");
     } else {
       if (aligned)
-        launch_spmm_csr<VMAX, V, X>(c, m, B, ldb, C, ldc, k, alpha, beta, off32, s);
+        ran = launch_spmm_csr<VMAX, V, X>(c, m, B, ldb, C, ldc, k, alpha, beta, off32, shared, s);
       else
-        launch_spmm_csr<1, V, X>(c, m, B, ldb, C, ldc, k, alpha, beta, off32, s);
+        ran = launch_spmm_csr<1, V, X>(c, m, B, ldb, C, ldc, k, alpha, beta, off32, shared, s);
     }
   });
   PLS_LAUNCH_CHECK();
+  return ran;
 }
 
 // Kernel choice for a CSR SpMM, measured once per call signature (k, ldb,
 // value and API types): the row-group kernel with 64-bit and, when the
 // offsets fit, 32-bit address arithmetic (the better of the two differs
-// with k and the value type), and the staged kernel when it applies. With
-// more than one candidate, the first SpMM of the signature runs each on a
-// scratch C (beta = 0, CUDA events, one warm-up and two timed runs) and
+// with k and the value type), the row-group kernel with shared entry loads
+// when the lane shape allows them, and the staged kernel when it applies.
+// With more than one candidate, the first SpMM of the signature runs each on
+// a scratch C (beta = 0, CUDA events, one warm-up and two timed runs) and
 // keeps the fastest; later calls use the kept one. choice: 0 row group
-// 64-bit, 2 row group 32-bit, 1 staged.
+// 64-bit, 2 row group 32-bit, 3 row group with shared entries (32-bit
+// offsets when they fit), 1 staged.
 template <class X>
 void spmm_csr(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
               int64_t ldc, int k, X alpha, X beta, cudaStream_t s) {
@@ -105,23 +158,28 @@ void spmm_csr(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
                       ((int64_t)sizeof(X) << 4) ^ (int64_t)c.evt();
   TileDev &t = c.tiles;
   const bool fits32 = rows_off32_fits(c, m, ldb, ldc);
-  if (t.forced == 0) {
-    spmm_rows<X>(c, m, B, ldb, C, ldc, k, alpha, beta, fits32, s);
-    t.last_path = 0;
+  if (t.forced == 0 || t.forced == 2) {
+    t.last_path = spmm_rows<X>(c, m, B, ldb, C, ldc, k, alpha, beta, fits32, t.forced == 2, s)
+                      ? 2
+                      : 0;
     return;
   }
   if (t.forced == 1) {
     const bool staged = spmm_tiled<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s, true);
     if (!staged)
-      spmm_rows<X>(c, m, B, ldb, C, ldc, k, alpha, beta, fits32, s);
+      spmm_rows<X>(c, m, B, ldb, C, ldc, k, alpha, beta, fits32, false, s);
     t.last_path = staged ? 1 : 0;
     return;
   }
   if (t.choice_sig != sig) {
     const bool staged_ok = spmm_tiled<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s, false);
+    constexpr int VMAX = 16 / sizeof(X);
+    const bool vec_ok = k >= VMAX && ((uintptr_t)B % 16 == 0) && (ldb % VMAX == 0);
+    const bool shared_ok = shared_entries_fit(
+        rows_shape(k, vec_ok ? VMAX : 1, (double)c.nnz / std::max<int32_t>(m, 1)));
     t.choice = 0;
     t.ms_rows = t.ms_staged = 0.f;
-    if (staged_ok || fits32) {
+    if (staged_ok || fits32 || shared_ok) {
       DevBuf scratch;
       scratch.reserve(sizeof(X) * (size_t)m * k);
       X *sc = scratch.as<X>();
@@ -139,15 +197,24 @@ void spmm_csr(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
         PLS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
         return ms / 2;
       };
-      const float ms64 =
-          time2([&] { spmm_rows<X>(c, m, B, ldb, sc, (int64_t)k, k, X(1), X(0), false, s); });
+      const bool sc32 = fits32 && rows_off32_fits(c, m, ldb, k);
+      const float ms64 = time2(
+          [&] { spmm_rows<X>(c, m, B, ldb, sc, (int64_t)k, k, X(1), X(0), false, false, s); });
       float best = ms64;
-      if (fits32 && rows_off32_fits(c, m, ldb, k)) {
-        const float ms32 =
-            time2([&] { spmm_rows<X>(c, m, B, ldb, sc, (int64_t)k, k, X(1), X(0), true, s); });
+      if (sc32) {
+        const float ms32 = time2(
+            [&] { spmm_rows<X>(c, m, B, ldb, sc, (int64_t)k, k, X(1), X(0), true, false, s); });
         if (ms32 < best) {
           best = ms32;
           t.choice = 2;
+        }
+      }
+      if (shared_ok) {
+        const float mss = time2(
+            [&] { spmm_rows<X>(c, m, B, ldb, sc, (int64_t)k, k, X(1), X(0), sc32, true, s); });
+        if (mss < best) {
+          best = mss;
+          t.choice = 3;
         }
       }
       t.ms_rows = best;
@@ -166,8 +233,10 @@ void spmm_csr(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
     t.last_path = 1;
     return;
   }
-  spmm_rows<X>(c, m, B, ldb, C, ldc, k, alpha, beta, t.choice == 2, s);
-  t.last_path = 0;
+  t.last_path = spmm_rows<X>(c, m, B, ldb, C, ldc, k, alpha, beta,
+                             t.choice == 2 || (t.choice == 3 && fits32), t.choice == 3, s)
+                    ? 2
+                    : 0;
 }
 
 // ---------------------------------------------------------------- BSR

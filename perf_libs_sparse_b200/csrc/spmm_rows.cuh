@@ -158,19 +158,31 @@ struct BsrRows {
 
 constexpr int kSpmmInFlight = 4;  // U: nonzeros in flight per lane
 
+// How the lanes of a row get its entries (column, value):
+//   kEntriesLane   each lane loads the U entries of its group itself, then
+//                  their B rows (two round trips per group);
+//   kEntriesAhead  the same, with the next group's entries loaded while
+//                  this group's B rows are in flight (one round trip per
+//                  group, about 12 more registers). It pays where occupancy
+//                  is already bound by other registers (the batched kernel:
+//                  3.99 -> 3.85 ms on its 512-instance workload) and costs
+//                  where it is not (the single SpMM on a 27-point stencil:
+//                  FP64 k = 32 1.32 -> 1.57 ms, 64 instead of 48 registers);
+//   kEntriesShared the TK lanes of a row load TK consecutive entries at once
+//                  (one coalesced load per array; the next TK are loaded
+//                  while these are used) and hand them round with shuffles,
+//                  so TK nonzeros cost one entry round trip. Needs TN = 1;
+//                  the warp runs to its longest row.
+constexpr int kEntriesLane = 0, kEntriesAhead = 1, kEntriesShared = 2;
+
 // One group's row. Every lane of the warp must call this together (the
 // reduction shuffles over the whole warp); lanes whose row is past the end
 // pass live = false and only take part in the shuffles. TK, TN (as log2)
 // and k are uniform across the warp.
 // OFF32: every offset into B and C (row * ld + column) fits in 32 bits, so
 // the address arithmetic stays 32-bit.
-// PIPE: load the next group's entries while this group's B rows are in
-// flight (one round trip per group instead of two, for about 12 more
-// registers). It pays where occupancy is already bound by other registers
-// (the batched kernel: 3.99 -> 3.85 ms on its 512-instance workload) and
-// costs where it is not (the single SpMM on a 27-point stencil: FP64 k = 32
-// 1.32 -> 1.57 ms, at 64 instead of 48 registers).
-template <int VEC, int NV, class Acc, class X, class Rows, bool OFF32 = false, bool PIPE = false>
+template <int VEC, int NV, class Acc, class X, class Rows, bool OFF32 = false,
+          int ENTRIES = kEntriesLane>
 __device__ __forceinline__ void spmm_row_group(const Rows &A, int64_t row, bool live, int lg_tk,
                                                int lg_tn, const X *__restrict__ B, int64_t ldb,
                                                X *__restrict__ C, int64_t ldc, int k, X alpha,
@@ -183,6 +195,12 @@ __device__ __forceinline__ void spmm_row_group(const Rows &A, int64_t row, bool 
   int32_t s = 0, e = 0, aux = 0;
   if (live)
     A.range(row, s, e, aux);
+  int32_t longest = 0;  // kEntriesShared: the warp's longest row
+  if constexpr (ENTRIES == kEntriesShared) {
+    longest = e - s;
+    for (int o = 16; o > 0; o >>= 1)
+      longest = max(longest, __shfl_xor_sync(0xffffffffu, longest, o));
+  }
   const int tile = TK * VEC * NV;
   for (int k0 = 0; k0 < k; k0 += tile) {
     Acc acc[NV][VEC];
@@ -191,38 +209,25 @@ __device__ __forceinline__ void spmm_row_group(const Rows &A, int64_t row, bool 
 #pragma unroll
       for (int v = 0; v < VEC; ++v)
         acc[nv][v] = Acc(0);
-    // Entries (column, value) of U nonzeros from position p0 on, -1 past the
-    // row end.
-    const auto load_entries = [&](int32_t p0, int32_t(&c)[U], Acc(&a)[U]) {
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int32_t q = p0 + u * TN;
-        if (q < e) {
-          typename Rows::V av;
-          A.entry(q, aux, c[u], av, pol);
-          a[u] = to_acc<Acc>(av);
-        } else {
-          c[u] = -1;
-          a[u] = Acc(0);
-        }
+    // Entry q of the row, column -1 past the row end.
+    const auto load_entry = [&](int32_t q, int32_t &c, Acc &a) {
+      if (q < e) {
+        typename Rows::V av;
+        A.entry(q, aux, c, av, pol);
+        a = to_acc<Acc>(av);
+      } else {
+        c = -1;
+        a = Acc(0);
       }
     };
-    int32_t cn[U];
-    Acc an[U];
-    if constexpr (PIPE)
-      load_entries(s + tn, cn, an);
-    for (int32_t p = s + tn; p < e; p += U * TN) {
-      int32_t c[U];
-      Acc a[U];
-      if constexpr (PIPE) {
+    // Entries of U nonzeros from position p0 on, TN apart.
+    const auto load_entries = [&](int32_t p0, int32_t(&c)[U], Acc(&a)[U]) {
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-          c[u] = cn[u];
-          a[u] = an[u];
-        }
-      } else {
-        load_entries(p, c, a);
-      }
+      for (int u = 0; u < U; ++u)
+        load_entry(p0 + u * TN, c[u], a[u]);
+    };
+    // The B rows of U entries (column -1: none) and their FMAs.
+    const auto consume = [&](const int32_t(&c)[U], const Acc(&a)[U], auto &&in_flight) {
       X b[U][NV][VEC];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
@@ -240,8 +245,7 @@ __device__ __forceinline__ void spmm_row_group(const Rows &A, int64_t row, bool 
           }
         }
       }
-      if constexpr (PIPE)
-        load_entries(p + U * TN, cn, an);
+      in_flight();  // loads to overlap with the B rows
 #pragma unroll
       for (int u = 0; u < U; ++u)
 #pragma unroll
@@ -249,6 +253,50 @@ __device__ __forceinline__ void spmm_row_group(const Rows &A, int64_t row, bool 
 #pragma unroll
           for (int v = 0; v < VEC; ++v)
             acc[nv][v] = fma(a[u], to_acc<Acc>(b[u][nv][v]), acc[nv][v]);
+    };
+    if constexpr (ENTRIES == kEntriesShared) {
+      int32_t cn;
+      Acc an;
+      load_entry(s + tk, cn, an);
+      for (int32_t base = 0; base < longest; base += TK) {
+        const int32_t cm = cn;
+        const Acc am = an;
+        load_entry(s + base + TK + tk, cn, an);
+        const int32_t cnt = min(TK, longest - base);
+        for (int32_t u0 = 0; u0 < cnt; u0 += U) {
+          int32_t c[U];
+          Acc a[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int32_t src = u0 + u;
+            c[u] = __shfl_sync(0xffffffffu, cm, src & (TK - 1), TK);
+            a[u] = __shfl_sync(0xffffffffu, am, src & (TK - 1), TK);
+            if (src >= cnt)
+              c[u] = -1;
+          }
+          consume(c, a, [] {});
+        }
+      }
+    } else {
+      int32_t cn[U];
+      Acc an[U];
+      if constexpr (ENTRIES == kEntriesAhead)
+        load_entries(s + tn, cn, an);
+      for (int32_t p = s + tn; p < e; p += U * TN) {
+        int32_t c[U];
+        Acc a[U];
+        if constexpr (ENTRIES == kEntriesAhead) {
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            c[u] = cn[u];
+            a[u] = an[u];
+          }
+          consume(c, a, [&] { load_entries(p + U * TN, cn, an); });
+        } else {
+          load_entries(p, c, a);
+          consume(c, a, [] {});
+        }
+      }
     }
     for (int o = TK; o < TK * TN; o <<= 1)
 #pragma unroll

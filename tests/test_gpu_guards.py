@@ -19,7 +19,9 @@ SUITES = ["test_gpu_spmv.py", "test_gpu_edges.py", "test_gpu_spmm.py", "test_gpu
 
 
 def test_parity_suites_under_guard_build():
-    assert os.path.exists(GUARD_LIB), "build the guard library: python -m perf_libs_sparse_b200.build --guards"
+    from perf_libs_sparse_b200 import build as b
+
+    assert b.build(guards=True) == GUARD_LIB  # rebuilt only when older than its sources
     env = dict(os.environ, PERFLIBS_B200_LIBRARY=GUARD_LIB)
     r = subprocess.run(
         [sys.executable, "-m", "pytest", "-q", "-x", "-m", "gpu", "-p", "no:cacheprovider",

@@ -215,9 +215,51 @@ def test_staged_spmm_vs_oracle(dt):
                 assert err <= tol, (mm, k, ldb, err)
 
 
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+def test_shared_entries_spmm_vs_oracle(dt):
+    """The row-group kernel with shared entry loads (a row's lanes load its
+    entries together and pass them round): ragged rows with empty ones in
+    one warp (the warp runs to its longest row), a stencil, a band; aligned
+    and unaligned k, beta != 0. Each result equals the plain row-group
+    kernel's bit for bit (same per-lane summation order) and the oracle
+    within the tolerance."""
+    import torch
+
+    rng = np.random.default_rng(11)
+    tol = 1e-12 if dt == np.float64 else 1e-5
+    tdt = torch.float64 if dt == np.float64 else torch.float32
+    rpr, cr, vr = W.random_csr(3000, 2000, 60, rng, empty_frac=0.3)
+    cases = [(3000, 2000, rpr, cr, vr), W.stencil_27pt(12, seed=2), W.banded_csr(4000, 7, rng)]
+    for (m, n, rp, c, v) in cases:
+        v = v.astype(dt)
+        A = pls.SpMat.csr(m, n, rp, c, v)
+        for k in (8, 13, 32, 72, 130):
+            Bd = rng.uniform(-1, 1, (n, k)).astype(dt)
+            C0 = rng.uniform(-1, 1, (m, k)).astype(dt)
+            Bt = torch.tensor(Bd, device="cuda")
+            out = {}
+            for path in (0, 2):
+                A.set_spmm_path(path)
+                Ct = torch.tensor(C0, device="cuda")
+                torch.cuda.synchronize()
+                A.spmm_dev(Bt.data_ptr(), k, k, Ct.data_ptr(), k, 1.25, -0.5)
+                torch.cuda.synchronize()
+                out[path] = (Ct.cpu().numpy(), A.spmm_info()["path"])
+            vec = 16 // np.dtype(dt).itemsize
+            cols = -(-k // vec) if k % vec == 0 else k
+            assert out[2][1] == (2 if cols >= 4 else 0), (m, k, out[2][1])
+            np.testing.assert_array_equal(out[0][0], out[2][0])
+            v64, B64, C064 = v.astype(np.float64), Bd.astype(np.float64), C0.astype(np.float64)
+            ref = spmm_ref(rp, c, v64, B64, 1.25, -0.5, C064)
+            assert scaled_err(out[2][0].astype(np.float64), ref, rp, c, v64, B64, 1.25, -0.5,
+                              C064) <= tol, (m, k)
+        A.destroy()
+
+
 def test_random_matrix_keeps_row_group_kernel():
     """B rows of a random matrix are not reused within row blocks: the
-    staged path declines and the row-group kernel gives the result."""
+    staged path declines and a row-group kernel (plain or with shared
+    entries, whichever measured faster) gives the result."""
     rng = np.random.default_rng(8)
     rp, c, v = W.random_csr(3000, 3000, 20, rng)
     Bd = rng.uniform(-1, 1, (3000, 32))
@@ -226,7 +268,7 @@ def test_random_matrix_keeps_row_group_kernel():
     Cm = pls.SpMat.null(3000, 32)
     assert pls.spmm_exec(pls.OPERATION_NOTRANS, pls.OPERATION_NOTRANS, 1.0, A, B, 0.0, Cm) == 0
     info = A.spmm_info()
-    assert info["tile_rows"] == 0 and info["path"] == 0, info
+    assert info["tile_rows"] == 0 and info["path"] in (0, 2), info
     ref = spmm_ref(rp, c, v, Bd, 1.0, 0.0, None)
     assert scaled_err(Cm.export_dense(), ref, rp, c, v, Bd, 1.0, 0.0, None) <= 1e-12
 
@@ -248,7 +290,7 @@ def test_spmm_measured_choice_matches_oracle():
         A.spmm_dev(Bt.data_ptr(), k, k, Ct.data_ptr(), k, 0.75, 1.5, s.cuda_stream)
         s.synchronize()
         info = A.spmm_info()
-        assert info["path"] in (0, 1) and info["ms_staged"] > 0 and info["ms_rows"] > 0, info
+        assert info["path"] in (0, 1, 2) and info["ms_staged"] > 0 and info["ms_rows"] > 0, info
         ref = spmm_ref(rp, c, v, Bd, 0.75, 1.5, C0)
         assert scaled_err(Ct.cpu().numpy(), ref, rp, c, v, Bd, 0.75, 1.5, C0) <= 1e-12
 
