@@ -45,6 +45,8 @@ def main():
     ap.add_argument("--storage", default="native", choices=["native", "fp32", "bf16"])
     ap.add_argument("--fp32-api", action="store_true")
     ap.add_argument("--reps", type=int, default=10)
+    ap.add_argument("--spmm-path", type=int, default=-1,
+                    help="-1 measured choice, 0 row group, 1 staged, 2 row group with shared entries")
     args = ap.parse_args()
 
     m, n, rp, c, v = make(args.matrix, args.rows)
@@ -65,6 +67,7 @@ def main():
     s = torch.cuda.Stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if args.k > 0:
+        A.set_spmm_path(args.spmm_path)
         B = torch.rand((n, args.k), dtype=tdt, device="cuda") * 2 - 1
         Cm = torch.empty((m, args.k), dtype=tdt, device="cuda")
         run = lambda: A.spmm_dev(B.data_ptr(), args.k, args.k, Cm.data_ptr(), args.k, 1.0, 0.0, s.cuda_stream)
