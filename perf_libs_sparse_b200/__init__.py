@@ -114,6 +114,7 @@ def lib():
             "perflibs_b200_spmat_spmm_info": [vp, vp, vp, vp, vp, vp, vp],
             "perflibs_b200_spmat_set_spmm_path": [vp, i32],
             "perflibs_b200_spmat_set_host_bands": [vp, i32],
+            "perflibs_b200_spmat_create_csr_d_dev": [vp, i32, i32, vp, vp, vp, vp],
             "perflibs_b200_spmat_host_bands_used": [vp, vp],
             "perflibs_b200_spmat_tune_source": [vp, vp],
             "perflibs_b200_tune_cache_save": [C.c_char_p],
@@ -194,6 +195,17 @@ class SpMat:
         if check:
             _check(st, "create_csr")
         return M
+
+    @staticmethod
+    def csr_dev(m, n, row_ptr_ptr: int, col_ptr: int, vals_ptr: int, stream: int = 0):
+        """FP64 CSR handle from arrays already on the device (int32 row
+        pointers and columns, double values; copied), e.g. torch tensors'
+        data_ptr()."""
+        h = C.c_void_p()
+        _check(lib().perflibs_b200_spmat_create_csr_d_dev(
+            C.byref(h), m, n, C.c_void_p(row_ptr_ptr), C.c_void_p(col_ptr), C.c_void_p(vals_ptr),
+            C.c_void_p(stream)), "create_csr_d_dev")
+        return SpMat(h, np.float64)
 
     @staticmethod
     def coo(m, n, row, col, vals, flags=0, check=True):
