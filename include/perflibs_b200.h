@@ -41,13 +41,14 @@ perflibs_status_t perflibs_b200_spmv_exec_s_dev(
  * A must already hold its SELL-C-sigma layout (perflibs_spmv_optimize chose
  * SELL, or perflibs_b200_spmat_build_sell / force_config + optimize); other
  * formats return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR. The partial sums of
- * sliced wide chunks go to one fixed 16 MiB device array (2^21 FP64
- * elements) that every GPU loading the library holds until exit; a matrix
- * that needs more returns PERFLIBS_STATUS_INPUT_PARAMETER_ERROR with the
- * sizes in the handle's error message. The first call on a device looks the
- * array's address up (cudaGetSymbolAddress), so make that first call before
- * any stream capture. All calls share the array: calls that overlap on the
- * GPU race, so serialise them (one stream, or events between streams). */
+ * sliced wide chunks and their completion counts go to fixed device arrays
+ * (2^21 FP64 elements and 2^18 counts, 17 MiB) that every GPU loading the
+ * library holds until exit; a matrix that needs more returns
+ * PERFLIBS_STATUS_INPUT_PARAMETER_ERROR with the sizes in the handle's
+ * error message. The first call on a device looks the arrays' addresses up
+ * (cudaGetSymbolAddress), so make that first call before any stream
+ * capture. All calls share the arrays: calls that overlap on the GPU race,
+ * so serialise them (one stream, or events between streams). */
 perflibs_status_t perflibs_b200_spmv_exec_d_noalloc(double alpha,
                                                     perflibs_spmat_t A,
                                                     const double *x,
