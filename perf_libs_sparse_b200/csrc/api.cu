@@ -597,10 +597,10 @@ perflibs_status_t spmv_exec_host(int trans, X alpha, Mat *A, const X *x, X beta,
     A->ybuf.reserve(sizeof(X) * ylen);
     if (xlen > 0)
       PLS_CUDA(cudaMemcpyAsync(A->xbuf.p, x, sizeof(X) * xlen, cudaMemcpyHostToDevice, s));
+    // With beta = 0 every kernel writes all of y without reading it (the
+    // reference's y = alpha*A*x: old values, NaN included, do not propagate).
     if (beta != X(0))
       PLS_CUDA(cudaMemcpyAsync(A->ybuf.p, y, sizeof(X) * ylen, cudaMemcpyHostToDevice, s));
-    else
-      PLS_CUDA(cudaMemsetAsync(A->ybuf.p, 0, sizeof(X) * ylen, s));
     const int n_bands = band_count<X>(A, trans, alpha, xlen, ylen);
     if (n_bands > 1 && spmv_banded<X>(A, n_bands, alpha, beta, y, s))
       return PERFLIBS_STATUS_SUCCESS;
@@ -626,9 +626,7 @@ perflibs_status_t spmv_exec_dev(int trans, X alpha, Mat *A, const X *x, X beta, 
     align_operation(A, trans);
     prepare_values(A);
     cudaStream_t s = stream ? (cudaStream_t)stream : stream_of(A);
-    const int64_t ylen = trans == PERFLIBS_SPARSE_OPERATION_NOTRANS ? A->m : A->n;
-    if (ylen > 0 && beta == X(0))
-      PLS_CUDA(cudaMemsetAsync(y, 0, sizeof(X) * ylen, s));
+    // beta = 0: every kernel writes all of y without reading it.
     return spmv_device<X>(trans, alpha, A, x, beta, y, s);
   });
 }
@@ -845,9 +843,7 @@ perflibs_status_t spmm_impl(int transA, int transB, X alpha, Mat *A, Mat *B, X b
           strided_copy<X>(cc, c_sr, cw.as<X>(), 1, m, s);
         cc = cw.as<X>();
       }
-      if (beta == X(0) && m > 0)
-        PLS_CUDA(cudaMemsetAsync(cc, 0, sizeof(X) * m, s));
-      spmv_device<X>(transA, alpha, A, bc, beta, cc, s);
+      spmv_device<X>(transA, alpha, A, bc, beta, cc, s);  // beta = 0: cc written, not read
       if (c_sr != 1)
         strided_copy<X>(cc, 1, cdst, c_sr, m, s);
     }
