@@ -286,13 +286,18 @@ def run_b200(args):
         return max_over_ranks(ms, dev) / K
 
     K, Wm = args.steps, max(args.warmup, 3)
-    # Keep the GPU busy ~0.5 s before the timed region so that the clock
-    # samples see the kernel under load.
+    # Keep the GPU busy ~0.5 s before each timed region, so that the clock
+    # samples see the kernel under load and every arm (tuned, plain CSR, the
+    # selector's) is timed in the same sustained power state.
     soak = max(1, int(args.soak_seconds / max(bytes_step / 6.0e12, 1e-6)))
+
+    def measure(M, label="untimed"):
+        timed(M, soak, 1)
+        return timed(M, K, Wm, label)
+
     with ClockSampler(local) as clk:
-        timed(A, soak, 1)
-        ms_tuned = timed(A, K, Wm, "timed")
-    ms_plain = timed(A_plain, K, Wm)
+        ms_tuned = measure(A, "timed")
+    ms_plain = measure(A_plain)
 
     # Parity of the timed result (full size) against the oracle.
     import oracle
@@ -337,7 +342,7 @@ def run_b200(args):
             t0 = time.perf_counter()
             assert As.optimize() == 0
             t_sel = time.perf_counter() - t0
-            ms_s = timed(As, K, Wm)
+            ms_s = measure(As)
             step(As)
             torch.cuda.synchronize()
             ys = yd.cpu().numpy()
