@@ -48,8 +48,10 @@ __global__ void __launch_bounds__(256)
   if (skip_len > 0 && e - s > skip_len)
     return;  // uniform across the row's lanes
   // Groups of G elements per lane: all value / column loads of a group are
-  // issued (predicated past the row end) before the dependent x gathers.
-  constexpr int G = 4;
+  // issued (predicated past the row end) before the dependent x gathers. One
+  // lane per row takes 8, so the short rows that configuration is picked for
+  // (stencils) cost one stream round trip and one gather round trip.
+  constexpr int G = TPR == 1 ? 8 : 4;
   const L2Policy pol = make_l2_policy();
   Acc sum = 0;
   for (int32_t j = s + sub; j < e; j += G * TPR) {
