@@ -114,23 +114,45 @@ static bool launch_spmm_csr(const CsrDev &c, int32_t m, const X *B, int64_t ldb,
   return shared;
 }
 
+// Vector width (columns per load) of the row-group kernel for k columns:
+// 16-byte vectors when B and C allow them, else one column. With shared
+// entries the width is halved while that leaves fewer than 4 column lanes per
+// row (FP32 k = 8: two lanes of 4 columns become four of 2), since the
+// shared loads need at least 4 lanes per row.
+template <class X>
+static int rows_vec(const CsrDev &c, int32_t m, const X *B, int64_t ldb, const X *C,
+                    int64_t ldc, int k, bool shared) {
+  constexpr int VMAX = 16 / sizeof(X);
+  const bool aligned = k >= VMAX && ((uintptr_t)B % 16 == 0) && ((uintptr_t)C % 16 == 0) &&
+                       (ldb % VMAX == 0) && (ldc % VMAX == 0);
+  int vec = aligned ? VMAX : 1;
+  const double mean = (double)c.nnz / std::max<int32_t>(m, 1);
+  while (shared && vec > 1 && !shared_entries_fit(rows_shape(k, vec, mean)))
+    vec /= 2;
+  return vec;
+}
+
 // Row-group SpMM (the launch half of spmm_csr), with 32-bit address
 // arithmetic when `off32` and the offsets fit, and shared entry loads when
 // `shared` and the lane shape allows them (returns whether they ran).
 template <class X>
 static bool spmm_rows(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64_t ldc,
                       int k, X alpha, X beta, bool off32, bool shared, cudaStream_t s) {
-  constexpr int VMAX = 16 / sizeof(X);
-  const bool aligned = k >= VMAX && ((uintptr_t)B % 16 == 0) && ((uintptr_t)C % 16 == 0) &&
-                       (ldb % VMAX == 0) && (ldc % VMAX == 0);
+  const int vec = rows_vec<X>(c, m, B, ldb, C, ldc, k, shared);
   bool ran = false;
   with_vt(c.evt(), [&](auto tag) {
     using V = typename decltype(tag)::type;
     if constexpr (std::is_same_v<X, float> && std::is_same_v<V, double>) {
       throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE, "FP64 storage with FP32 API");
     } else {
-      if (aligned)
-        ran = launch_spmm_csr<VMAX, V, X>(c, m, B, ldb, C, ldc, k, alpha, beta, off32, shared, s);
+      if constexpr (sizeof(X) == 4) {
+        if (vec == 4) {
+          ran = launch_spmm_csr<4, V, X>(c, m, B, ldb, C, ldc, k, alpha, beta, off32, shared, s);
+          return;
+        }
+      }
+      if (vec == 2)
+        ran = launch_spmm_csr<2, V, X>(c, m, B, ldb, C, ldc, k, alpha, beta, off32, shared, s);
       else
         ran = launch_spmm_csr<1, V, X>(c, m, B, ldb, C, ldc, k, alpha, beta, off32, shared, s);
     }
@@ -173,10 +195,9 @@ void spmm_csr(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
   }
   if (t.choice_sig != sig) {
     const bool staged_ok = spmm_tiled<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s, false);
-    constexpr int VMAX = 16 / sizeof(X);
-    const bool vec_ok = k >= VMAX && ((uintptr_t)B % 16 == 0) && (ldb % VMAX == 0);
+    const int vec_s = rows_vec<X>(c, m, B, ldb, C, ldc, k, true);
     const bool shared_ok = shared_entries_fit(
-        rows_shape(k, vec_ok ? VMAX : 1, (double)c.nnz / std::max<int32_t>(m, 1)));
+        rows_shape(k, vec_s, (double)c.nnz / std::max<int32_t>(m, 1)));
     t.choice = 0;
     t.ms_rows = t.ms_staged = 0.f;
     if (staged_ok || fits32 || shared_ok) {

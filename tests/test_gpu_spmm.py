@@ -220,9 +220,10 @@ def test_shared_entries_spmm_vs_oracle(dt):
     """The row-group kernel with shared entry loads (a row's lanes load its
     entries together and pass them round): ragged rows with empty ones in
     one warp (the warp runs to its longest row), a stencil, a band; aligned
-    and unaligned k, beta != 0. Each result equals the plain row-group
-    kernel's bit for bit (same per-lane summation order) and the oracle
-    within the tolerance."""
+    and unaligned k, beta != 0. Each result matches the oracle within the
+    tolerance, and equals the plain row-group kernel's bit for bit where
+    that kernel also keeps each row's nonzeros in one lane (same summation
+    order)."""
     import torch
 
     rng = np.random.default_rng(11)
@@ -245,10 +246,13 @@ def test_shared_entries_spmm_vs_oracle(dt):
                 A.spmm_dev(Bt.data_ptr(), k, k, Ct.data_ptr(), k, 1.25, -0.5)
                 torch.cuda.synchronize()
                 out[path] = (Ct.cpu().numpy(), A.spmm_info()["path"])
+            # Shared entries need at least 4 column lanes per row; the vector
+            # width is halved until there are (FP32 k = 8: 4 lanes of 2).
+            assert out[2][1] == 2, (m, k, out[2][1])
             vec = 16 // np.dtype(dt).itemsize
             cols = -(-k // vec) if k % vec == 0 else k
-            assert out[2][1] == (2 if cols >= 4 else 0), (m, k, out[2][1])
-            np.testing.assert_array_equal(out[0][0], out[2][0])
+            if cols > 2:  # the plain kernel also gives each row one lane group (TN = 1)
+                np.testing.assert_array_equal(out[0][0], out[2][0])
             v64, B64, C064 = v.astype(np.float64), Bd.astype(np.float64), C0.astype(np.float64)
             ref = spmm_ref(rp, c, v64, B64, 1.25, -0.5, C064)
             assert scaled_err(out[2][0].astype(np.float64), ref, rp, c, v64, B64, 1.25, -0.5,
