@@ -312,7 +312,11 @@ perflibs_status_t perflibs_b200_spmat_set_selector(perflibs_spmat_t A,
  * (ldc_i) and its own k_i) in ONE persistent kernel launch: a work list of
  * (instance, row tile) items is consumed by a grid sized to the SMs through
  * an atomic counter, so uneven instances balance without waits. exec
- * replays a CUDA graph holding the counter reset and the launch. */
+ * replays a CUDA graph holding the counter reset and the launch. The batch
+ * keeps a copy of each CSR instance's column indices and values, packed side
+ * by side at creation (one 8-byte load per entry); values changed in the
+ * handle afterwards (perflibs_spmat_update) are not seen until the batch is
+ * created again. BSR instances are read from their handles. */
 typedef struct perflibs_b200_batch_s *perflibs_b200_batch_t;
 perflibs_status_t perflibs_b200_batch_create(
     perflibs_b200_batch_t *Bt, int32_t count, const perflibs_spmat_t *mats,

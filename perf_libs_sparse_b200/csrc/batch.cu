@@ -30,6 +30,7 @@ struct InstDesc {
   const int32_t *rp;
   const int32_t *col;
   const float *val;
+  const int2 *cv;  // CSR: the batch's packed (column, value) copy
   const float *B;
   float *C;
   int64_t ldb, ldc;
@@ -89,11 +90,18 @@ __global__ void __launch_bounds__(256)
                       d.layout == PERFLIBS_ROW_MAJOR};
       batch_rows<BsrRows, OFF32>(A, d, w, lane, alpha, beta, beta_nz, pol);
     } else {
-      const CsrRows<float> A{d.rp, d.col, d.val};
-      batch_rows<CsrRows<float>, OFF32>(A, d, w, lane, alpha, beta, beta_nz, pol);
+      const PackedRows A{d.rp, d.cv};
+      batch_rows<PackedRows, OFF32>(A, d, w, lane, alpha, beta, beta_nz, pol);
     }
     it = __shfl_sync(0xffffffffu, next, 0);
   }
+}
+
+__global__ void k_pack_cv(int64_t nnz, const int32_t *__restrict__ col,
+                          const float *__restrict__ val, int2 *__restrict__ cv) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nnz)
+    cv[i] = make_int2(col[i], __float_as_int(val[i]));
 }
 
 }  // namespace
@@ -106,6 +114,7 @@ struct perflibs_b200_batch_s {
   std::vector<pls::InstDesc> host;
   std::vector<double> work_per_row;  // nonzeros per row x k (for ordering)
   pls::DevBuf inst, items, counter;
+  pls::DevBuf packed;  // CSR instances' (column, value) pairs, packed at creation
   int64_t n_items = 0;
   int32_t tile = 0;
   int grid = 0;
@@ -256,6 +265,27 @@ perflibs_status_t perflibs_b200_batch_create(perflibs_b200_batch_t *out, int32_t
       B->host.push_back(d);
       B->work_per_row.push_back(((double)A->nnz / std::max(A->m, 1) + 1.0) * std::max(k[i], 1));
     }
+    // One 8-byte load per CSR entry instead of two 4-byte ones: each of a
+    // row's column lanes loads every entry, so the loads are a large share
+    // of the kernel's instructions.
+    int64_t packed = 0;
+    for (int32_t i = 0; i < count; ++i)
+      if (!B->host[i].is_bsr)
+        packed += mats[i]->csr.nnz;
+    B->packed.reserve(sizeof(int2) * std::max<int64_t>(packed, 1));
+    packed = 0;
+    for (int32_t i = 0; i < count; ++i) {
+      InstDesc &d = B->host[i];
+      if (d.is_bsr)
+        continue;
+      const int64_t nnz = mats[i]->csr.nnz;
+      d.cv = B->packed.as<int2>() + packed;
+      if (nnz > 0)
+        k_pack_cv<<<(unsigned)div_up(nnz, 256), 256, 0, B->stream>>>(nnz, d.col, d.val,
+                                                                    B->packed.as<int2>() + packed);
+      packed += nnz;
+    }
+    PLS_LAUNCH_CHECK();
     B->inst.reserve(sizeof(InstDesc) * count);
     PLS_CUDA(cudaMemcpyAsync(B->inst.p, B->host.data(), sizeof(InstDesc) * count,
                              cudaMemcpyHostToDevice, B->stream));

@@ -70,6 +70,13 @@ __device__ __forceinline__ int32_t ld_stream(const int32_t *p, uint64_t pol) {
   asm("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
   return v;
 }
+__device__ __forceinline__ int2 ld_stream(const int2 *p, uint64_t pol) {
+  int2 v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.s32 {%0, %1}, [%2], %3;"
+      : "=r"(v.x), "=r"(v.y)
+      : "l"(p), "l"(pol));
+  return v;
+}
 __device__ __forceinline__ uint32_t ld_stream(const uint32_t *p, uint64_t pol) {
   uint32_t v;
   asm("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));

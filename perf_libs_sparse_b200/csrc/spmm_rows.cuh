@@ -94,6 +94,25 @@ template <class Val> struct CsrRows {
   }
 };
 
+// FP32 CSR with each entry's column and value side by side (int2: column,
+// value bits), so one 8-byte load brings both.
+struct PackedRows {
+  using V = float;
+  const int32_t *rp;
+  const int2 *cv;
+  __device__ __forceinline__ void range(int64_t r, int32_t &s, int32_t &e, int32_t &aux) const {
+    s = __ldg(rp + r);
+    e = __ldg(rp + r + 1);
+    aux = 0;
+  }
+  __device__ __forceinline__ void entry(int32_t q, int32_t, int32_t &c, float &a,
+                                        const L2Policy &pol) const {
+    const int2 t = ld_stream(cv + q, pol.stream);
+    c = t.x;
+    a = __int_as_float(t.y);
+  }
+};
+
 // FP32 CSR or BSR behind one runtime flag (the batched kernel mixes both).
 // A BSR scalar row r is row i = r % bs of block row r / bs; its entries
 // q in [rp[br] * bs, rp[br + 1] * bs) are column jj = q % bs of block q / bs,
