@@ -313,10 +313,12 @@ perflibs_status_t perflibs_b200_spmat_set_selector(perflibs_spmat_t A,
  * (instance, row tile) items is consumed by a grid sized to the SMs through
  * an atomic counter, so uneven instances balance without waits. exec
  * replays a CUDA graph holding the counter reset and the launch. The batch
- * keeps a copy of each CSR instance's column indices and values, packed side
- * by side at creation (one 8-byte load per entry); values changed in the
- * handle afterwards (perflibs_spmat_update) are not seen until the batch is
- * created again. BSR instances are read from their handles. */
+ * keeps its own copy of every instance's entries, column index and value
+ * side by side (one 8-byte load per entry; BSR instances expanded to scalar
+ * rows, blocks in stored order), made at creation: values changed in the
+ * handles afterwards (perflibs_spmat_update) are not seen until the batch is
+ * created again. The copy takes 8 bytes of device memory per stored scalar
+ * entry. */
 typedef struct perflibs_b200_batch_s *perflibs_b200_batch_t;
 perflibs_status_t perflibs_b200_batch_create(
     perflibs_b200_batch_t *Bt, int32_t count, const perflibs_spmat_t *mats,

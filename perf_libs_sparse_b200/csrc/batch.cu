@@ -11,8 +11,10 @@
 //
 // Inside an item, rows go through the row-group loop of spmm_rows.cuh with
 // the instance's own lane shape (TK lanes over C's columns, 16-byte vectors
-// when its B and C allow, TN lanes over a row's entries); a BSR instance is
-// read as scalar rows whose entries are (block, column-in-block) pairs.
+// when its B and C allow, TN lanes over a row's entries). Every instance is
+// read from the batch's own copy of its entries, (column, value) side by
+// side; a BSR instance is expanded at creation into scalar rows whose
+// entries are its blocks' rows in stored order.
 #include <algorithm>
 #include <cstring>
 #include <numeric>
@@ -42,8 +44,7 @@ struct Item {
   int32_t inst, row0, row1, pad;
 };
 
-// One item's rows with the instance's row kind (CSR or BSR, resolved at
-// compile time) and vector shape.
+// One item's rows with the instance's vector shape.
 template <class Rows, bool OFF32>
 __device__ __forceinline__ void batch_rows(const Rows &A, const InstDesc &d, const Item &w,
                                            int lane, float alpha, float beta, int beta_nz,
@@ -82,17 +83,8 @@ __global__ void __launch_bounds__(256)
       next = atomicAdd(counter, 1ull);
     const Item w = items[it];
     const InstDesc d = inst[w.inst];
-    if (d.is_bsr) {
-      int lg = 0;
-      while ((1 << lg) < d.bs)
-        ++lg;
-      const BsrRows A{d.rp, d.col, d.val, d.bs, (1 << lg) == d.bs ? lg : -1,
-                      d.layout == PERFLIBS_ROW_MAJOR};
-      batch_rows<BsrRows, OFF32>(A, d, w, lane, alpha, beta, beta_nz, pol);
-    } else {
-      const PackedRows A{d.rp, d.cv};
-      batch_rows<PackedRows, OFF32>(A, d, w, lane, alpha, beta, beta_nz, pol);
-    }
+    const PackedRows A{d.rp, d.cv};
+    batch_rows<PackedRows, OFF32>(A, d, w, lane, alpha, beta, beta_nz, pol);
     it = __shfl_sync(0xffffffffu, next, 0);
   }
 }
@@ -102,6 +94,42 @@ __global__ void k_pack_cv(int64_t nnz, const int32_t *__restrict__ col,
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < nnz)
     cv[i] = make_int2(col[i], __float_as_int(val[i]));
+}
+
+// A BSR instance as scalar CSR rows. Row i of block row br holds, block by
+// block in stored order, the bs entries of the block's row i: it starts
+// after the br block rows before it (bs * bs entries per block) and the i
+// rows of br before it (bs entries per block of br).
+__global__ void k_bsr_scalar_rp(int32_t mb, int32_t bs, const int32_t *__restrict__ rp,
+                                int32_t *__restrict__ srp) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r > (int64_t)mb * bs)
+    return;
+  if (r == (int64_t)mb * bs) {
+    srp[r] = rp[mb] * bs * bs;
+    return;
+  }
+  const int32_t br = (int32_t)(r / bs), i = (int32_t)(r % bs);
+  srp[r] = rp[br] * bs * bs + i * bs * (rp[br + 1] - rp[br]);
+}
+
+// The entries of scalar row r: (column, value) for every block of its block
+// row and every column jj of the block, in that order (the order the BSR
+// kernels add them in); blocks are row-major (value i*bs + jj) or
+// column-major (jj*bs + i).
+__global__ void k_bsr_pack(int32_t mb, int32_t bs, int rowmajor, const int32_t *__restrict__ rp,
+                           const int32_t *__restrict__ col, const float *__restrict__ val,
+                           const int32_t *__restrict__ srp, int2 *__restrict__ cv) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= (int64_t)mb * bs)
+    return;
+  const int32_t br = (int32_t)(r / bs), i = (int32_t)(r % bs);
+  int64_t pos = srp[r];
+  for (int32_t b = rp[br]; b < rp[br + 1]; ++b)
+    for (int32_t jj = 0; jj < bs; ++jj) {
+      const float v = val[(int64_t)b * bs * bs + (rowmajor ? i * bs + jj : jj * bs + i)];
+      cv[pos++] = make_int2(col[b] * bs + jj, __float_as_int(v));
+    }
 }
 
 }  // namespace
@@ -114,7 +142,8 @@ struct perflibs_b200_batch_s {
   std::vector<pls::InstDesc> host;
   std::vector<double> work_per_row;  // nonzeros per row x k (for ordering)
   pls::DevBuf inst, items, counter;
-  pls::DevBuf packed;  // CSR instances' (column, value) pairs, packed at creation
+  pls::DevBuf packed;  // every instance's (column, value) pairs, packed at creation
+  pls::DevBuf scalar_rp;  // row pointers of the BSR instances' scalar rows
   int64_t n_items = 0;
   int32_t tile = 0;
   int grid = 0;
@@ -244,7 +273,7 @@ perflibs_status_t perflibs_b200_batch_create(perflibs_b200_batch_t *out, int32_t
         d.col = A->csr.col.as<int32_t>();
         d.val = A->csr.vals.as<float>();
       }
-      if (d.is_bsr && (int64_t)A->bsr.nnzb * d.bs > INT32_MAX) {
+      if (d.is_bsr && (int64_t)A->bsr.nnzb * d.bs * d.bs > INT32_MAX) {
         delete B;
         *out = nullptr;
         return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
@@ -265,25 +294,42 @@ perflibs_status_t perflibs_b200_batch_create(perflibs_b200_batch_t *out, int32_t
       B->host.push_back(d);
       B->work_per_row.push_back(((double)A->nnz / std::max(A->m, 1) + 1.0) * std::max(k[i], 1));
     }
-    // One 8-byte load per CSR entry instead of two 4-byte ones: each of a
-    // row's column lanes loads every entry, so the loads are a large share
-    // of the kernel's instructions.
-    int64_t packed = 0;
-    for (int32_t i = 0; i < count; ++i)
-      if (!B->host[i].is_bsr)
-        packed += mats[i]->csr.nnz;
+    // Every instance is read as scalar CSR rows whose column and value sit
+    // side by side (one 8-byte load per entry: each of a row's column lanes
+    // loads every entry, so these loads are a large share of the kernel's
+    // instructions); BSR instances are expanded to such rows here.
+    int64_t packed = 0, srows = 0;
+    for (int32_t i = 0; i < count; ++i) {
+      const InstDesc &d = B->host[i];
+      packed += d.is_bsr ? mats[i]->bsr.nnzb * d.bs * d.bs : mats[i]->csr.nnz;
+      if (d.is_bsr)
+        srows += (int64_t)d.m + 1;
+    }
     B->packed.reserve(sizeof(int2) * std::max<int64_t>(packed, 1));
-    packed = 0;
+    B->scalar_rp.reserve(sizeof(int32_t) * std::max<int64_t>(srows, 1));
+    packed = srows = 0;
     for (int32_t i = 0; i < count; ++i) {
       InstDesc &d = B->host[i];
-      if (d.is_bsr)
-        continue;
-      const int64_t nnz = mats[i]->csr.nnz;
-      d.cv = B->packed.as<int2>() + packed;
-      if (nnz > 0)
-        k_pack_cv<<<(unsigned)div_up(nnz, 256), 256, 0, B->stream>>>(nnz, d.col, d.val,
-                                                                    B->packed.as<int2>() + packed);
-      packed += nnz;
+      int2 *cv = B->packed.as<int2>() + packed;
+      if (d.is_bsr) {
+        const BsrDev &b = mats[i]->bsr;
+        int32_t *srp = B->scalar_rp.as<int32_t>() + srows;
+        const int64_t rows = (int64_t)b.mb * b.bs;
+        k_bsr_scalar_rp<<<(unsigned)div_up(rows + 1, 256), 256, 0, B->stream>>>(b.mb, b.bs, d.rp,
+                                                                                srp);
+        if (rows > 0)
+          k_bsr_pack<<<(unsigned)div_up(rows, 256), 256, 0, B->stream>>>(
+              b.mb, b.bs, d.layout == PERFLIBS_ROW_MAJOR, d.rp, d.col, d.val, srp, cv);
+        d.rp = srp;
+        srows += rows + 1;
+        packed += b.nnzb * b.bs * b.bs;
+      } else {
+        const int64_t nnz = mats[i]->csr.nnz;
+        if (nnz > 0)
+          k_pack_cv<<<(unsigned)div_up(nnz, 256), 256, 0, B->stream>>>(nnz, d.col, d.val, cv);
+        packed += nnz;
+      }
+      d.cv = cv;
     }
     PLS_LAUNCH_CHECK();
     B->inst.reserve(sizeof(InstDesc) * count);

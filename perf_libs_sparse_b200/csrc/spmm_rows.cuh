@@ -113,68 +113,6 @@ struct PackedRows {
   }
 };
 
-// FP32 CSR or BSR behind one runtime flag (the batched kernel mixes both).
-// A BSR scalar row r is row i = r % bs of block row r / bs; its entries
-// q in [rp[br] * bs, rp[br + 1] * bs) are column jj = q % bs of block q / bs,
-// whose value sits at i * bs + jj (row-major blocks) or jj * bs + i
-// (column-major blocks).
-struct MixedRows {
-  using V = float;
-  const int32_t *rp, *col;
-  const float *val;
-  int32_t bs, rowmajor, is_bsr;
-  __device__ __forceinline__ void range(int64_t r, int32_t &s, int32_t &e, int32_t &aux) const {
-    if (!is_bsr) {
-      s = __ldg(rp + r);
-      e = __ldg(rp + r + 1);
-      aux = 0;
-    } else {
-      const int32_t br = (int32_t)(r / bs);
-      aux = (int32_t)r - br * bs;
-      s = __ldg(rp + br) * bs;
-      e = __ldg(rp + br + 1) * bs;
-    }
-  }
-  __device__ __forceinline__ void entry(int32_t q, int32_t aux, int32_t &c, float &a,
-                                        const L2Policy &pol) const {
-    if (!is_bsr) {
-      c = ld_stream(col + q, pol.stream);
-      a = ld_stream(val + q, pol.stream);
-    } else {
-      const int32_t b = q / bs, jj = q - b * bs;
-      c = __ldg(col + b) * bs + jj;
-      a = ld_stream(val + (int64_t)b * bs * bs + (rowmajor ? aux * bs + jj : jj * bs + aux),
-                    pol.stream);
-    }
-  }
-};
-
-// FP32 BSR seen as scalar rows (the batched kernel's BSR instances), with
-// the block size's log2 when it is a power of two (shifts instead of
-// divisions), else -1.
-struct BsrRows {
-  using V = float;
-  const int32_t *rp, *col;
-  const float *val;
-  int32_t bs, lg_bs, rowmajor;
-  __device__ __forceinline__ int32_t div_bs(int32_t q) const {
-    return lg_bs >= 0 ? q >> lg_bs : q / bs;
-  }
-  __device__ __forceinline__ void range(int64_t r, int32_t &s, int32_t &e, int32_t &aux) const {
-    const int32_t br = div_bs((int32_t)r);
-    aux = (int32_t)r - br * bs;
-    s = __ldg(rp + br) * bs;
-    e = __ldg(rp + br + 1) * bs;
-  }
-  __device__ __forceinline__ void entry(int32_t q, int32_t aux, int32_t &c, float &a,
-                                        const L2Policy &pol) const {
-    const int32_t b = div_bs(q), jj = q - b * bs;
-    c = __ldg(col + b) * bs + jj;
-    a = ld_stream(val + (int64_t)b * bs * bs + (rowmajor ? aux * bs + jj : jj * bs + aux),
-                  pol.stream);
-  }
-};
-
 constexpr int kSpmmInFlight = 4;  // U: nonzeros in flight per lane
 
 // How the lanes of a row get its entries (column, value):
