@@ -279,6 +279,7 @@ perflibs_status_t perflibs_b200_selector_create(perflibs_b200_selector_t *out, i
     for (int f = 0; f < NF; ++f)
       h[S->oistd() + f] = 1.f;
     PLS_CUDA(cudaMemcpy(S->params.p, h.data(), 4 * S->Ptot, cudaMemcpyHostToDevice));
+    PLS_CUDA(cudaDeviceSynchronize());  // legacy-stream copy, may still be in flight
     *out = S;
     return PERFLIBS_STATUS_SUCCESS;
   } catch (const Error &e) {
@@ -312,7 +313,10 @@ perflibs_status_t perflibs_b200_selector_set_params(perflibs_b200_selector_t S,
                                                     const float *params) {
   if (!S || !params)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
-  return cudaMemcpy(S->params.p, params, 4 * S->Ptot, cudaMemcpyHostToDevice) == cudaSuccess
+  // Legacy-stream copy from pageable memory: synchronise before the
+  // selector's own stream reads the parameters.
+  return cudaMemcpy(S->params.p, params, 4 * S->Ptot, cudaMemcpyHostToDevice) == cudaSuccess &&
+                 cudaDeviceSynchronize() == cudaSuccess
              ? PERFLIBS_STATUS_SUCCESS
              : PERFLIBS_STATUS_EXECUTION_FAILURE;
 }

@@ -311,6 +311,10 @@ void build_sell(const CsrDev &c, int32_t m, int C, int sigma, SellDev &out,
         S.order.reserve(sizeof(int32_t) * S.nC);
         PLS_CUDA(cudaMemcpy(S.order.p, ord.data(), sizeof(int32_t) * S.nC,
                             cudaMemcpyHostToDevice));
+        // The copy runs on the legacy stream, which the library's
+        // non-blocking streams do not wait for, and a copy from pageable
+        // memory may still be in flight when cudaMemcpy returns.
+        PLS_CUDA(cudaDeviceSynchronize());
       }
     }
     S.max_width = wmax;

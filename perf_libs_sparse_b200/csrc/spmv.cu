@@ -424,6 +424,11 @@ static void to_device(DevBuf &b, const std::vector<T> &h) {
     PLS_CUDA(cudaMemcpy(b.p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
 }
 
+// Plans are uploaded with cudaMemcpy / cudaMemset on the legacy stream, which
+// the library's non-blocking streams do not wait for (and a copy from
+// pageable memory may still be in flight when cudaMemcpy returns): a plan
+// ends with a device synchronisation before any kernel reads it.
+
 // Stable grouping of `v` by band: band b's elements keep their order and
 // land in [first[b], first[b + 1]).
 template <class T, class F>
@@ -508,6 +513,7 @@ void sell_plan_bands(SellDev &s, int64_t m, int n_bands) {
     s.bands.split_w = 2 * kBandSliceW;
   }
   s.bands.bands = std::move(bands);
+  PLS_CUDA(cudaDeviceSynchronize());
 }
 
 template <class X>
@@ -553,6 +559,7 @@ void csr_plan_bands(CsrDev &c, int32_t m, int n_bands) {
     to_device(c.bands.order, rows);
   }
   c.bands.bands = std::move(bands);
+  PLS_CUDA(cudaDeviceSynchronize());
 }
 
 template <class X>
