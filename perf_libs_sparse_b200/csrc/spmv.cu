@@ -192,11 +192,17 @@ void spmv_csr_split(const CsrDev &c, int32_t m, const X *x, X *y, X alpha,
 // (stride C between consecutive columns of the row). Columns are taken in
 // groups of kSellGroup: all value and offset loads of a group are issued
 // (predicated past len) before any of the group's dependent x gathers, so a
-// short row costs two memory round trips instead of two per column. The
+// row costs two memory round trips per group instead of two per column. The
 // products are still added one by one in column order j = 0 .. len-1, the
 // order of the reference's spmv_scs<T,C> (src/sell_c_sigma.cpp:727-775).
-constexpr int kSellGroup = 8;
-// 128-thread blocks (10 per SM at 48 registers): on power-law layouts a
+// Groups of 4 hold 40 registers, which lets 12 blocks of 128 threads share
+// an SM where groups of 8 (48 registers) let 10: the extra warps keep more
+// rows' loads in flight. Measured in alternating runs: C2 339 -> 323 us, a
+// 16.7 M-row 5-point Laplacian 319 -> 264 us, the 27-point stencil 113.7 ->
+// 112.7 us (C = 32).
+constexpr int kSellGroup = 4;
+constexpr int kSellBlocksPerSm = 12;
+// 128-thread blocks: on power-law layouts a
 // block waits for its slowest chunk, and smaller blocks waste less of the
 // SM on that wait than 256-thread ones (measured 1.4% on the C2 matrix,
 // 3.4% on a 16.7 M-row Laplacian).
@@ -253,7 +259,7 @@ __device__ __forceinline__ typename AccOf<V, X>::type sell_row_sum(const V *vp, 
 // the CUDA programming guide's last-block reduction. The finisher puts the
 // count back to zero, so done[] is all zero between launches.
 template <int C, class V, class O, class X>
-__global__ void __launch_bounds__(kSellThreads, 10)
+__global__ void __launch_bounds__(kSellThreads, kSellBlocksPerSm)
     k_sell(int64_t nC, int64_t c_base, int32_t split_w, int32_t slice_w, int64_t n_items,
            int64_t slice_blocks, const int4 *__restrict__ items,
            const int32_t *__restrict__ order, const int64_t *__restrict__ cs,
