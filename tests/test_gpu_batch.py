@@ -67,3 +67,68 @@ def test_batch_matches_oracle(tile):
         den = np.maximum(np.abs(ref), scale)
         den[den == 0] = 1
         assert (np.abs(got - ref) / den).max() <= 1e-5
+
+
+def test_batch_odd_blocks_layouts_and_values_at_creation():
+    """BSR instances of block sizes 1, 2, 3 and 5 in both block layouts, with
+    empty block rows; a CSR instance with empty rows; k from 1 to 13 with
+    and without 16-byte vectors. The batch expands BSR instances into scalar
+    rows at creation and reads its own copy of every instance's entries:
+    values updated in a handle afterwards are seen once the batch is created
+    again."""
+    import torch
+
+    rng = np.random.default_rng(9)
+    mats, descs = [], []
+    for bs, layout, k in [(1, pls.ROW_MAJOR, 3), (2, pls.COL_MAJOR, 8), (3, pls.ROW_MAJOR, 13),
+                          (5, pls.COL_MAJOR, 4), (3, pls.COL_MAJOR, 1)]:
+        mb, nb = 40, 30
+        counts = rng.integers(0, 4, mb)
+        counts[::7] = 0  # empty block rows
+        rp = np.zeros(mb + 1, np.int32)
+        rp[1:] = np.cumsum(counts)
+        col = np.concatenate([np.sort(rng.choice(nb, c, replace=False)) for c in counts]).astype(np.int32)
+        vals = rng.uniform(-1, 1, int(rp[-1]) * bs * bs).astype(np.float32)
+        mats.append(pls.SpMat.bsr(layout, mb * bs, nb * bs, bs, rp, col, vals))
+        descs.append(dict(kind="bsr", row_ptr=rp, col=col, vals=vals, bs=bs, layout=layout, m=mb * bs,
+                          n=nb * bs, k=k))
+    m, n = 700, 500
+    rp, c, v = W.random_csr(m, n, 12, rng, empty_frac=0.3)
+    v = v.astype(np.float32)
+    mats.append(pls.SpMat.csr(m, n, rp, c, v))
+    descs.append(dict(kind="csr", row_ptr=rp, col=c, vals=v, m=m, n=n, k=9))
+    Bs, Cs = [], []
+    for d in descs:
+        d["B"] = rng.uniform(-1, 1, (d["n"], d["k"])).astype(np.float32)
+        Bs.append(torch.tensor(d["B"], device="cuda"))
+        Cs.append(torch.zeros((d["m"], d["k"]), dtype=torch.float32, device="cuda"))
+    ks = [d["k"] for d in descs]
+    s = torch.cuda.Stream()
+
+    def run_and_check():
+        bt = pls.Batch(mats, ks, [b.data_ptr() for b in Bs], ks, [c.data_ptr() for c in Cs], ks,
+                       stream=s.cuda_stream)
+        bt.set_tile(8)
+        bt.exec(1.0, 0.0)
+        s.synchronize()
+        for d, cm in zip(descs, Cs):
+            ref, scale = _reference(d, 1.0, 0.0, np.zeros((d["m"], d["k"])))
+            got = cm.cpu().numpy().astype(np.float64)
+            den = np.maximum(np.abs(ref), scale)
+            den[den == 0] = 1
+            assert (np.abs(got - ref) / den).max() <= 1e-5, (d["kind"], d.get("bs"), d["k"])
+        return bt
+
+    bt = run_and_check()
+    # change the CSR instance's values: the existing batch keeps its copy
+    rows = np.repeat(np.arange(m), np.diff(rp))[:5].astype(np.int32)
+    cols = c[:5].astype(np.int32)
+    assert mats[-1].update(rows, cols, np.full(5, 7.0, np.float32)) == 0
+    descs[-1]["vals"] = v.copy()
+    descs[-1]["vals"][:5] = 7.0
+    bt.exec(1.0, 0.0)
+    s.synchronize()
+    old = _reference(dict(descs[-1], vals=v), 1.0, 0.0, np.zeros((m, 9)))[0]
+    np.testing.assert_allclose(Cs[-1].cpu().numpy(), old, rtol=1e-5, atol=1e-5)
+    bt.destroy()
+    run_and_check()  # a new batch sees the new values
