@@ -722,6 +722,85 @@ __global__ void k_add_transposed(int32_t m, int32_t n, const X *__restrict__ T, 
   *c = beta_nz ? t + beta * *c : t;
 }
 
+// ---- identity and dense x dense products (not a hot path) ----------------
+// Element (i, j) of op(D) for a dense D of leading dimension ld: row-major
+// D[i * ld + j], column-major D[j * ld + i]; the transpose swaps i and j.
+template <class X>
+__device__ __forceinline__ X dense_at(const X *D, int64_t ld, int rowmajor, int trans, int64_t i,
+                                      int64_t j) {
+  if (trans) {
+    const int64_t t = i;
+    i = j;
+    j = t;
+  }
+  return rowmajor ? D[i * ld + j] : D[j * ld + i];
+}
+
+template <class X>
+__device__ __forceinline__ X *dense_ptr(X *C, int64_t ld, int rowmajor, int64_t i, int64_t j) {
+  return rowmajor ? C + i * ld + j : C + j * ld + i;
+}
+
+// C = alpha * op(A) op(B) + beta * C for dense A (m x k after op) and B
+// (k x n): one thread per element of C, products added in the order of the
+// inner index (the reference hands this case to cblas_dgemm,
+// src/matmul.cpp:383-441).
+template <class X>
+__global__ void k_dense_gemm(int32_t m, int32_t n, int32_t k, const X *__restrict__ A, int64_t lda,
+                             int a_rm, int ta, const X *__restrict__ B, int64_t ldb, int b_rm,
+                             int tb, X *__restrict__ C, int64_t ldc, int c_rm, X alpha, X beta,
+                             int beta_nz) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)m * n)
+    return;
+  const int64_t i = idx / n, j = idx % n;
+  X sum = 0;
+  for (int64_t l = 0; l < k; ++l)
+    sum += dense_at(A, lda, a_rm, ta, i, l) * dense_at(B, ldb, b_rm, tb, l, j);
+  X *c = dense_ptr(C, ldc, c_rm, i, j);
+  *c = beta_nz ? alpha * sum + beta * *c : alpha * sum;
+}
+
+// C = alpha * op(D) + beta * C for a dense D (an identity factor times D).
+template <class X>
+__global__ void k_dense_axpby(int32_t m, int32_t n, const X *__restrict__ D, int64_t ldd,
+                              int d_rm, int td, X *__restrict__ C, int64_t ldc, int c_rm,
+                              X alpha, X beta, int beta_nz) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)m * n)
+    return;
+  const int64_t i = idx / n, j = idx % n;
+  X *c = dense_ptr(C, ldc, c_rm, i, j);
+  const X d = alpha * dense_at(D, ldd, d_rm, td, i, j);
+  *c = beta_nz ? d + beta * *c : d;
+}
+
+// C += alpha * op(S) for a CSR S, C already scaled by beta: one thread per
+// row i of S, whose entries all land in row i of C (column i when
+// transposed), so no two threads write one element and repeated entries of
+// a row are added in stored order.
+template <class X>
+__global__ void k_csr_add_dense(int32_t rows, const int32_t *__restrict__ rp,
+                                const int32_t *__restrict__ col, const X *__restrict__ val,
+                                X alpha, int trans, X *__restrict__ C, int64_t ldc, int c_rm) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rows)
+    return;
+  for (int32_t p = rp[i]; p < rp[i + 1]; ++p) {
+    const int64_t j = col[p];
+    X *c = trans ? dense_ptr(C, ldc, c_rm, j, i) : dense_ptr(C, ldc, c_rm, i, j);
+    *c += alpha * val[p];
+  }
+}
+
+// C += alpha on the diagonal (the identity times the identity).
+template <class X>
+__global__ void k_add_diag(int32_t n, X alpha, X *__restrict__ C, int64_t ldc) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n)
+    C[i * ldc + i] += alpha;
+}
+
 // The sparse x dense branch of the reference's spmm_exec_checked
 // (src/matmul.cpp:343-652), on the device. exec == false is the optimize
 // call: it prepares layouts and tunes without computing.
@@ -793,10 +872,58 @@ perflibs_status_t spmm_impl(int transA, int transB, X alpha, Mat *A, Mat *B, X b
     C->dense.is_zero = false;
     return PERFLIBS_STATUS_SUCCESS;
   }
+  // Identity factors (src/matmul.cpp:654-740 dispatch): I op(S) and op(S) I
+  // are alpha * op(S) + beta * C for S dense, sparse or the identity; and
+  // dense x dense. Simple kernels: these are not the hot path.
+  const bool a_id = A->fmt == Fmt::IDENTITY, b_id = B->fmt == Fmt::IDENTITY;
+  if ((a_id || b_id || (A->fmt == Fmt::DENSE && B->fmt == Fmt::DENSE)) &&
+      (C->fmt == Fmt::DENSE || c_null) && A != C && B != C) {
+    if ((!a_id && A->dt != dt) || (!b_id && B->dt != dt))
+      return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+    if (c_null)
+      make_dense_zero<X>(C, dt, m, n, PERFLIBS_ROW_MAJOR);
+    if (!exec)
+      return PERFLIBS_STATUS_SUCCESS;
+    X *cv = C->dense.vals.as<X>();
+    const int64_t ldc = C->dense.lda;
+    const int c_rm = C->dense.layout == PERFLIBS_ROW_MAJOR;
+    const unsigned blocks = (unsigned)div_up((int64_t)m * n, 256);
+    const int bnz = beta != X(0);
+    if (!a_id && !b_id) {
+      k_dense_gemm<X><<<blocks, 256, 0, s>>>(
+          m, n, k, A->dense.vals.as<X>(), A->dense.lda, A->dense.layout == PERFLIBS_ROW_MAJOR, ta,
+          B->dense.vals.as<X>(), B->dense.lda, B->dense.layout == PERFLIBS_ROW_MAJOR, tb, cv, ldc,
+          c_rm, alpha, beta, bnz);
+    } else {
+      Mat *S = a_id ? B : A;  // the other factor
+      const bool ts = a_id ? tb : ta;
+      if (S->fmt == Fmt::DENSE) {
+        k_dense_axpby<X><<<blocks, 256, 0, s>>>(m, n, S->dense.vals.as<X>(), S->dense.lda,
+                                                S->dense.layout == PERFLIBS_ROW_MAJOR, ts, cv, ldc,
+                                                c_rm, alpha, beta, bnz);
+      } else {
+        scal<X>((int64_t)m * n, beta, cv, s);  // C is packed: m * n elements
+        if (S->fmt == Fmt::IDENTITY) {
+          k_add_diag<X><<<(unsigned)div_up(std::max<int64_t>(std::min(m, n), 1), 256), 256, 0,
+                          s>>>(std::min(m, n), alpha, cv, ldc);
+        } else {
+          if (S->fmt == Fmt::BSR)
+            bsr_become_csr(S);  // as the reference's SpMM does (src/matmul.cpp:616-631)
+          k_csr_add_dense<X><<<(unsigned)div_up(std::max<int32_t>(S->m, 1), 256), 256, 0, s>>>(
+              S->m, S->csr.row_ptr.as<int32_t>(), S->csr.col.as<int32_t>(), S->csr.vals.as<X>(),
+              alpha, ts, cv, ldc, c_rm);
+        }
+      }
+    }
+    PLS_LAUNCH_CHECK();
+    PLS_CUDA(cudaStreamSynchronize(s));
+    C->dense.is_zero = false;
+    return PERFLIBS_STATUS_SUCCESS;
+  }
   if (!(is_sparse(A->fmt) && B->fmt == Fmt::DENSE && (C->fmt == Fmt::DENSE || c_null) && A != C &&
         B != C))
     throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE,
-                "sparse x sparse and identity products are not provided by the B200 execute path");
+                "sparse x sparse products are not provided by the B200 execute path");
   if (A->dt != dt || B->dt != dt)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
 

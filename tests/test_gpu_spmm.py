@@ -55,6 +55,82 @@ def test_kat_matmul_variants(kats):
     np.testing.assert_allclose(Cc.export_dense(pls.COL_MAJOR), k["alpha_beta"] * Ad @ Bd + C0, atol=k["tol"])
 
 
+def _dense_of(m, n, rp, c, v):
+    D = np.zeros((m, n))
+    for i in range(m):
+        for p in range(rp[i], rp[i + 1]):
+            D[i, c[p]] += v[p]
+    return D
+
+
+def test_kat_matmul_dispatch_paths(kats):
+    """test/matmul_dispatch_paths_d.c: dense x dense (the reference's
+    cblas_dgemm path), dense x sparse, identity x sparse and sparse x
+    identity, with the file's own data and expected values."""
+    k = kats["matmul_dispatch_paths_d"]
+    NT = pls.OPERATION_NOTRANS
+    g = k["gemm"]
+    A4, B4, C04 = (np.array(g[n]).reshape(4, 4) for n in ("A", "B", "C0"))
+    A = pls.SpMat.dense(pls.ROW_MAJOR, 4, 4, 4, np.array(g["A"]))
+    B = pls.SpMat.dense(pls.ROW_MAJOR, 4, 4, 4, np.array(g["B"]))
+    Cm = pls.SpMat.dense(pls.ROW_MAJOR, 4, 4, 4, np.array(g["C0"]))
+    assert pls.spmm_exec(NT, NT, g["alpha"], A, B, g["beta"], Cm) == 0
+    np.testing.assert_allclose(Cm.export_dense(), g["alpha"] * A4 @ B4 + g["beta"] * C04,
+                               atol=k["tol"])
+    d = k["dense_sparse"]
+    rp, c, v = np.array(d["row_ptr"]), np.array(d["col"]), np.array(d["vals"])
+    Bs = pls.SpMat.csr(4, 4, rp, c, v)
+    Ad = pls.SpMat.dense(pls.ROW_MAJOR, 4, 4, 4, np.array(d["A"]))
+    Cm = pls.SpMat.null(4, 4)
+    assert pls.spmm_exec(NT, NT, 1.0, Ad, Bs, 0.0, Cm) == 0
+    Bd = _dense_of(4, 4, rp, c, v)
+    np.testing.assert_allclose(Cm.export_dense(), np.array(d["A"]).reshape(4, 4) @ Bd,
+                               atol=k["tol"])
+    Cm = pls.SpMat.null(4, 4)
+    assert pls.spmm_exec(NT, NT, k["identity_left_alpha"], pls.SpMat.identity(4), Bs, 0.0, Cm) == 0
+    np.testing.assert_allclose(Cm.export_dense(), k["identity_left_alpha"] * Bd, atol=k["tol"])
+    r = k["identity_right"]
+    X = pls.SpMat.csr(4, 4, np.array(r["row_ptr"]), np.array(r["col"]), np.array(r["vals"]))
+    Cm = pls.SpMat.null(4, 4)
+    assert pls.spmm_exec(NT, NT, r["alpha"], X, pls.SpMat.identity(4), 0.0, Cm) == 0
+    np.testing.assert_allclose(Cm.export_dense().reshape(-1), r["expected"], atol=k["tol"])
+
+
+@pytest.mark.parametrize("ta", [pls.OPERATION_NOTRANS, pls.OPERATION_TRANS])
+@pytest.mark.parametrize("tb", [pls.OPERATION_NOTRANS, pls.OPERATION_TRANS])
+def test_identity_and_dense_products_vs_numpy(ta, tb):
+    """Identity factors and dense x dense beyond the reference's cases:
+    transposes, rectangular factors, a column-major C, beta != 0 (C = alpha
+    op(A) op(B) + beta C), BSR and CSR operands, and I x I."""
+    rng = np.random.default_rng(5)
+    T = lambda M, t: M.T if t != pls.OPERATION_NOTRANS else M  # noqa: E731
+    m, kk, n = 6, 4, 5
+    Ad = rng.uniform(-1, 1, (m, kk) if ta == pls.OPERATION_NOTRANS else (kk, m))
+    Bd = rng.uniform(-1, 1, (kk, n) if tb == pls.OPERATION_NOTRANS else (n, kk))
+    C0 = rng.uniform(-1, 1, (m, n))
+    A = pls.SpMat.dense(pls.COL_MAJOR, Ad.shape[0], Ad.shape[1], Ad.shape[0], Ad.T.reshape(-1))
+    B = pls.SpMat.dense(pls.ROW_MAJOR, Bd.shape[0], Bd.shape[1], Bd.shape[1], Bd.reshape(-1))
+    Cm = pls.SpMat.dense(pls.COL_MAJOR, m, n, m, C0.T.reshape(-1))
+    assert pls.spmm_exec(ta, tb, 0.75, A, B, -0.5, Cm) == 0
+    np.testing.assert_allclose(Cm.export_dense(), 0.75 * T(Ad, ta) @ T(Bd, tb) - 0.5 * C0,
+                               atol=1e-12)
+    # identity x sparse (CSR, then BSR) and sparse x identity, beta != 0
+    rp, c, v = W.random_csr(6, 6, 4, rng)
+    S = _dense_of(6, 6, rp, c, v)
+    C1 = rng.uniform(-1, 1, (6, 6))
+    for Sm in (pls.SpMat.csr(6, 6, rp, c, v),
+               pls.SpMat.bsr(pls.ROW_MAJOR, 6, 6, 2, *oracle.csr2bsr(rp, c, v, 6, 6, 2, pls.ROW_MAJOR))):
+        Cm = pls.SpMat.dense(pls.ROW_MAJOR, 6, 6, 6, C1.reshape(-1))
+        assert pls.spmm_exec(ta, tb, 1.25, pls.SpMat.identity(6), Sm, 0.5, Cm) == 0
+        np.testing.assert_allclose(Cm.export_dense(), 1.25 * T(S, tb) + 0.5 * C1, atol=1e-12)
+        Cm = pls.SpMat.dense(pls.ROW_MAJOR, 6, 6, 6, C1.reshape(-1))
+        assert pls.spmm_exec(ta, tb, -2.0, Sm, pls.SpMat.identity(6), 0.0, Cm) == 0
+        np.testing.assert_allclose(Cm.export_dense(), -2.0 * T(S, ta), atol=1e-12)
+    Cm = pls.SpMat.dense(pls.ROW_MAJOR, 6, 6, 6, C1.reshape(-1))
+    assert pls.spmm_exec(ta, tb, 3.0, pls.SpMat.identity(6), pls.SpMat.identity(6), 1.0, Cm) == 0
+    np.testing.assert_allclose(Cm.export_dense(), 3.0 * np.eye(6) + C1, atol=1e-12)
+
+
 def test_kat_matrix_kernel_ops(kats):
     k = kats["matrix_kernel_ops_spmm"]
     rp, c, v = np.array(k["row_ptr"]), np.array(k["col"]), np.array(k["vals"])
