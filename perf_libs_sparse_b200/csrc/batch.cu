@@ -29,14 +29,14 @@ namespace pls {
 namespace {
 
 struct InstDesc {
-  const int32_t *rp;
-  const int32_t *col;
+  const int32_t *rp;   // row pointers of the scalar rows (a BSR instance's: the batch's)
+  const int32_t *col;  // the handle's arrays, read once at creation
   const float *val;
-  const int2 *cv;  // CSR: the batch's packed (column, value) copy
+  const int2 *cv;      // the batch's packed (column, value) copy the kernel reads
   const float *B;
   float *C;
   int64_t ldb, ldc;
-  int32_t m, k, bs, layout, is_bsr;
+  int32_t m, k, bs, layout, is_bsr;  // bs / is_bsr: block-aligned items for BSR
   int32_t lg_tk, lg_tn, path;  // path: 0 = VEC 4, 1 = VEC 1 x 1, 2 = VEC 1 x 2
 };
 
