@@ -590,7 +590,7 @@ def run_extra(args):
         line.update(metric="Batched SpMM GB/s (algorithmic bytes), 512 uneven FP32 instances, one persistent launch",
                     dtype="f32", value=b / ms / 1e6, ms_per_step=ms,
                     config={"workload": "C4 512 instances n in [1024, 65536], k in [1, 64]", "tile_rows": tile,
-                            **bt.info(), "rows_total": int(sum(d["m"] for d in inst))})
+                            **bt.info(), **bt.stage_info(), "rows_total": int(sum(d["m"] for d in inst))})
     line["roofline"] = {"bound": "hbm", "achieved": line["value"], "peak": hbm, "unit": "GB/s",
                         "frac": line["value"] / hbm, "peak_source": peak_kind}
     emit(line, args)

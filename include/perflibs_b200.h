@@ -339,6 +339,19 @@ perflibs_status_t perflibs_b200_batch_info(perflibs_b200_batch_t Bt,
                                            int64_t *n_items,
                                            int32_t *launches_per_exec,
                                            int32_t *tile);
+/* Staged items: blocks of rows whose entries read a narrow window of B's
+ * rows (banded, block-diagonal) are computed by whole CTAs from a copy of
+ * that window in shared memory, at most 32 columns of C per item. Which
+ * blocks qualify is fixed at creation; the tuner times the batch with and
+ * without them and keeps the faster. set_staging(0) sends every row to the
+ * per-warp items, set_staging(1) brings the staged items back.
+ * staged_items counts the staged items built at creation; on reports
+ * whether they run. */
+perflibs_status_t perflibs_b200_batch_set_staging(perflibs_b200_batch_t Bt,
+                                                  int32_t on);
+perflibs_status_t perflibs_b200_batch_stage_info(perflibs_b200_batch_t Bt,
+                                                 int64_t *staged_items,
+                                                 int32_t *on);
 perflibs_status_t perflibs_b200_batch_destroy(perflibs_b200_batch_t Bt);
 
 /* Library / device information: SM count, L2 bytes, device ordinal. */

@@ -517,6 +517,8 @@ class Batch:
                            "perflibs_b200_batch_tune": [vp, vp, vp],
                            "perflibs_b200_batch_exec": [vp, C.c_float, C.c_float],
                            "perflibs_b200_batch_info": [vp, vp, vp, vp],
+                           "perflibs_b200_batch_set_staging": [vp, C.c_int32],
+                           "perflibs_b200_batch_stage_info": [vp, vp, vp],
                            "perflibs_b200_batch_destroy": [vp]}.items():
             getattr(L, name).argtypes = args
             getattr(L, name).restype = C.c_int
@@ -548,21 +550,16 @@ class Batch:
         _check(lib().perflibs_b200_batch_info(self.h, C.byref(n), C.byref(l), C.byref(t)), "batch_info")
         return {"n_items": n.value, "launches": l.value, "tile": t.value}
 
-    def set_host_bands(self, n_bands):
-        """Row bands of host-buffer SpMV: 0 by size (default), 1 none, 2..64 that many."""
-        _check(lib().perflibs_b200_spmat_set_host_bands(self.h, n_bands), "set_host_bands")
+    def set_staging(self, on):
+        """Run the staged (shared-memory window) items (True) or send every
+        row to the per-warp items (False)."""
+        _check(lib().perflibs_b200_batch_set_staging(self.h, 1 if on else 0), "batch_set_staging")
 
-    def tune_source(self):
-        """How the active SpMV configuration was chosen (TUNE_SOURCE_*)."""
-        r = C.c_int32()
-        _check(lib().perflibs_b200_spmat_tune_source(self.h, C.byref(r)), "tune_source")
-        return r.value
-
-    def host_bands_used(self):
-        """Bands the last host-buffer SpMV ran in (0 = one launch)."""
-        r = C.c_int32()
-        _check(lib().perflibs_b200_spmat_host_bands_used(self.h, C.byref(r)), "host_bands_used")
-        return r.value
+    def stage_info(self):
+        """{'staged_items': built at creation, 'staging': whether they run}."""
+        n, on = C.c_int64(), C.c_int32()
+        _check(lib().perflibs_b200_batch_stage_info(self.h, C.byref(n), C.byref(on)), "batch_stage_info")
+        return {"staged_items": n.value, "staging": bool(on.value)}
 
     def destroy(self):
         if self.h is not None and self.h.value:

@@ -15,7 +15,20 @@
 // read from the batch's own copy of its entries, (column, value) side by
 // side; a BSR instance is expanded at creation into scalar rows whose
 // entries are its blocks' rows in stored order.
+//
+// Staged items come first. Where a block of rows reads only a narrow window
+// of B's rows (banded matrices: a block of 128 rows with half-bandwidth 64
+// reads 256 rows of B, each of them up to 129 times; BSR block diagonals:
+// each row of B bs times), a whole CTA takes the block: it copies the
+// window's rows of B, up to 32 columns at a time, into shared memory once
+// and computes every row of the block from there, so each B element comes
+// from L2 once per block instead of once per nonzero that reads it. The CTA
+// takes the next staged item from a second counter; when none are left its
+// warps go on to the per-warp items. Which blocks are staged is decided at
+// creation from each block's column window; the tuner times the batch with
+// and without them.
 #include <algorithm>
+#include <climits>
 #include <cstring>
 #include <numeric>
 #include <vector>
@@ -44,6 +57,19 @@ struct Item {
   int32_t inst, row0, row1, pad;
 };
 
+// A staged item: rows [row0, row1) of instance `inst`, whose entries all
+// have columns in [lo, lo + w), for C's columns [c0, c0 + ks) (ks <= 32).
+// The window sits in shared memory as w rows of 4 * tk floats (ks rounded
+// up to whole float4s, zero past ks).
+struct SItem {
+  int32_t inst, row0, row1, lo;
+  int32_t w, c0, ks, tk;
+};
+
+constexpr int kBatchThreads = 256;
+constexpr int kStageFloats = 8192;  // 32 KB of shared memory per CTA
+constexpr int kStageCols = 32;      // widest column slice of a staged item
+
 // One item's rows with the instance's vector shape.
 template <class Rows, bool OFF32>
 __device__ __forceinline__ void batch_rows(const Rows &A, const InstDesc &d, const Item &w,
@@ -65,27 +91,165 @@ __device__ __forceinline__ void batch_rows(const Rows &A, const InstDesc &d, con
   }
 }
 
+// One staged item, by the whole CTA. The window of B (rows lo .. lo + w - 1,
+// columns c0 .. c0 + ks - 1) is copied into `stage` (row stride 4 tk
+// floats); then tk lanes per row own 4 columns each, and every row of the
+// item adds its entries in stored order from the staged rows. Each entry's
+// column lies in the window (the item was built from the minimum and
+// maximum column of its entries), so the stage reads stay inside
+// w * 4 tk floats.
+__device__ __forceinline__ void staged_item(const SItem &w, const InstDesc &d,
+                                            float *__restrict__ stage, float alpha, float beta,
+                                            int beta_nz) {
+  constexpr int warps = kBatchThreads / 32;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int TK = w.tk, KSP = 4 * w.tk;
+  {
+    // 32 / KSP window rows per warp pass, a lane per column
+    const int per = 32 / KSP;
+    const int rs = lane / KSP, c = lane - rs * KSP;
+    if (rs < per) {
+      const bool in = c < w.ks;
+      const float *src = d.B + (int64_t)w.lo * d.ldb + w.c0 + (in ? c : 0);
+      for (int r = warp * per + rs; r < w.w; r += warps * per)
+        stage[r * KSP + c] = in ? __ldg(src + (int64_t)r * d.ldb) : 0.f;
+    }
+  }
+  __syncthreads();
+  const float4 *st4 = reinterpret_cast<const float4 *>(stage);
+  const int per = 32 / TK;  // rows per warp
+  const int rs = lane / TK, tk = lane - rs * TK;
+  if (rs >= per)
+    return;
+  const int kk = w.c0 + 4 * tk;  // this lane's first column of C
+  const int kend = w.c0 + w.ks;
+  const bool vec = d.path == 0 && kk + 4 <= kend;
+  for (int32_t row = w.row0 + warp * per + rs; row < w.row1; row += warps * per) {
+    const int32_t s = __ldg(d.rp + row), e = __ldg(d.rp + row + 1);
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    const auto add = [&](int2 t) {
+      const float4 b = st4[(t.x - w.lo) * TK + tk];
+      const float a = __int_as_float(t.y);
+      acc.x = fmaf(a, b.x, acc.x);
+      acc.y = fmaf(a, b.y, acc.y);
+      acc.z = fmaf(a, b.z, acc.z);
+      acc.w = fmaf(a, b.w, acc.w);
+    };
+    int32_t q = s;
+    for (; q + 4 <= e; q += 4) {
+      int2 t[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        t[u] = __ldg(d.cv + q + u);
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        add(t[u]);
+    }
+    for (; q < e; ++q)
+      add(__ldg(d.cv + q));
+    float *crow = d.C + (int64_t)row * d.ldc + kk;
+    const float sum[4] = {acc.x, acc.y, acc.z, acc.w};
+    if (vec) {
+      float out[4];
+      if (beta_nz) {
+        const float4 old = *reinterpret_cast<const float4 *>(crow);
+        const float o[4] = {old.x, old.y, old.z, old.w};
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          out[v] = sum[v] * alpha + beta * o[v];
+      } else {
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          out[v] = sum[v] * alpha;
+      }
+      *reinterpret_cast<float4 *>(crow) = make_float4(out[0], out[1], out[2], out[3]);
+    } else {
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+        if (kk + v < kend) {
+          float o = sum[v] * alpha;
+          if (beta_nz)
+            o += beta * crow[v];
+          crow[v] = o;
+        }
+    }
+  }
+}
+
+// counters[0] hands out the per-warp items, counters[1] the staged ones.
+// The dynamic shared memory (kStageFloats floats) is needed only when there
+// are staged items.
 template <bool OFF32>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kBatchThreads)
     k_batch_spmm(const InstDesc *__restrict__ inst, const Item *__restrict__ items,
-                 int64_t n_items, unsigned long long *__restrict__ counter, float alpha,
-                 float beta, int beta_nz) {
+                 int64_t n_items, const SItem *__restrict__ sitems, int64_t n_sitems,
+                 unsigned long long *__restrict__ counters, float alpha, float beta,
+                 int beta_nz) {
+  extern __shared__ float4 stage4[];
+  __shared__ unsigned long long s_ticket;
+  if (n_sitems > 0) {
+    for (;;) {
+      if (threadIdx.x == 0)
+        s_ticket = atomicAdd(counters + 1, 1ull);
+      __syncthreads();
+      const unsigned long long t = s_ticket;
+      if (t >= (unsigned long long)n_sitems)
+        break;  // every thread read the same ticket: the whole CTA leaves
+      const SItem w = sitems[t];
+      staged_item(w, inst[w.inst], reinterpret_cast<float *>(stage4), alpha, beta, beta_nz);
+      __syncthreads();  // the stage and s_ticket are reused by the next item
+    }
+  }
   const L2Policy pol = make_l2_policy();
   const int lane = threadIdx.x & 31;
   unsigned long long it = 0;
   if (lane == 0)
-    it = atomicAdd(counter, 1ull);
+    it = atomicAdd(counters, 1ull);
   it = __shfl_sync(0xffffffffu, it, 0);
   while (it < (unsigned long long)n_items) {
     // Take the next ticket now; its round trip overlaps this item's loads.
     unsigned long long next = 0;
     if (lane == 0)
-      next = atomicAdd(counter, 1ull);
+      next = atomicAdd(counters, 1ull);
     const Item w = items[it];
     const InstDesc d = inst[w.inst];
     const PackedRows A{d.rp, d.cv};
     batch_rows<PackedRows, OFF32>(A, d, w, lane, alpha, beta, beta_nz, pol);
     it = __shfl_sync(0xffffffffu, next, 0);
+  }
+}
+
+// The column window of each block of rs rows of one instance: x = smallest
+// column, y = largest (INT32_MAX / INT32_MIN for a block without entries),
+// z = the block's entries. One CTA of 256 threads per block.
+__global__ void __launch_bounds__(256)
+    k_block_window(int32_t m, int32_t rs, const int32_t *__restrict__ rp,
+                   const int2 *__restrict__ cv, int4 *__restrict__ out) {
+  __shared__ int s_lo[8], s_hi[8];
+  const int64_t r0 = (int64_t)blockIdx.x * rs;
+  const int64_t r1 = r0 + rs < (int64_t)m ? r0 + rs : (int64_t)m;
+  const int32_t p0 = rp[r0], p1 = rp[r1];
+  int lo = INT32_MAX, hi = INT32_MIN;
+  for (int32_t p = p0 + (int32_t)threadIdx.x; p < p1; p += 256) {
+    const int c = cv[p].x;
+    lo = min(lo, c);
+    hi = max(hi, c);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    s_lo[threadIdx.x >> 5] = lo;
+    s_hi[threadIdx.x >> 5] = hi;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 1; i < 8; ++i) {
+      lo = min(lo, s_lo[i]);
+      hi = max(hi, s_hi[i]);
+    }
+    out[blockIdx.x] = make_int4(lo, hi, p1 - p0, 0);
   }
 }
 
@@ -144,7 +308,13 @@ struct perflibs_b200_batch_s {
   pls::DevBuf inst, items, counter;
   pls::DevBuf packed;  // every instance's (column, value) pairs, packed at creation
   pls::DevBuf scalar_rp;  // row pointers of the BSR instances' scalar rows
+  pls::DevBuf sitems;     // staged items, largest first
+  // Per instance, the row ranges left to the per-warp items when staged
+  // items are on (the blocks that were not staged).
+  std::vector<std::vector<std::pair<int32_t, int32_t>>> warp_ranges;
   int64_t n_items = 0;
+  int64_t n_sitems = 0;  // staged items built at creation
+  bool staging = true;   // run them (else every row goes to per-warp items)
   int32_t tile = 0;
   int grid = 0;
   cudaGraphExec_t graph = nullptr;
@@ -166,6 +336,8 @@ using Batch = perflibs_b200_batch_s;
 
 namespace {
 
+// The per-warp items: the rows not in staged items (all rows when staging
+// is off), cut into items of `tile` rows.
 void build_items(Batch *B, int32_t tile) {
   std::vector<std::pair<double, Item>> v;
   for (int32_t i = 0; i < (int32_t)B->host.size(); ++i) {
@@ -173,10 +345,12 @@ void build_items(Batch *B, int32_t tile) {
     int32_t R = tile;
     if (d.is_bsr)
       R = std::max<int32_t>(d.bs, (tile / d.bs) * d.bs);
-    for (int32_t r0 = 0; r0 < d.m; r0 += R) {
-      Item it{i, r0, std::min(d.m, r0 + R), 0};
-      v.push_back({B->work_per_row[i] * (it.row1 - it.row0), it});
-    }
+    const std::vector<std::pair<int32_t, int32_t>> all{{0, d.m}};
+    for (const auto &rg : B->staging ? B->warp_ranges[i] : all)
+      for (int32_t r0 = rg.first; r0 < rg.second; r0 += R) {
+        Item it{i, r0, std::min(rg.second, r0 + R), 0};
+        v.push_back({B->work_per_row[i] * (it.row1 - it.row0), it});
+      }
   }
   std::stable_sort(v.begin(), v.end(), [](auto &a, auto &b) { return a.first > b.first; });
   std::vector<Item> items(v.size());
@@ -192,6 +366,73 @@ void build_items(Batch *B, int32_t tile) {
   B->graph_valid = false;
 }
 
+// The staged items, once at creation (the packed entries must be in
+// place). Each instance with k >= 1 is cut into blocks of rs rows, rs half
+// the window rows its widest column slice (min(k, 32) columns, rounded up
+// to float4s) leaves in kStageFloats. A block is staged when its entries'
+// column window fits in the stage and holds at most half as many rows of B
+// as the block has entries (each staged B row read at least twice on
+// average); it then gives one item per column slice of 32. The other rows
+// go to the per-warp items.
+void build_staged(Batch *B) {
+  const int32_t count = (int32_t)B->host.size();
+  B->warp_ranges.assign(count, {});
+  std::vector<std::pair<double, SItem>> v;
+  DevBuf win;
+  std::vector<int4> hw;
+  for (int32_t i = 0; i < count; ++i) {
+    const InstDesc &d = B->host[i];
+    auto &ranges = B->warp_ranges[i];
+    const auto to_warps = [&](int32_t r0, int32_t r1) {
+      if (!ranges.empty() && ranges.back().second == r0)
+        ranges.back().second = r1;
+      else
+        ranges.push_back({r0, r1});
+    };
+    if (d.m == 0)
+      continue;
+    if (d.k < 1) {
+      to_warps(0, d.m);
+      continue;
+    }
+    const int32_t ksp0 = 4 * (int32_t)div_up(std::min(d.k, kStageCols), 4);
+    const int32_t wmax = kStageFloats / ksp0;
+    const int32_t rs = wmax / 2;
+    const int64_t nblk = div_up((int64_t)d.m, (int64_t)rs);
+    win.reserve(sizeof(int4) * nblk);
+    k_block_window<<<(unsigned)nblk, 256, 0, B->stream>>>(d.m, rs, d.rp, d.cv, win.as<int4>());
+    PLS_LAUNCH_CHECK();
+    hw.resize(nblk);
+    PLS_CUDA(cudaMemcpyAsync(hw.data(), win.p, sizeof(int4) * nblk, cudaMemcpyDeviceToHost,
+                             B->stream));
+    PLS_CUDA(cudaStreamSynchronize(B->stream));
+    for (int64_t j = 0; j < nblk; ++j) {
+      const int32_t r0 = (int32_t)(j * rs), r1 = (int32_t)std::min<int64_t>(d.m, r0 + (int64_t)rs);
+      const int4 b = hw[j];
+      const int64_t w = (int64_t)b.y - b.x + 1;
+      if (b.z == 0 || w > wmax || (int64_t)b.z < 2 * w) {
+        to_warps(r0, r1);
+        continue;
+      }
+      for (int32_t c0 = 0; c0 < d.k; c0 += kStageCols) {
+        const int32_t ks = std::min(kStageCols, d.k - c0);
+        const SItem it{i, r0, r1, b.x, (int32_t)w, c0, ks, (int32_t)div_up(ks, 4)};
+        v.push_back({(double)b.z * it.tk + (double)w * it.tk, it});
+      }
+    }
+  }
+  std::stable_sort(v.begin(), v.end(), [](auto &a, auto &b) { return a.first > b.first; });
+  std::vector<SItem> items(v.size());
+  for (size_t j = 0; j < v.size(); ++j)
+    items[j] = v[j].second;
+  B->n_sitems = (int64_t)items.size();
+  B->sitems.reserve(sizeof(SItem) * std::max<size_t>(items.size(), 1));
+  if (!items.empty())
+    PLS_CUDA(cudaMemcpyAsync(B->sitems.p, items.data(), sizeof(SItem) * items.size(),
+                             cudaMemcpyHostToDevice, B->stream));
+  PLS_CUDA(cudaStreamSynchronize(B->stream));
+}
+
 void capture(Batch *B, float alpha, float beta) {
   if (B->graph) {
     cudaGraphExecDestroy(B->graph);
@@ -200,12 +441,14 @@ void capture(Batch *B, float alpha, float beta) {
   cudaGraph_t g;
   cudaStream_t s = B->stream;
   PLS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-  cudaMemsetAsync(B->counter.p, 0, 8, s);
-  if (B->n_items > 0)
-  {
+  cudaMemsetAsync(B->counter.p, 0, 16, s);
+  const int64_t n_s = B->staging ? B->n_sitems : 0;
+  if (B->n_items > 0 || n_s > 0) {
     auto kern = B->off32 ? k_batch_spmm<true> : k_batch_spmm<false>;
-    kern<<<B->grid, 256, 0, s>>>(B->inst.as<InstDesc>(), B->items.as<Item>(), B->n_items,
-                                 B->counter.as<unsigned long long>(), alpha, beta, beta != 0.f);
+    const size_t smem = n_s > 0 ? sizeof(float) * kStageFloats : 0;
+    kern<<<B->grid, kBatchThreads, smem, s>>>(
+        B->inst.as<InstDesc>(), B->items.as<Item>(), B->n_items, B->sitems.as<SItem>(), n_s,
+        B->counter.as<unsigned long long>(), alpha, beta, beta != 0.f);
   }
   PLS_CUDA(cudaStreamEndCapture(s, &g));
   PLS_CUDA(cudaGraphInstantiate(&B->graph, g, 0));
@@ -335,11 +578,13 @@ perflibs_status_t perflibs_b200_batch_create(perflibs_b200_batch_t *out, int32_t
     B->inst.reserve(sizeof(InstDesc) * count);
     PLS_CUDA(cudaMemcpyAsync(B->inst.p, B->host.data(), sizeof(InstDesc) * count,
                              cudaMemcpyHostToDevice, B->stream));
-    B->counter.reserve(8);
+    build_staged(B);
+    B->counter.reserve(16);
     int sms = 0, per_sm = 0;
     PLS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, B->device));
     PLS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, B->off32 ? k_batch_spmm<true> : k_batch_spmm<false>, 256, 0));
+        &per_sm, B->off32 ? k_batch_spmm<true> : k_batch_spmm<false>, kBatchThreads,
+        sizeof(float) * kStageFloats));
     B->grid = sms * std::max(per_sm, 1);
     build_items(B, 64);
     *out = B;
@@ -372,8 +617,13 @@ perflibs_status_t perflibs_b200_batch_tune(perflibs_b200_batch_t B, int32_t *bes
     PLS_CUDA(cudaEventCreate(&e0));
     PLS_CUDA(cudaEventCreate(&e1));
     int32_t best = 64;
+    bool best_staging = false;
     float bms = 1e30f;
+    for (const bool staging : {true, false})
     for (int32_t tile : {8, 32, 128, 512, 2048}) {
+      if (staging && B->n_sitems == 0)
+        continue;
+      B->staging = staging;
       build_items(B, tile);
       run(B, 1.f, 0.f);
       run(B, 1.f, 0.f);
@@ -391,10 +641,12 @@ perflibs_status_t perflibs_b200_batch_tune(perflibs_b200_batch_t B, int32_t *bes
       if (t[t.size() / 2] < bms) {
         bms = t[t.size() / 2];
         best = tile;
+        best_staging = staging;
       }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    B->staging = best_staging;
     build_items(B, best);
     if (best_tile)
       *best_tile = best;
@@ -404,6 +656,29 @@ perflibs_status_t perflibs_b200_batch_tune(perflibs_b200_batch_t B, int32_t *bes
   } catch (const Error &e) {
     return e.status;
   }
+}
+
+perflibs_status_t perflibs_b200_batch_set_staging(perflibs_b200_batch_t B, int32_t on) {
+  if (!B)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  try {
+    B->staging = on != 0;
+    build_items(B, B->tile);
+    return PERFLIBS_STATUS_SUCCESS;
+  } catch (const Error &e) {
+    return e.status;
+  }
+}
+
+perflibs_status_t perflibs_b200_batch_stage_info(perflibs_b200_batch_t B, int64_t *staged_items,
+                                                 int32_t *on) {
+  if (!B)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  if (staged_items)
+    *staged_items = B->n_sitems;
+  if (on)
+    *on = B->staging ? 1 : 0;
+  return PERFLIBS_STATUS_SUCCESS;
 }
 
 perflibs_status_t perflibs_b200_batch_exec(perflibs_b200_batch_t B, float alpha, float beta) {
@@ -424,7 +699,7 @@ perflibs_status_t perflibs_b200_batch_info(perflibs_b200_batch_t B, int64_t *n_i
   if (n_items)
     *n_items = B->n_items;
   if (launches)
-    *launches = B->n_items > 0 ? 1 : 0;
+    *launches = B->n_items > 0 || (B->staging && B->n_sitems > 0) ? 1 : 0;
   if (tile)
     *tile = B->tile;
   return PERFLIBS_STATUS_SUCCESS;

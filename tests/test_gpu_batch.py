@@ -132,3 +132,90 @@ def test_batch_odd_blocks_layouts_and_values_at_creation():
     np.testing.assert_allclose(Cs[-1].cpu().numpy(), old, rtol=1e-5, atol=1e-5)
     bt.destroy()
     run_and_check()  # a new batch sees the new values
+
+
+def _banded(n, hb, rng):
+    rows = np.arange(n)
+    lo = np.maximum(rows - hb, 0)
+    hi = np.minimum(rows + hb, n - 1)
+    lens = hi - lo + 1
+    rp = np.zeros(n + 1, np.int32)
+    rp[1:] = np.cumsum(lens)
+    col = (np.repeat(lo, lens) + np.arange(rp[-1]) - np.repeat(rp[:-1], lens)).astype(np.int32)
+    return rp, col, rng.uniform(-1, 1, int(rp[-1])).astype(np.float32)
+
+
+def test_batch_staged_items_against_oracle_and_per_warp_items():
+    """Banded and block-diagonal instances have blocks of rows that read a
+    narrow window of B's rows; the batch computes those from a copy of the
+    window in shared memory, at most 32 columns of C per item (k = 33, 64
+    and 70 take two or three column slices; k = 1, 3 and 5 a padded
+    float4). Leading dimensions that are not multiples of 4 keep C's stores
+    scalar. A random instance has no narrow windows and stays on the
+    per-warp items. Results with the staged items on and off both match the
+    oracle within the FP32 bound, for beta = 0 and beta != 0."""
+    import torch
+
+    rng = np.random.default_rng(21)
+    mats, descs = [], []
+    for n, hb, k, pad in [(3000, 2, 1, 0), (2500, 17, 3, 0), (4100, 64, 5, 0), (3000, 30, 8, 0),
+                          (2000, 64, 32, 0), (2200, 9, 33, 3), (1800, 40, 64, 0), (1500, 5, 70, 1),
+                          (2600, 64, 16, 2)]:
+        rp, c, v = _banded(n, hb, rng)
+        mats.append(pls.SpMat.csr(n, n, rp, c, v))
+        descs.append(dict(kind="csr", row_ptr=rp, col=c, vals=v, m=n, n=n, k=k, ldb=k + pad, ldc=k + pad))
+    for bs, k in [(4, 6), (8, 16), (4, 40)]:
+        nb = 700
+        blocks = rng.uniform(-1, 1, (nb, bs * bs)).astype(np.float32)
+        blocks[rng.random((nb, bs * bs)) >= 0.6] = 0.0
+        rp = np.arange(nb + 1, dtype=np.int32)
+        col = np.arange(nb, dtype=np.int32)
+        mats.append(pls.SpMat.bsr(pls.ROW_MAJOR, nb * bs, nb * bs, bs, rp, col, blocks.reshape(-1)))
+        descs.append(dict(kind="bsr", row_ptr=rp, col=col, vals=blocks.reshape(-1), bs=bs,
+                          layout=pls.ROW_MAJOR, m=nb * bs, n=nb * bs, k=k, ldb=k, ldc=k))
+    m = 5000
+    rp, c, v = W.random_csr(m, m, 10, rng)
+    v = v.astype(np.float32)
+    mats.append(pls.SpMat.csr(m, m, rp, c, v))
+    descs.append(dict(kind="csr", row_ptr=rp, col=c, vals=v, m=m, n=m, k=12, ldb=12, ldc=12))
+    Bs, Cs, C0s = [], [], []
+    for d in descs:
+        d["B"] = rng.uniform(-1, 1, (d["n"], d["k"])).astype(np.float32)
+        Bfull = np.zeros((d["n"], d["ldb"]), np.float32)
+        Bfull[:, :d["k"]] = d["B"]
+        Bs.append(torch.tensor(Bfull, device="cuda"))
+        c0 = rng.uniform(-1, 1, (d["m"], d["ldc"])).astype(np.float32)
+        C0s.append(c0)
+        Cs.append(torch.tensor(c0, device="cuda"))
+    s = torch.cuda.Stream()
+    bt = pls.Batch(mats, [d["k"] for d in descs], [b.data_ptr() for b in Bs], [d["ldb"] for d in descs],
+                   [cm.data_ptr() for cm in Cs], [d["ldc"] for d in descs], stream=s.cuda_stream)
+    info = bt.stage_info()
+    assert info["staged_items"] > 0 and info["staging"]
+
+    def check(alpha, beta):
+        for cm, c0 in zip(Cs, C0s):
+            cm.copy_(torch.tensor(c0, device="cuda"))
+        torch.cuda.synchronize()
+        bt.exec(alpha, beta)
+        s.synchronize()
+        for d, cm, c0 in zip(descs, Cs, C0s):
+            k = d["k"]
+            ref, scale = _reference(d, alpha, beta, c0[:, :k].astype(np.float64))
+            got = cm.cpu().numpy()
+            den = np.maximum(np.abs(ref), scale)
+            den[den == 0] = 1
+            assert (np.abs(got[:, :k].astype(np.float64) - ref) / den).max() <= 1e-5, (d["kind"], d["m"], k)
+            np.testing.assert_array_equal(got[:, k:], c0[:, k:])  # padding columns untouched
+
+    for staging in (True, False):
+        bt.set_staging(staging)
+        assert bt.stage_info()["staging"] is staging
+        for tile in (8, 128):
+            bt.set_tile(tile)
+            check(1.0, 0.0)
+        check(1.5, -0.5)
+    best, ms = bt.tune()
+    assert best > 0 and ms > 0
+    check(0.5, 2.0)
+    bt.destroy()
