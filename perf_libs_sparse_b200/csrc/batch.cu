@@ -104,13 +104,37 @@ __device__ __forceinline__ void staged_item(const SItem &w, const InstDesc &d,
   constexpr int warps = kBatchThreads / 32;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int TK = w.tk, KSP = 4 * w.tk;
-  {
+  if ((d.ldb & 3) == 0 && ((uintptr_t)d.B & 15) == 0) {
+    // TK lanes per window row, a float4 each (c0 is a multiple of 32, so
+    // every row segment starts on 16 bytes)
+    const int per = 32 / TK;
+    const int rs = lane / TK, c4 = lane - rs * TK, c = 4 * c4;
+    if (rs < per) {
+      const float *src = d.B + (int64_t)w.lo * d.ldb + w.c0 + c;
+      float4 *dst = reinterpret_cast<float4 *>(stage) + c4;
+#pragma unroll 4
+      for (int r = warp * per + rs; r < w.w; r += warps * per) {
+        const float *p = src + (int64_t)r * d.ldb;
+        float4 v;
+        if (c + 4 <= w.ks) {
+          v = __ldg(reinterpret_cast<const float4 *>(p));
+        } else {
+          v.x = c < w.ks ? __ldg(p) : 0.f;
+          v.y = c + 1 < w.ks ? __ldg(p + 1) : 0.f;
+          v.z = c + 2 < w.ks ? __ldg(p + 2) : 0.f;
+          v.w = 0.f;  // c + 3 >= ks here
+        }
+        dst[r * TK] = v;
+      }
+    }
+  } else {
     // 32 / KSP window rows per warp pass, a lane per column
     const int per = 32 / KSP;
     const int rs = lane / KSP, c = lane - rs * KSP;
     if (rs < per) {
       const bool in = c < w.ks;
       const float *src = d.B + (int64_t)w.lo * d.ldb + w.c0 + (in ? c : 0);
+#pragma unroll 4
       for (int r = warp * per + rs; r < w.w; r += warps * per)
         stage[r * KSP + c] = in ? __ldg(src + (int64_t)r * d.ldb) : 0.f;
     }
