@@ -1248,6 +1248,10 @@ perflibs_status_t update(Mat *A, int32_t nu, const int32_t *rows, const int32_t 
     // Authoritative values first, then the reduced copy and SELL values.
     const int64_t applied = update_csr_values(A->csr, nullptr, A->m, A->n, nu, rows, cols, vals,
                                               A->dt, A->index_base, s);
+    // The cached CSR of A^T holds the old values: the next transposed
+    // product builds it again.
+    A->has_csrT = false;
+    ++A->csr.vals_version;
     if (A->csr.lo || A->fmt == Fmt::SELL) {
       // Re-derive the kernels' copies of the updated entries.
       CsrDev &c = A->csr;
@@ -1730,7 +1734,7 @@ void perflibs_spmat_print_err(perflibs_spmat_t A) {
 // ---------------------------------------------------------- extensions
 
 perflibs_status_t perflibs_b200_spmat_set_spmm_path(perflibs_spmat_t A, int32_t path) {
-  if (!A || path < -1 || path > 2)
+  if (!A || path < -1 || path > 3)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
   A->csr.tiles.forced = path;
   A->csr.tiles.choice_sig = -1;

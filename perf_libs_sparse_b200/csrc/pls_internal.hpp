@@ -279,23 +279,41 @@ struct TileDev {
   HostFlag err;
   // Measured choice between the SpMM kernels for the call signature
   // `choice_sig` (k, ldb, value and API types): 0 row group 64-bit offsets,
-  // 2 row group 32-bit, 3 row group with shared entries, 1 staged, -1 not
-  // measured; with the staged and the best row-group timing (ms).
+  // 2 row group 32-bit, 3 row group with shared entries, 1 staged, 4
+  // diagonal form, -1 not measured; with the staged and the best row-group
+  // timing (ms).
   int64_t choice_sig = -1;
   int choice = -1;
   float ms_staged = 0.f, ms_rows = 0.f;
   // Path forced by perflibs_b200_spmat_set_spmm_path: -1 measured choice,
   // 0 row group, 1 staged (when it applies), 2 row group with shared entries
-  // (when the lane shape allows them).
+  // (when the lane shape allows them), 3 diagonal form (when it applies).
   int forced = -1;
   // Path of the last SpMM: 1 staged, 0 row group, 2 row group with shared
-  // entries.
+  // entries, 3 diagonal form.
   int last_path = -1;
+};
+
+// Diagonal form of a CSR matrix for SpMM (built on the first SpMM that
+// measures the kernel choice): every entry (r, c) lies on one of nd
+// diagonals c - r = offs[d] (ascending); vals holds, for every block of
+// kDiaRows rows and every diagonal, the block's kDiaRows values (an
+// absent entry is a reserved NaN bit pattern the kernel skips). state:
+// 0 not examined, 1 built, -1 unsuitable.
+constexpr int kDiaRows = 4;
+constexpr int kDiaMax = 32;
+struct DiaDev {
+  int state = 0;
+  int nd = 0;
+  int32_t offs[kDiaMax] = {};
+  DevBuf vals;
+  uint64_t version = 0;  // vals_version of the values copied
 };
 
 struct CsrDev {
   DevBuf row_ptr, col, vals;  // vals in the API type (authoritative)
   int64_t nnz = 0;
+  uint64_t vals_version = 0;  // counts value updates (invalidates value copies)
   int32_t ncols = 0;  // columns (bound of col); 0 when not recorded
   Vt vt = Vt::F64;
   // Reduced-precision copy of the values used by the kernels when the
@@ -312,6 +330,7 @@ struct CsrDev {
   int long_threshold = 0;
   // Staged-SpMM tiles (built on the first suitable SpMM).
   TileDev tiles;
+  DiaDev dia;
   BandPlan bands;
 };
 
@@ -505,6 +524,13 @@ void spmm_csr(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
 template <class X>
 bool spmm_tiled(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64_t ldc, int k,
                 X alpha, X beta, cudaStream_t s, bool launch = true);
+// Diagonal-form SpMM (a few diagonals, rows sorted and free of duplicate
+// columns, values in the API type, B and C in 16-byte vectors); false
+// (nothing launched) when it does not apply. With launch = false it only
+// builds the diagonal form and says whether it applies.
+template <class X>
+bool spmm_dia(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64_t ldc, int k,
+              X alpha, X beta, cudaStream_t s, bool launch = true);
 template <class X>
 void spmm_bsr(const BsrDev &b, const X *B, int64_t ldb, X *C, int64_t ldc,
               int k, X alpha, X beta, cudaStream_t s);

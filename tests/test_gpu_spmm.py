@@ -467,3 +467,92 @@ def test_staged_wait_timeout_is_reported_and_recoverable():
     s.synchronize()
     ref = spmm_ref(rp, c, v, Bd, 1.0, 0.0, None)
     assert scaled_err(Ct.cpu().numpy(), ref, rp, c, v, Bd, 1.0, 0.0, None) <= 1e-12
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+def test_diagonal_form_spmm(dt):
+    """The diagonal-form SpMM (entries on a few diagonals, kept per block of
+    rows with absent entries skipped). On a 27-point stencil, a 2D Laplacian
+    and a narrow band it takes the diagonal path and equals the row-group
+    kernel bit for bit with beta = 0 (same entries, same ascending order,
+    one fma each); with beta != 0 it matches the oracle. A NaN in a row of B
+    reaches exactly the rows that store an entry in that column. A random
+    matrix does not qualify and keeps the row-group kernel. After the
+    values are updated, the diagonal form is rebuilt from the new values."""
+    import torch
+
+    rng = np.random.default_rng(17)
+    tol = 1e-12 if dt == np.float64 else 1e-5
+    vec = 16 // np.dtype(dt).itemsize
+    cases = [W.stencil_27pt(10, seed=2), W.laplacian_2d(37), W.banded_csr(3001, 3, rng)]
+    for (m, n, rp, c, v) in cases:
+        v = v.astype(dt)
+        A = pls.SpMat.csr(m, n, rp, c, v)
+        for k in (vec, 8, 32, 40, 136):
+            if k % vec:
+                continue
+            Bd = rng.uniform(-1, 1, (n, k)).astype(dt)
+            C0 = rng.uniform(-1, 1, (m, k)).astype(dt)
+            Bt = torch.tensor(Bd, device="cuda")
+            out = {}
+            for path in (0, 3):
+                A.set_spmm_path(path)
+                Ct = torch.zeros((m, k), dtype=Bt.dtype, device="cuda")
+                torch.cuda.synchronize()
+                A.spmm_dev(Bt.data_ptr(), k, k, Ct.data_ptr(), k, 1.0, 0.0)
+                torch.cuda.synchronize()
+                out[path] = (Ct.cpu().numpy(), A.spmm_info()["path"])
+            assert out[3][1] == 3, (m, k)
+            v64, B64 = v.astype(np.float64), Bd.astype(np.float64)
+            if k // vec > 2:  # the row-group kernel also keeps each row in one lane group
+                np.testing.assert_array_equal(out[0][0], out[3][0])
+            Z = np.zeros((m, k))
+            assert scaled_err(out[3][0].astype(np.float64), spmm_ref(rp, c, v64, B64, 1.0, 0.0, Z),
+                              rp, c, v64, B64, 1.0, 0.0, Z) <= tol, (m, k)
+            Ct = torch.tensor(C0, device="cuda")
+            A.spmm_dev(Bt.data_ptr(), k, k, Ct.data_ptr(), k, 1.25, -0.5)
+            torch.cuda.synchronize()
+            v64, B64, C064 = v.astype(np.float64), Bd.astype(np.float64), C0.astype(np.float64)
+            ref = spmm_ref(rp, c, v64, B64, 1.25, -0.5, C064)
+            assert scaled_err(Ct.cpu().numpy().astype(np.float64), ref, rp, c, v64, B64, 1.25, -0.5,
+                              C064) <= tol, (m, k)
+        # a NaN in one row of B reaches the rows with an entry in that column
+        k = 2 * vec
+        Bd = rng.uniform(-1, 1, (n, k)).astype(dt)
+        j = n // 2
+        Bd[j, :] = np.nan
+        Bt = torch.tensor(Bd, device="cuda")
+        Ct = torch.zeros((m, k), dtype=Bt.dtype, device="cuda")
+        A.set_spmm_path(3)
+        A.spmm_dev(Bt.data_ptr(), k, k, Ct.data_ptr(), k, 1.0, 0.0)
+        torch.cuda.synchronize()
+        assert A.spmm_info()["path"] == 3
+        rows_with_j = np.unique(np.repeat(np.arange(m), np.diff(rp))[c == j])
+        nan_rows = np.where(np.isnan(Ct.cpu().numpy()).any(axis=1))[0]
+        np.testing.assert_array_equal(nan_rows, rows_with_j)
+        # updated values: the diagonal form is built again
+        k = 8 if vec <= 8 else vec
+        Bd = rng.uniform(-1, 1, (n, k)).astype(dt)
+        Bt = torch.tensor(Bd, device="cuda")
+        rows = np.repeat(np.arange(m), np.diff(rp))[::5].astype(np.int32)
+        assert A.update(rows, c[::5].astype(np.int32), np.full(len(rows), 2.5, dt)) == 0
+        v2 = v.astype(np.float64)
+        v2[::5] = 2.5
+        Ct = torch.zeros((m, k), dtype=Bt.dtype, device="cuda")
+        A.spmm_dev(Bt.data_ptr(), k, k, Ct.data_ptr(), k, 1.0, 0.0)
+        torch.cuda.synchronize()
+        assert A.spmm_info()["path"] == 3
+        ref = spmm_ref(rp, c, v2, Bd.astype(np.float64), 1.0, 0.0, np.zeros((m, k)))
+        assert scaled_err(Ct.cpu().numpy().astype(np.float64), ref, rp, c, v2, Bd.astype(np.float64),
+                          1.0, 0.0, np.zeros((m, k))) <= tol
+        A.destroy()
+    # a random matrix has no diagonal form: the forced path falls back
+    rp, c, v = W.random_csr(2000, 2000, 20, rng)
+    A = pls.SpMat.csr(2000, 2000, rp, c, v.astype(dt))
+    A.set_spmm_path(3)
+    Bt = torch.tensor(rng.uniform(-1, 1, (2000, 8)).astype(dt), device="cuda")
+    Ct = torch.zeros((2000, 8), dtype=Bt.dtype, device="cuda")
+    A.spmm_dev(Bt.data_ptr(), 8, 8, Ct.data_ptr(), 8, 1.0, 0.0)
+    torch.cuda.synchronize()
+    assert A.spmm_info()["path"] == 0
+    A.destroy()

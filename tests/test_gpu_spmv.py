@@ -323,6 +323,15 @@ def test_transpose_ops():
     # and back to NOTRANS
     xr = rng.uniform(-1, 1, 300)
     np.testing.assert_allclose(A.spmv(xr), oracle.csr_spmv(rp, c, v, xr), rtol=1e-12, atol=1e-13)
+    # values updated after the CSR of A^T was built: the transpose sees them
+    rows = np.repeat(np.arange(400), np.diff(rp))[::7].astype(np.int32)
+    cols = c[::7].astype(np.int32)
+    assert A.update(rows, cols, np.full(len(rows), 3.0)) == 0
+    v2 = v.copy()
+    v2[::7] = 3.0
+    yref2 = oracle.csr_spmv_trans(rp, c, v2, 300, x, y=y0, alpha=1.25, beta=0.5)
+    y = A.spmv(x, y0.copy(), alpha=1.25, beta=0.5, trans=pls.OPERATION_TRANS)
+    np.testing.assert_allclose(y, yref2, rtol=1e-11, atol=1e-12)
 
 
 def test_device_pointer_exec_on_torch_stream():
