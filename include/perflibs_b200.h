@@ -135,10 +135,17 @@ perflibs_status_t perflibs_b200_spmat_exec_info(perflibs_spmat_t A,
  * and passing them round. The first SpMM of each (k, ldb, value type) times
  * the candidates that apply (the staged kernel needs B rows reused inside
  * row blocks, B 16-byte aligned, ldb and k multiples of 16 bytes) on scratch
- * output and keeps the fastest. set_spmm_path overrides that: -1 measured
- * choice (default), 0 row-group kernel, 1 staged kernel whenever it
- * applies, 2 row-group kernel with shared entries whenever the lane shape
- * allows (at least 4 lanes per row of C). */
+ * output and keeps the fastest. The diagonal-form kernel is a candidate
+ * when A's entries lie on at most 32 diagonals (the longest row's
+ * offsets covering every entry, at least half the diagonal slots filled),
+ * its rows are sorted without duplicate columns, its values are in the API
+ * type, and B and C rows are 16-byte vectors: each thread computes 4
+ * consecutive rows and loads each row of B once per run of consecutive
+ * diagonals. set_spmm_path overrides the choice: -1 measured choice
+ * (default), 0 row-group kernel, 1 staged kernel whenever it applies, 2
+ * row-group kernel with shared entries whenever the lane shape allows (at
+ * least 4 lanes per row of C), 3 diagonal-form kernel whenever it
+ * applies. */
 perflibs_status_t perflibs_b200_spmat_set_spmm_path(perflibs_spmat_t A, int32_t path);
 
 /* Host-buffer SpMV (perflibs_spmv_exec_{s,d}) in row bands: the kernels of
@@ -158,8 +165,8 @@ perflibs_status_t perflibs_b200_spmat_host_bands_used(perflibs_spmat_t A, int32_
 /* SpMM plan of the handle: the staged tiles' block height R (0 when none
  * were built: the staged kernel does not apply), the B rows staged per
  * column tile over all blocks and the copy runs; the path the last SpMM
- * took (1 staged, 0 row-group, 2 row-group with shared entries, -1 none
- * yet); and the two timings of the
+ * took (1 staged, 0 row-group, 2 row-group with shared entries, 3
+ * diagonal form, -1 none yet); and the two timings of the
  * measured choice in milliseconds (0 when not measured). Any output may be
  * NULL. */
 perflibs_status_t perflibs_b200_spmat_spmm_info(perflibs_spmat_t A, int32_t *tile_rows,
