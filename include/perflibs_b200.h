@@ -138,8 +138,8 @@ perflibs_status_t perflibs_b200_spmat_exec_info(perflibs_spmat_t A,
  * output and keeps the fastest. The diagonal-form kernel is a candidate
  * when A's entries lie on at most 32 diagonals (the longest row's
  * offsets covering every entry, at least half the diagonal slots filled),
- * its rows are sorted without duplicate columns, its values are in the API
- * type, and B and C rows are 16-byte vectors: each thread computes 4
+ * its rows are sorted without duplicate columns, and B and C rows are
+ * 16-byte vectors (any storage mode): each thread computes 4
  * consecutive rows and loads each row of B once per run of consecutive
  * diagonals. set_spmm_path overrides the choice: -1 measured choice
  * (default), 0 row-group kernel, 1 staged kernel whenever it applies, 2

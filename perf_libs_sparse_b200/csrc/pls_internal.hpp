@@ -297,9 +297,9 @@ struct TileDev {
 // Diagonal form of a CSR matrix for SpMM (built on the first SpMM that
 // measures the kernel choice): every entry (r, c) lies on one of nd
 // diagonals c - r = offs[d] (ascending); vals holds, for every block of
-// kDiaRows rows and every diagonal, the block's kDiaRows values (an
-// absent entry is a reserved NaN bit pattern the kernel skips). state:
-// 0 not examined, 1 built, -1 unsuitable.
+// kDiaRows rows and every diagonal, the block's kDiaRows values in the
+// kernels' value type (an absent entry is a reserved NaN bit pattern the
+// kernel skips). state: 0 not examined, 1 built, -1 unsuitable.
 constexpr int kDiaRows = 4;
 constexpr int kDiaMax = 32;
 struct DiaDev {
@@ -307,7 +307,11 @@ struct DiaDev {
   int nd = 0;
   int32_t offs[kDiaMax] = {};
   DevBuf vals;
-  uint64_t version = 0;  // vals_version of the values copied
+  // What was examined: vals_version, type and buffer of the kernels' values
+  // (a change of any of them means examining the matrix again).
+  uint64_t version = 0;
+  Vt vt = Vt::F64;
+  const void *src = nullptr;
 };
 
 struct CsrDev {
@@ -525,7 +529,7 @@ template <class X>
 bool spmm_tiled(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64_t ldc, int k,
                 X alpha, X beta, cudaStream_t s, bool launch = true);
 // Diagonal-form SpMM (a few diagonals, rows sorted and free of duplicate
-// columns, values in the API type, B and C in 16-byte vectors); false
+// columns, B and C in 16-byte vectors); false
 // (nothing launched) when it does not apply. With launch = false it only
 // builds the diagonal form and says whether it applies.
 template <class X>

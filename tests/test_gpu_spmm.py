@@ -546,6 +546,26 @@ def test_diagonal_form_spmm(dt):
         assert scaled_err(Ct.cpu().numpy().astype(np.float64), ref, rp, c, v2, Bd.astype(np.float64),
                           1.0, 0.0, np.zeros((m, k))) <= tol
         A.destroy()
+    # reduced value storage (FP32 / BF16 values, FP32 accumulation): the
+    # diagonal form keeps the stored values and sums like the row-group kernel
+    m, n, rp, c, v = W.stencil_27pt(9, seed=4)
+    A = pls.SpMat.csr(m, n, rp, c, v.astype(dt))
+    k = 32
+    Bd = rng.uniform(-1, 1, (n, k)).astype(dt)
+    Bt = torch.tensor(Bd, device="cuda")
+    storages = [pls.STORAGE_BF16] + ([pls.STORAGE_FP32] if dt == np.float64 else [])
+    for storage in storages:
+        A.set_storage(storage)
+        out = {}
+        for path in (0, 3):
+            A.set_spmm_path(path)
+            Ct = torch.zeros((m, k), dtype=Bt.dtype, device="cuda")
+            A.spmm_dev(Bt.data_ptr(), k, k, Ct.data_ptr(), k, 1.0, 0.0)
+            torch.cuda.synchronize()
+            out[path] = (Ct.cpu().numpy(), A.spmm_info()["path"])
+        assert out[3][1] == 3, storage
+        np.testing.assert_array_equal(out[0][0], out[3][0])
+    A.destroy()
     # a random matrix has no diagonal form: the forced path falls back
     rp, c, v = W.random_csr(2000, 2000, 20, rng)
     A = pls.SpMat.csr(2000, 2000, rp, c, v.astype(dt))
