@@ -341,7 +341,9 @@ perflibs_status_t perflibs_b200_batch_tune(perflibs_b200_batch_t Bt,
                                            float *best_ms);
 perflibs_status_t perflibs_b200_batch_exec(perflibs_b200_batch_t Bt,
                                            float alpha, float beta);
-/* Work items and kernel launches of one exec. */
+/* Per-warp work items (the staged items are counted by
+ * perflibs_b200_batch_stage_info), kernel launches of one exec, and the
+ * rows per item. */
 perflibs_status_t perflibs_b200_batch_info(perflibs_b200_batch_t Bt,
                                            int64_t *n_items,
                                            int32_t *launches_per_exec,
