@@ -3,13 +3,13 @@
 Default workload (N=1): FP64 SELL-C-sigma SpMV on the power-law matrix
 (n = 4,194,304 rows, row lengths Zipf-Mandelbrot p(k) ~ (k + q)^-2 on
 [1, 4096] with q solved for mean 16, uniform unique columns, N(0,1) values,
-x ~ U[-1,1], seed 1), C and sigma
-picked by the exhaustive autotuner, compared with the plain CSR kernel on
-the same matrix. A step is one y = A*x over the whole matrix with inputs
-resident in HBM (889 MB of algorithmic traffic: larger than the 126 MB L2,
-so no flush is needed between steps).
+x ~ U[-1,1], seed 1), C and sigma (sigma in 32..8192) picked by the
+exhaustive autotuner, compared with the plain CSR kernel on the same matrix.
+A step is one y = A*x over the whole matrix with inputs resident in HBM
+(889 MB of algorithmic traffic: larger than the 126 MB L2, so no flush is
+needed between steps).
 
-Reported:
+Reported on the one line:
   value      algorithmic GB/s of the tuned kernel (x, y and the matrix
              counted once, SELL padding not counted), summed over ranks;
   e2e        the same metric through the drop-in C call
@@ -18,11 +18,19 @@ Reported:
              each band's copy overlapping the next band's kernels);
   roofline   the dominant kernel's achieved GB/s vs the measured HBM peak;
   cpu_baseline  the reference library (compiled from its own sources,
-             OpenMP on all host cores) on the same matrix, same metric.
+             OpenMP on all host cores) on the same matrix, same metric;
+  configs    the other matrix configurations, each with its own time,
+             roofline and max relative error against the FP64 oracle:
+             c1 (5-point Laplacian 512^2, plain FP64 CSR SpMV, timed over
+             rotating copies so that L2 cannot hold them), c3 (CSR SpMM on
+             the 27-point 128^3 stencil, k = 8 / 32 / 128 in FP64 and k = 32
+             with FP32 / BF16 value storage) and c4 (512 uneven FP32 SpMMs
+             in one persistent launch, a CUDA graph).
 
---impl reference times only the reference CPU implementation.
+--impl reference times only the reference CPU implementation, on the same
+metric, unit and workload as the default line.
 Multi-GPU (torchrun): independent replicas, one per GPU (the path needs no
-exchange), max time over ranks.
+exchange), max time over ranks; the extra configurations run at N = 1 only.
 """
 from __future__ import annotations
 
@@ -43,6 +51,12 @@ sys.path.insert(0, ROOT)
 from perf_libs_sparse_b200 import workloads as W  # noqa: E402
 
 FALLBACK_HBM_GBS = 6650.0
+# The headline metric, printed identically by both arms (this library on the
+# GPU and the reference library on the host cores).
+METRIC = "SpMV/SpMM GB/s vs B200 HBM roofline; tuned vs plain CSR at ≤1e-12 rel err"
+C2_WORKLOAD = "C2 power-law SpMV n=4194304 nnz={nnz}, FP64, sigma in 32..8192"
+SIGMA_RANGE = (32, 8192)
+KIND_NAMES = {0: "CSR", 1: "SELL-C-sigma", 2: "CSR-split"}
 
 
 def peaks():
@@ -146,6 +160,57 @@ def make_c2():
     return m, n, rp, c, v, x
 
 
+def roofline(gbs: float, traffic=None):
+    hbm, kind = peaks()
+    return {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+            "peak_source": kind, "traffic": traffic}
+
+
+# ------------------------------------------------------------------ parity
+# The FP64 oracle (the reference algorithm restated in C, oracle/) checks each
+# timed result after its timing.
+
+
+def spmv_rel_err(y, rp, c, v, x):
+    """max_i |y_i - y_ref_i| / max(|y_ref_i|, sum_j |a_ij x_j|)."""
+    import oracle
+
+    y_ref = oracle.csr_spmv(rp, c, v, x)
+    den = np.maximum(np.abs(y_ref), oracle.csr_absdot(rp, c, v, x))
+    den[den == 0] = 1
+    return float((np.abs(y - y_ref) / den).max()), y_ref
+
+
+def spmm_rel_err_rows(get_rows, rp, c, v, B, k, blocks):
+    """Per-row scaled error of C = A*B over the row blocks [r0, r1): the
+    reference is the FP64 oracle on A's FP64 values and the FP64 B; the
+    scale of row i is sum_j |a_ij| |B_j|. get_rows(r0, r1) returns the
+    computed rows as an FP64 array."""
+    import oracle
+
+    worst = 0.0
+    for r0, r1 in blocks:
+        p0, p1 = int(rp[r0]), int(rp[r1])
+        sub = (rp[r0:r1 + 1] - rp[r0]).astype(np.int32)
+        cc, vv = c[p0:p1], v[p0:p1]
+        ref = oracle.csr_spmm(sub, cc, vv, B, k)
+        scale = oracle.csr_spmm(sub, cc, np.abs(vv), np.abs(B), k)
+        got = get_rows(r0, r1)
+        den = np.maximum(np.abs(ref), scale)
+        den[den == 0] = 1
+        worst = max(worst, float((np.abs(got - ref) / den).max()))
+    return worst
+
+
+def row_blocks(m: int, full: bool, block=16384, count=8):
+    """All rows in blocks, or `count` blocks of `block` rows spread evenly
+    (the first and the last included)."""
+    if full:
+        return [(r, min(m, r + 262144)) for r in range(0, m, 262144)]
+    starts = np.linspace(0, m - block, count).astype(np.int64)
+    return [(int(s), int(s) + block) for s in starts]
+
+
 # ------------------------------------------------------------------ CPU leg
 
 
@@ -177,8 +242,10 @@ def cpu_reference_spmv(m, n, rp, c, v, x, reps: int, budget_s: float = 20.0):
                 break
         fmt = A.format()
         A.destroy()
+        # spmat_format_t (src/util.hpp:256-275): 0 CSR, 2 SELL-C-sigma.
+        fname = {0: "CSR", 2: "SELL-C-sigma"}.get(fmt[0], f"format {fmt[0]}")
         sample = (f"full matrix, {len(times)} perflibs_spmv_exec_d calls after perflibs_spmv_optimize "
-                  f"(audition chose format {fmt[0]}, C={fmt[1]}, sigma={fmt[2]}); OMP threads={threads}")
+                  f"(its audition chose {fname}, C={fmt[1]}, sigma={fmt[2]}); OMP threads={threads}")
     else:
         t_opt = 0.0
         oracle.csr_spmv(rp, c, v, x, y=y)
@@ -205,11 +272,11 @@ def run_reference(args):
     reps = max(1, args.warmup + args.steps)
     gbs, sec, t_opt, threads, kind, sample = cpu_reference_spmv(m, n, rp, c, v, x, reps, budget_s=120.0)
     line = {
-        "metric": "SpMV GB/s (algorithmic bytes), FP64, power-law matrix",
+        "metric": METRIC,
         "value": gbs, "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "C2 power-law SpMV n=4194304 nnz=%d" % int(rp[-1]), "optimize_s": t_opt},
+        "config": {"workload": C2_WORKLOAD.format(nnz=int(rp[-1])), "optimize_s": t_opt},
         "impl": "reference",
         "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -219,6 +286,217 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------ GPU leg
+
+
+class Timer:
+    """CUDA-event timing on one stream: W untimed steps, then K steps under
+    one event pair (a synchronize and, with a process group, a barrier on
+    both sides)."""
+
+    def __init__(self, stream, world=1, device=None):
+        import torch
+
+        self.torch = torch
+        self.stream = stream
+        self.world = world
+        self.device = device
+
+    def __call__(self, step, K, Wm, label=None):
+        torch = self.torch
+        with torch.cuda.stream(self.stream):
+            for _ in range(Wm):
+                step()
+            torch.cuda.synchronize()
+            if self.world > 1:
+                torch.distributed.barrier()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            if label:
+                torch.cuda.nvtx.range_push(label)
+            e0.record(self.stream)
+            for _ in range(K):
+                step()
+            e1.record(self.stream)
+            torch.cuda.synchronize()
+            if label:
+                torch.cuda.nvtx.range_pop()
+            ms = e0.elapsed_time(e1)
+        return max_over_ranks(ms, self.device) / K
+
+
+def c1_config(args, timer, sp):
+    """C1: plain FP64 CSR SpMV on the 5-point Laplacian 512^2 (21 MB). One
+    step is one SpMV; steps go round R copies of the matrix, x and y
+    (R * 21 MB > 2 x 126 MB of L2), so every step reads its inputs from HBM.
+    The R-step rounds are captured in one CUDA graph and K steps are timed
+    under one event pair."""
+    import torch
+
+    import perf_libs_sparse_b200 as pls
+
+    m, n, rp, c, v = W.laplacian_2d(512)
+    x = W.uniform_vector(n, 0)
+    nnz = int(rp[-1])
+    R = 12
+    mats, xs, ys = [], [], []
+    for _ in range(R):
+        A = pls.SpMat.csr(m, n, rp, c, v)
+        A.set_stream(sp)
+        A.hint(pls.HINT_SPMV_INVOCATIONS, pls.INVOCATIONS_SINGLE)  # plain CSR, no tuning
+        assert A.optimize() == 0
+        mats.append(A)
+        xs.append(torch.tensor(x, device="cuda"))
+        ys.append(torch.zeros(m, dtype=torch.float64, device="cuda"))
+
+    def round_():
+        for i in range(R):
+            mats[i].spmv_dev(xs[i].data_ptr(), ys[i].data_ptr(), 1.0, 0.0, sp)
+
+    graph = None
+    try:
+        round_()
+        torch.cuda.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=timer.stream, capture_error_mode="thread_local"):
+            round_()
+        torch.cuda.synchronize()
+        step = graph.replay
+    except Exception:
+        graph = None
+        step = round_
+    rounds = max(8, args.steps)
+    ms_round = timer(step, rounds, max(args.warmup, 3))
+    ms = ms_round / R
+    err, _ = spmv_rel_err(ys[0].cpu().numpy(), rp, c, v, x)
+    b = W.algorithmic_bytes_spmv(m, n, nnz, 8, 8, False)
+    gbs = b / ms / 1e6
+    cfg = mats[0].config()
+    out = {"workload": f"C1 5-point Laplacian 512x512 n={m} nnz={nnz}, plain FP64 CSR SpMV",
+           "kernel": f"CSR threads-per-row {cfg['tpr']}", "value": gbs, "unit": "GB/s",
+           "ms_per_step": ms, "steps": rounds * R, "gflops": 2.0 * nnz / ms / 1e6,
+           "max_rel_err": err, "tolerance": 1e-12,
+           "l2": f"{R} rotating copies of matrix, x and y ({R * b / 1e6:.0f} MB) "
+                 f"in {'one CUDA graph per round' if graph else 'direct launches'}",
+           "algorithmic_bytes_per_step": b, "roofline": roofline(gbs)}
+    del graph
+    for A in mats:
+        A.destroy()
+    return out
+
+
+def c3_config(args, timer, sp, arms):
+    """C3: CSR SpMM C = A*B on the 27-point 128^3 stencil (n = 2,097,152,
+    nnz = 55,742,968), B n x k row-major U[-1,1] (seed 2). Each arm is one
+    (k, storage) pair; the kernel is the library's measured choice. A step
+    is one SpMM; inputs exceed L2 at every k, so no flush."""
+    import torch
+
+    import perf_libs_sparse_b200 as pls
+
+    m, n, rp, c, v = W.stencil_27pt(128, seed=2)
+    nnz = int(rp[-1])
+    out = {"workload": f"C3 27-point stencil 128^3 n={m} nnz={nnz}, CSR SpMM C = A*B",
+           "arms": []}
+    kmax = max(k for k, _ in arms)
+    Bfull = np.random.default_rng(2).uniform(-1, 1, (n, kmax))
+    for k, storage in arms:
+        B = np.ascontiguousarray(Bfull[:, :k]) if k < kmax else Bfull
+        native = storage == "native"
+        dt = np.float64 if native else np.float32
+        tdt = torch.float64 if native else torch.float32
+        A = pls.SpMat.csr(m, n, rp, c, v.astype(dt))
+        A.set_storage({"native": pls.STORAGE_NATIVE, "fp32": pls.STORAGE_FP32,
+                       "bf16": pls.STORAGE_BF16}[storage])
+        A.set_stream(sp)
+        assert A.optimize() == 0
+        Bd = torch.tensor(B, dtype=tdt, device="cuda")
+        Cd = torch.zeros((m, k), dtype=tdt, device="cuda")
+        t0 = time.perf_counter()
+        A.spmm_dev(Bd.data_ptr(), k, k, Cd.data_ptr(), k, 1.0, 0.0, sp)  # measured choice
+        torch.cuda.synchronize()
+        t_choice = time.perf_counter() - t0
+        K = max(args.steps, 10)
+        ms = timer(lambda: A.spmm_dev(Bd.data_ptr(), k, k, Cd.data_ptr(), k, 1.0, 0.0, sp),
+                   K, max(args.warmup, 3))
+        torch.cuda.synchronize()
+        full = k <= 32
+        err = spmm_rel_err_rows(lambda r0, r1: Cd[r0:r1].cpu().numpy().astype(np.float64),
+                                rp, c, v, B, k, row_blocks(m, full))
+        sv = 8 if native else (4 if storage == "fp32" else 2)
+        sb = 8 if native else 4
+        b = W.algorithmic_bytes_spmm(m, n, nnz, k, sv, sb, False)
+        gbs = b / ms / 1e6
+        info = A.spmm_info()
+        out["arms"].append({
+            "k": k, "storage": storage,
+            "dtype": {"native": "f64", "fp32": "f32 values, B and C; f32 accumulate",
+                      "bf16": "bf16 values, f32 B and C; f32 accumulate"}[storage],
+            "value": gbs, "unit": "GB/s", "ms_per_step": ms, "steps": K,
+            "gflops": 2.0 * nnz * k / ms / 1e6, "max_rel_err": err,
+            "tolerance": {"native": 1e-12, "fp32": 1e-5, "bf16": 1e-2}[storage],
+            "rows_checked": "all" if full else "8 blocks of 16384 rows",
+            "kernel": SPMM_PATHS.get(info["path"], str(info["path"])),
+            "first_call_s": t_choice, "algorithmic_bytes_per_step": b,
+            "roofline": roofline(gbs)})
+        del Bd, Cd
+        A.destroy()
+    return out
+
+
+SPMM_PATHS = {-1: "none", 0: "row group", 1: "staged", 2: "row group, shared entries",
+              3: "diagonal form", 4: "diagonal form, TMA-staged B", 5: "BSR tensor core"}
+
+
+def c4_config(args, timer, sp):
+    """C4: 512 uneven FP32 SpMMs (banded, random uniform and BSR
+    block-diagonal instances, n in [1024, 65536], k in [1, 64], seed 3) in
+    one persistent launch, replayed as a CUDA graph; tile schedule from the
+    batch autotuner. A step is one batch launch (2.9 GB, beyond L2)."""
+    import torch
+
+    import oracle
+    import perf_libs_sparse_b200 as pls
+
+    inst = W.batched_instances(512, seed=3)
+    mats, Bs, Cs = [], [], []
+    for d in inst:
+        if d["kind"] == "bsr":
+            mats.append(pls.SpMat.bsr(d["layout"], d["m"], d["n"], d["bs"], d["row_ptr"], d["col"], d["vals"]))
+        else:
+            mats.append(pls.SpMat.csr(d["m"], d["n"], d["row_ptr"], d["col"], d["vals"]))
+        Bs.append(torch.tensor(d["B"], device="cuda"))
+        Cs.append(torch.zeros((d["m"], d["k"]), dtype=torch.float32, device="cuda"))
+    ks = [d["k"] for d in inst]
+    bt = pls.Batch(mats, ks, [b_.data_ptr() for b_ in Bs], ks, [c_.data_ptr() for c_ in Cs], ks, stream=sp)
+    tile, _ = bt.tune()
+    K = max(args.steps, 10)
+    ms = timer(lambda: bt.exec(1.0, 0.0), K, max(args.warmup, 3))
+    torch.cuda.synchronize()
+    worst = 0.0
+    for d, Cd in zip(inst, Cs):
+        if d["kind"] == "bsr":
+            rp, cc, vv = oracle.bsr2csr(d["row_ptr"], d["col"], d["vals"].astype(np.float64), d["bs"], d["layout"])
+        else:
+            rp, cc, vv = d["row_ptr"], d["col"], d["vals"].astype(np.float64)
+        B = d["B"].astype(np.float64)
+        ref = oracle.csr_spmm(rp, cc, vv, B, d["k"])
+        scale = oracle.csr_spmm(rp, cc, np.abs(vv), np.abs(B), d["k"])
+        den = np.maximum(np.abs(ref), scale)
+        den[den == 0] = 1
+        worst = max(worst, float((np.abs(Cd.cpu().numpy().astype(np.float64) - ref) / den).max()))
+    b = sum(W.algorithmic_bytes_spmm(d["m"], d["n"], W.instance_nnz(d), d["k"], 4, 4, False) for d in inst)
+    gbs = b / ms / 1e6
+    out = {"workload": "C4 512 uneven FP32 instances (banded / random / BSR bs 4-8), n in [1024, 65536], "
+                       "k in [1, 64], one persistent launch per step",
+           "value": gbs, "unit": "GB/s", "ms_per_step": ms, "steps": K, "max_rel_err": worst,
+           "tolerance": 1e-5, "rows_checked": "all instances, all rows",
+           "tile_rows": tile, **bt.info(), **bt.stage_info(),
+           "rows_total": int(sum(d["m"] for d in inst)), "algorithmic_bytes_per_step": b,
+           "roofline": roofline(gbs)}
+    bt.destroy()
+    for A in mats:
+        A.destroy()
+    return out
 
 
 def run_b200(args):
@@ -243,6 +521,7 @@ def run_b200(args):
 
     stream = torch.cuda.Stream(device=dev)
     sp = stream.cuda_stream
+    timer = Timer(stream, world, dev)
 
     # Plain CSR baseline (the default kernel, no tuning).
     A_plain = pls.SpMat.csr(m, n, rp, c, v)
@@ -266,54 +545,33 @@ def run_b200(args):
     def step(M):
         M.spmv_dev(xd.data_ptr(), yd.data_ptr(), 1.0, 0.0, sp)
 
-    def timed(M, K, Wm, label="untimed"):
-        with torch.cuda.stream(stream):
-            for _ in range(Wm):
-                step(M)
-            torch.cuda.synchronize()
-            if world > 1:
-                torch.distributed.barrier()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            torch.cuda.nvtx.range_push(label)
-            e0.record(stream)
-            for _ in range(K):
-                step(M)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            torch.cuda.nvtx.range_pop()
-            ms = e0.elapsed_time(e1)
-        return max_over_ranks(ms, dev) / K
-
     K, Wm = args.steps, max(args.warmup, 3)
     # Keep the GPU busy ~0.5 s before each timed region, so that the clock
     # samples see the kernel under load and every arm (tuned, plain CSR, the
     # selector's) is timed in the same sustained power state.
     soak = max(1, int(args.soak_seconds / max(bytes_step / 6.0e12, 1e-6)))
 
-    def measure(M, label="untimed"):
-        timed(M, soak, 1)
-        return timed(M, K, Wm, label)
+    def measure(M, label=None):
+        timer(lambda: step(M), soak, 1)
+        return timer(lambda: step(M), K, Wm, label)
 
     with ClockSampler(local) as clk:
         ms_tuned = measure(A, "timed")
     ms_plain = measure(A_plain)
 
     # Parity of the timed result (full size) against the oracle.
-    import oracle
-
     step(A)
     torch.cuda.synchronize()
     y_gpu = yd.cpu().numpy()
-    y_ref = oracle.csr_spmv(rp, c, v, x)
-    scale = oracle.csr_absdot(rp, c, v, x)
-    den = np.maximum(np.abs(y_ref), scale)
+    max_rel, y_ref = spmv_rel_err(y_gpu, rp, c, v, x)
+    import oracle
+
+    den = np.maximum(np.abs(y_ref), oracle.csr_absdot(rp, c, v, x))
     den[den == 0] = 1
 
     def rel_err(y):
         return float((np.abs(y - y_ref) / den).max())
 
-    max_rel = rel_err(y_gpu)
     # FP64 inf-norm check of the result: ||y - y_ref||_inf / (||A||_inf ||x||_inf),
     # with ||A||_inf from the library's own FP64 norm.
     a_inf = float(A.norm(pls.NORM_INF))
@@ -348,7 +606,7 @@ def run_b200(args):
             ys = yd.cpu().numpy()
             cfg_s = As.config()
             selector_arms[name] = {
-                "format": {0: "CSR", 1: "SELL-C-sigma", 2: "CSR-split"}[cfg_s["kind"]],
+                "format": KIND_NAMES[cfg_s["kind"]],
                 "C": cfg_s["C"], "sigma": cfg_s["sigma"], "tpr": cfg_s["tpr"],
                 "ms_per_step": ms_s, "speedup_vs_plain_csr_fp64": ms_plain / ms_s,
                 "max_rel_err": rel_err(ys), "tolerance": tol, "inf_norm_check": inf_check(ys),
@@ -375,14 +633,13 @@ def run_b200(args):
         assert st == 0
     e2e_s = max_over_ranks((time.perf_counter() - t0) / Ke, dev)
     e2e_bands = A.host_bands_used()
+    e2e_err = rel_err(yh.numpy())
 
-    hbm, peak_kind = peaks()
     achieved = replica_gbs(bytes_step, ms_tuned * 1e-3, 1)  # per GPU
     info = A.exec_info()
     kernels_per_step = info["kernels_per_spmv"]
-    workload = f"C2 power-law SpMV n={m} nnz={nnz}"
     line = {
-        "metric": "SpMV GB/s (algorithmic bytes) vs B200 HBM roofline, FP64, tuned vs plain CSR",
+        "metric": METRIC,
         "value": replica_gbs(bytes_step, ms_tuned * 1e-3, world),
         "unit": "GB/s",
         "n_gpus": world,
@@ -395,9 +652,10 @@ def run_b200(args):
         "dtype": "f64",
         "data": "synthetic",
         "config": {
-            "workload": workload,
-            "format": {0: "CSR", 1: "SELL-C-sigma", 2: "CSR-split"}[cfg["kind"]],
+            "workload": C2_WORKLOAD.format(nnz=nnz),
+            "format": KIND_NAMES[cfg["kind"]],
             "C": cfg["C"], "sigma": cfg["sigma"], "tpr": cfg["tpr"], "col_bytes": cfg["col_bytes"],
+            "sigma_in_range": cfg["kind"] != pls.KIND_SELL or SIGMA_RANGE[0] <= cfg["sigma"] <= SIGMA_RANGE[1],
             "sell_items": info["n_items"], "sell_split_chunks": info["n_split"],
             "algorithmic_bytes_per_step": bytes_step,
             "l2": "inputs (889 MB) exceed the 126 MB L2; no flush between steps",
@@ -412,13 +670,22 @@ def run_b200(args):
         "selector": selector_arms or None,
         "e2e": {"value": replica_gbs(bytes_step, e2e_s, world), "unit": "GB/s",
                 "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": m * 8, "ms_per_step": e2e_s * 1e3,
-                "row_bands": e2e_bands},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "peak_source": peak_kind,
-                     "traffic": load_traffic("c2_spmv_fp64")},
+                "row_bands": e2e_bands, "max_rel_err": e2e_err},
+        "roofline": roofline(achieved, load_traffic("c2_spmv_fp64")),
         "gpu_launches": K * kernels_per_step,
         "clocks": clk.summary(),
     }
+    A.destroy()
+    A_plain.destroy()
+    del xd, yd
+    if rank == 0 and world == 1 and not args.no_configs:
+        torch.cuda.empty_cache()
+        line["configs"] = {
+            "c1": c1_config(args, timer, sp),
+            "c3": c3_config(args, timer, sp, [(8, "native"), (32, "native"), (128, "native"),
+                                              (32, "fp32"), (32, "bf16")]),
+            "c4": c4_config(args, timer, sp),
+        }
     if rank == 0 and world == 1 and not args.no_cpu:
         os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
         os.environ.setdefault("OMP_PROC_BIND", "close")
@@ -427,8 +694,6 @@ def run_b200(args):
                                 "sample": sample, "optimize_s": t_opt_cpu, "ms_per_step": sec * 1e3}
     if rank == 0:
         emit(line, args)
-    A.destroy()
-    A_plain.destroy()
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
@@ -436,54 +701,25 @@ def run_b200(args):
 
 
 def run_extra(args):
-    """Non-default workloads, one JSON line each (N = 1):
-    c1  FP64 CSR SpMV, 5-point Laplacian 512^2 (21 MB: L2-resident, so a
-        256 MB buffer is written between steps and only the SpMV is timed);
-    c3  CSR SpMM on the 27-point 128^3 stencil, k = --k, value storage
-        --storage (native = FP64 A, B, C; fp32 / bf16 = FP32 B, C and FP32 /
-        BF16 A values, FP32 accumulation), max relative error vs the FP64
-        oracle reported;
-    c4  the 512-instance uneven batch (FP32) in one persistent launch per
-        step (a CUDA graph), row tile picked by the batch autotuner."""
+    """One configuration alone, as its own JSON line (N = 1): c1, c3 (k =
+    --k, storage --storage), c4, or c3spmv (FP64 SpMV, tuned, on C3's
+    matrix: the structured counterpart of C2). The default line carries
+    c1 / c3 / c4 too; these lines are for profiling one kernel."""
     import torch
 
-    import oracle
     import perf_libs_sparse_b200 as pls
 
     torch.cuda.set_device(0)
     stream = torch.cuda.Stream()
     sp = stream.cuda_stream
-    hbm, peak_kind = peaks()
-    K, Wm = args.steps, max(args.warmup, 3)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-
-    def timed(step, flush=None):
-        with torch.cuda.stream(stream):
-            for _ in range(Wm):
-                step()
-            torch.cuda.synchronize()
-            if flush is None:
-                e0.record(stream)
-                for _ in range(K):
-                    step()
-                e1.record(stream)
-                torch.cuda.synchronize()
-                return e0.elapsed_time(e1) / K
-            tot = 0.0
-            for _ in range(K):
-                flush()
-                e0.record(stream)
-                step()
-                e1.record(stream)
-                torch.cuda.synchronize()
-                tot += e0.elapsed_time(e1)
-            return tot / K
-
-    line = {"n_gpus": 1, "steps": K, "warmup": Wm, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "data": "synthetic", "unit": "GB/s"}
-    if args.workload == "c3spmv":
-        # FP64 SpMV (tuned) on C3's matrix: the structured counterpart of C2,
-        # where x gathers are neighbours instead of uniformly random.
+    timer = Timer(stream)
+    if args.workload == "c1":
+        sub = c1_config(args, timer, sp)
+    elif args.workload == "c3":
+        sub = c3_config(args, timer, sp, [(args.k, args.storage)])["arms"][0]
+    elif args.workload == "c4":
+        sub = c4_config(args, timer, sp)
+    else:
         m, n, rp, c, v = W.stencil_27pt(128, seed=2)
         x = W.uniform_vector(n, 2)
         A = pls.SpMat.csr(m, n, rp, c, v)
@@ -496,103 +732,22 @@ def run_extra(args):
         assert P.optimize() == 0
         xd = torch.tensor(x, device="cuda")
         yd = torch.zeros(m, dtype=torch.float64, device="cuda")
-        ms_plain = timed(lambda: P.spmv_dev(xd.data_ptr(), yd.data_ptr(), 1.0, 0.0, sp))
-        ms = timed(lambda: A.spmv_dev(xd.data_ptr(), yd.data_ptr(), 1.0, 0.0, sp))
+        K, Wm = args.steps, max(args.warmup, 3)
+        ms_plain = timer(lambda: P.spmv_dev(xd.data_ptr(), yd.data_ptr(), 1.0, 0.0, sp), K, Wm)
+        ms = timer(lambda: A.spmv_dev(xd.data_ptr(), yd.data_ptr(), 1.0, 0.0, sp), K, Wm)
         torch.cuda.synchronize()
-        y = yd.cpu().numpy()
-        y_ref = oracle.csr_spmv(rp, c, v, x)
-        sc = oracle.csr_absdot(rp, c, v, x)
-        err = float((np.abs(y - y_ref) / np.maximum(np.maximum(np.abs(y_ref), sc), 1e-300)).max())
+        err, _ = spmv_rel_err(yd.cpu().numpy(), rp, c, v, x)
         b = W.algorithmic_bytes_spmv(m, n, int(rp[-1]), 8, 8, False)
         cfg = A.config()
-        line.update(metric="SpMV GB/s (algorithmic bytes), FP64, 27-point stencil 128^3, tuned vs plain CSR",
-                    dtype="f64", value=b / ms / 1e6, ms_per_step=ms, max_rel_err=err,
-                    plain_csr={"value": b / ms_plain / 1e6, "ms_per_step": ms_plain},
-                    speedup_vs_plain_csr=ms_plain / ms,
-                    config={"workload": "27-point stencil 128^3 n=2097152 nnz=55742968 (C3's matrix)",
-                            "format": {0: "CSR", 1: "SELL-C-sigma", 2: "CSR-split"}[cfg["kind"]],
-                            "C": cfg["C"], "sigma": cfg["sigma"], "tpr": cfg["tpr"],
-                            "l2": "inputs (711 MB) exceed L2; no flush"})
-    elif args.workload == "c1":
-        m, n, rp, c, v = W.laplacian_2d(512)
-        x = W.uniform_vector(n, 0)
-        A = pls.SpMat.csr(m, n, rp, c, v)
-        A.set_stream(sp)
-        assert A.optimize() == 0
-        xd = torch.tensor(x, device="cuda")
-        yd = torch.zeros(m, dtype=torch.float64, device="cuda")
-        flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-        ms = timed(lambda: A.spmv_dev(xd.data_ptr(), yd.data_ptr(), 1.0, 0.0, sp),
-                   flush=lambda: flush_buf.fill_(1))
-        torch.cuda.synchronize()
-        y = yd.cpu().numpy()
-        y_ref = oracle.csr_spmv(rp, c, v, x)
-        sc = oracle.csr_absdot(rp, c, v, x)
-        err = float((np.abs(y - y_ref) / np.maximum(np.maximum(np.abs(y_ref), sc), 1e-300)).max())
-        b = W.algorithmic_bytes_spmv(m, n, int(rp[-1]), 8, 8, False)
-        line.update(metric="SpMV GB/s (algorithmic bytes), FP64, 2D Laplacian 512^2", dtype="f64",
-                    value=b / ms / 1e6, ms_per_step=ms, max_rel_err=err,
-                    config={"workload": "C1 Laplacian 512x512 n=262144 nnz=1308672", **A.config(),
-                            "l2": "256 MB written between steps, SpMV alone timed"})
-    elif args.workload == "c3":
-        m, n, rp, c, v = W.stencil_27pt(128, seed=2)
-        k = args.k
-        B = np.random.default_rng(2).uniform(-1, 1, (n, k))
-        native = args.storage == "native"
-        dt = np.float64 if native else np.float32
-        tdt = torch.float64 if native else torch.float32
-        A = pls.SpMat.csr(m, n, rp, c, v.astype(dt))
-        A.set_storage({"native": pls.STORAGE_NATIVE, "fp32": pls.STORAGE_FP32, "bf16": pls.STORAGE_BF16}[args.storage])
-        A.set_stream(sp)
-        assert A.optimize() == 0
-        Bd = torch.tensor(B, dtype=tdt, device="cuda")
-        Cd = torch.zeros((m, k), dtype=tdt, device="cuda")
-        ms = timed(lambda: A.spmm_dev(Bd.data_ptr(), k, k, Cd.data_ptr(), k, 1.0, 0.0, sp))
-        torch.cuda.synchronize()
-        got = Cd.cpu().numpy().astype(np.float64)
-        rows = np.random.default_rng(7).choice(m, 20000, replace=False)
-        rows.sort()
-        # error on a row sample against the FP64 oracle (same seeds)
-        sub_rp = np.concatenate([[0], np.cumsum(rp[rows + 1] - rp[rows])]).astype(np.int32)
-        idx = np.concatenate([np.arange(rp[r], rp[r + 1]) for r in rows])
-        ref = oracle.csr_spmm(sub_rp, c[idx], v[idx], B, k)
-        scale = oracle.csr_spmm(sub_rp, c[idx], np.abs(v[idx]), np.abs(B), k)
-        err = float((np.abs(got[rows] - ref) / np.maximum(np.maximum(np.abs(ref), scale), 1e-300)).max())
-        # FP64 inf-norm check on the same rows: max row sum |C - C_ref| over
-        # ||A||_inf ||B||_inf (||A||_inf from the library's FP64 norm).
-        inf_chk = float(np.abs(got[rows] - ref).sum(axis=1).max()
-                        / max(float(A.norm(pls.NORM_INF)) * float(np.abs(B).sum(axis=1).max()), 1e-300))
-        sv = 8 if native else (4 if args.storage == "fp32" else 2)
-        sb = 8 if native else 4
-        b = W.algorithmic_bytes_spmm(m, n, int(rp[-1]), k, sv, sb, False)
-        line.update(metric=f"SpMM GB/s (algorithmic bytes), 27-point 128^3, k={k}, storage {args.storage}",
-                    dtype={"native": "f64", "fp32": "f32", "bf16": "bf16 values, f32 accumulate"}[args.storage],
-                    value=b / ms / 1e6, ms_per_step=ms, max_rel_err=err, inf_norm_check=inf_chk,
-                    gflops=2.0 * int(rp[-1]) * k / ms / 1e6,
-                    config={"workload": "C3 27-point stencil 128^3 n=2097152 nnz=55742968", "k": k,
-                            "storage": args.storage, "l2": "inputs exceed L2; no flush",
-                            "spmm": A.spmm_info()})
-    elif args.workload == "c4":
-        inst = W.batched_instances(512, seed=3)
-        mats, Bs, Cs = [], [], []
-        for d in inst:
-            if d["kind"] == "bsr":
-                mats.append(pls.SpMat.bsr(d["layout"], d["m"], d["n"], d["bs"], d["row_ptr"], d["col"], d["vals"]))
-            else:
-                mats.append(pls.SpMat.csr(d["m"], d["n"], d["row_ptr"], d["col"], d["vals"]))
-            Bs.append(torch.tensor(d["B"], device="cuda"))
-            Cs.append(torch.zeros((d["m"], d["k"]), dtype=torch.float32, device="cuda"))
-        ks = [d["k"] for d in inst]
-        bt = pls.Batch(mats, ks, [b_.data_ptr() for b_ in Bs], ks, [c_.data_ptr() for c_ in Cs], ks, stream=sp)
-        tile, _ = bt.tune()
-        ms = timed(lambda: bt.exec(1.0, 0.0))
-        b = sum(W.algorithmic_bytes_spmm(d["m"], d["n"], W.instance_nnz(d), d["k"], 4, 4, False) for d in inst)
-        line.update(metric="Batched SpMM GB/s (algorithmic bytes), 512 uneven FP32 instances, one persistent launch",
-                    dtype="f32", value=b / ms / 1e6, ms_per_step=ms,
-                    config={"workload": "C4 512 instances n in [1024, 65536], k in [1, 64]", "tile_rows": tile,
-                            **bt.info(), **bt.stage_info(), "rows_total": int(sum(d["m"] for d in inst))})
-    line["roofline"] = {"bound": "hbm", "achieved": line["value"], "peak": hbm, "unit": "GB/s",
-                        "frac": line["value"] / hbm, "peak_source": peak_kind}
+        sub = {"workload": "27-point stencil 128^3 n=2097152 nnz=55742968 (C3's matrix), FP64 SpMV",
+               "value": b / ms / 1e6, "unit": "GB/s", "ms_per_step": ms, "max_rel_err": err,
+               "plain_csr": {"value": b / ms_plain / 1e6, "ms_per_step": ms_plain},
+               "speedup_vs_plain_csr": ms_plain / ms, "format": KIND_NAMES[cfg["kind"]],
+               "C": cfg["C"], "sigma": cfg["sigma"], "tpr": cfg["tpr"],
+               "roofline": roofline(b / ms / 1e6)}
+    line = {"metric": f"{args.workload} GB/s (algorithmic bytes) vs B200 HBM roofline",
+            "n_gpus": 1, "warmup": max(args.warmup, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "data": "synthetic", **sub}
     emit(line, args)
     return 0
 
@@ -610,7 +765,8 @@ def emit(line, args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c3spmv", "c4"],
-                    help="c2 (default, the headline) or one of the other configurations")
+                    help="c2 (default: the headline line, with c1 / c3 / c4 inside it) or one "
+                         "configuration alone")
     ap.add_argument("--k", type=int, default=32, help="right-hand sides for --workload c3")
     ap.add_argument("--storage", default="native", choices=["native", "fp32", "bf16"])
     ap.add_argument("--gpus", type=int, default=1)
@@ -618,6 +774,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--no-configs", action="store_true", help="skip the c1 / c3 / c4 configurations")
     ap.add_argument("--log", default=None, help="append the result line to this JSON-lines file")
     ap.add_argument("--soak-seconds", type=float, default=0.5,
                     help="untimed load before the timed region, so the clock samples see the GPU busy")

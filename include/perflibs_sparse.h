@@ -8,10 +8,12 @@
  * kept identical so that existing callers recompile and relink unchanged;
  * each prototype cites the reference declaration it replaces.
  *
- * Not provided (outside the execute path): CSC/COO/supernodal creation,
- * sparse vectors, SpAdd, SpElMM, SDDMM, SpSV/SpSM, transposition and scaling
- * of a handle, and every complex (_c / _z) entry point. A caller that needs
- * them keeps linking the reference library for those symbols.
+ * Provided for input: CSR, BSR, COO and CSC creation (COO and CSC are
+ * converted to CSR on the device), dense, null and identity handles.
+ * Not provided (outside the execute path): supernodal creation, sparse
+ * vectors, SpAdd, SpElMM, SDDMM, SpSV/SpSM, transposition and scaling of a
+ * handle, and every complex (_c / _z) entry point. A caller that needs them
+ * keeps linking the reference library for those symbols.
  */
 #ifndef PERFLIBS_SPARSE_H
 #define PERFLIBS_SPARSE_H

@@ -329,6 +329,63 @@ class RefMatrix:
             raise RuntimeError(f"reference create_csc failed: {st}")
         return RefMatrix(h)
 
+    @staticmethod
+    def bsr(layout, m, n, bs, row_ptr, col, vals):
+        L = ref()
+        h = C.c_void_p()
+        row_ptr = np.ascontiguousarray(row_ptr, np.int32)
+        col = np.ascontiguousarray(col, np.int32)
+        vals = np.ascontiguousarray(vals, np.float64)
+        st = L.perflibs_spmat_create_bsr_d(C.byref(h), layout, m, n, bs, _p(row_ptr), _p(col), _p(vals), 0)
+        if st != 0:
+            raise RuntimeError(f"reference create_bsr failed: {st}")
+        return RefMatrix(h)
+
+    @staticmethod
+    def dense(M: np.ndarray):
+        """A row-major dense handle (the reference copies the values)."""
+        L = ref()
+        h = C.c_void_p()
+        M = np.ascontiguousarray(M, np.float64)
+        rows, cols = M.shape
+        st = L.perflibs_spmat_create_dense_d(C.byref(h), 91, rows, cols, cols, _p(M), 0)
+        if st != 0:
+            raise RuntimeError(f"reference create_dense failed: {st}")
+        return RefMatrix(h)
+
+    def export_dense(self):
+        """Row-major values of a dense handle (the reference's export_dense)."""
+        L = ref()
+        rows, cols = C.c_int32(), C.c_int32()
+        vv = C.c_void_p()
+        st = L.perflibs_spmat_export_dense_d(self.h, 91, C.byref(rows), C.byref(cols), C.byref(vv))
+        if st != 0:
+            raise RuntimeError(f"reference export_dense failed: {st}")
+        cnt = rows.value * cols.value
+        out = np.ctypeslib.as_array(C.cast(vv, C.POINTER(C.c_double)), (max(cnt, 1),))[:cnt].copy()
+        L.free_ptr(vv)
+        return out.reshape(rows.value, cols.value)
+
+    def spmm(self, m, B, alpha=1.0, beta=0.0, C0=None):
+        """C = alpha * A * B + beta * C0 through the reference's own
+        perflibs_spmm_exec_d (NOTRANS, NOTRANS): B a dense row-major handle,
+        C a null handle when C0 is None (the reference materialises it) or a
+        dense copy of C0. Returns C as an m x k FP64 array."""
+        L = ref()
+        Bh = RefMatrix.dense(B)
+        k = B.shape[1]
+        if C0 is None:
+            Ch = RefMatrix(C.c_void_p(L.perflibs_spmat_create_null(m, k)))
+        else:
+            Ch = RefMatrix.dense(C0)
+        st = L.perflibs_spmm_exec_d(300, 300, alpha, self.h, Bh.h, beta, Ch.h)
+        if st != 0:
+            raise RuntimeError(f"reference spmm_exec failed: {st}")
+        out = Ch.export_dense()
+        Bh.destroy()
+        Ch.destroy()
+        return out
+
     def export_csr(self, m, index_base=0):
         """The reference's own export (it converts the handle to CSR first)."""
         L = ref()

@@ -607,9 +607,42 @@ static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchElems];
 static __device__ int32_t g_noalloc_done[kNoAllocSlots];  // zero at load
 
 namespace {
+// The arrays' device addresses, per device, with the context they were
+// looked up in: after cudaDeviceReset the device's primary context (and the
+// module holding the arrays) is created anew, so a lookup is only reused
+// while the same context is current.
+struct NoAllocAddrs {
+  void *ctx = nullptr;
+  void *part = nullptr;
+  void *count = nullptr;
+};
 std::mutex g_noalloc_mu;
-void *g_noalloc_part[64] = {};
-void *g_noalloc_count[64] = {};
+NoAllocAddrs g_noalloc[64];
+
+// The driver's cuCtxGetCurrent, reached through the runtime (no link to the
+// driver library); null if the driver does not offer it.
+using CtxGetCurrentFn = int (*)(void **);
+CtxGetCurrentFn ctx_get_current() {
+  static const CtxGetCurrentFn fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (CtxGetCurrentFn) nullptr;
+    return reinterpret_cast<CtxGetCurrentFn>(p);
+  }();
+  return fn;
+}
+
+// The context current on this thread (the caller's DeviceGuard made the
+// device current, which binds its primary context); null if unknown.
+void *current_context() {
+  void *ctx = nullptr;
+  const CtxGetCurrentFn fn = ctx_get_current();
+  if (!fn || fn(&ctx) != 0)
+    return nullptr;
+  return ctx;
+}
 
 void *symbol_address(const void *sym, const char *what) {
   void *p = nullptr;
@@ -623,10 +656,12 @@ void *symbol_address(const void *sym, const char *what) {
 
 // The SELL SpMV with its slices' partial sums and counts in the fixed
 // arrays. Their device addresses come from cudaGetSymbolAddress (in host code
-// the arrays' names are only host-side stand-ins), once per device, with that
-// device current (the caller's DeviceGuard makes it current). Every slot a
-// call reads was written earlier in the same call, and the counts return to
-// zero by the end of every launch, so nothing needs clearing between calls.
+// the arrays' names are only host-side stand-ins), once per device and
+// context, with that device current (the caller's DeviceGuard makes it
+// current); a call that finds another context current (the device was reset
+// since) looks them up again. Every slot a call reads was written earlier in
+// the same call, and the counts return to zero by the end of every launch,
+// so nothing needs clearing between calls.
 void spmv_sell_noalloc(const SellDev &s, const double *x, double *y, double alpha, double beta,
                        int device, cudaStream_t st) {
   if (s.nC == 0)
@@ -640,14 +675,15 @@ void spmv_sell_noalloc(const SellDev &s, const double *x, double *y, double alph
   SellWork w = whole_work(s);
   {
     std::lock_guard<std::mutex> g(g_noalloc_mu);
-    void *&part = g_noalloc_part[device & 63];
-    void *&count = g_noalloc_count[device & 63];
-    if (!part) {
-      part = symbol_address(g_noalloc_scratch, "scratch");
-      count = symbol_address(g_noalloc_done, "counts");
+    NoAllocAddrs &a = g_noalloc[device & 63];
+    void *ctx = current_context();
+    if (!a.part || !ctx || ctx != a.ctx) {
+      a.part = symbol_address(g_noalloc_scratch, "scratch");
+      a.count = symbol_address(g_noalloc_done, "counts");
+      a.ctx = ctx;
     }
-    w.part = part;
-    w.done = static_cast<int32_t *>(count);
+    w.part = a.part;
+    w.done = static_cast<int32_t *>(a.count);
   }
   run_sell<double>(s, w, x, y, alpha, beta, st);
 }

@@ -145,7 +145,8 @@ double time_config(Mat *A, const SpmvConfig &cfg, int reps) {
   return t.empty() ? 0.0 : t[t.size() / 2];
 }
 
-// The candidate list (also the class list of the learned selector).
+// The candidate list (also the class list of the learned selector). Sorting
+// windows go up to 8192 rows; 0 is the unsorted layout.
 std::vector<SpmvConfig> tune_candidates(const Mat *A) {
   std::vector<SpmvConfig> out;
   for (int tpr : {1, 2, 4, 8, 16, 32}) {
@@ -161,7 +162,7 @@ std::vector<SpmvConfig> tune_candidates(const Mat *A) {
     out.push_back(c);
   }
   for (int C : {8, 16, 32})
-    for (int sigma : {0, 32, 256, 1024, 4096, 16384}) {
+    for (int sigma : {0, 32, 256, 1024, 4096, 8192}) {
       if (sigma != 0 && (sigma < C || sigma % C != 0))
         continue;
       SpmvConfig c;

@@ -72,3 +72,35 @@ def rel_err_rows(y, y_ref, scale):
     den = np.maximum(np.abs(y_ref), scale)
     den = np.where(den == 0, 1.0, den)
     return np.abs(y - y_ref) / den
+
+
+@pytest.fixture(scope="session")
+def ref_spmm():
+    return np.load(os.path.join(GOLDEN, "ref_spmm.npz"))
+
+
+def spmm_case_csr(f, name):
+    """A fixture case as 0-based CSR (BSR cases through the oracle's
+    bsr2csr, which keeps the reference's CSR view: explicit zeros dropped)."""
+    import oracle
+
+    if int(f[f"{name}/kind"]) == 1:
+        return oracle.bsr2csr(f[f"{name}/row_ptr"], f[f"{name}/col"], f[f"{name}/vals"],
+                              int(f[f"{name}/bs"]), int(f[f"{name}/layout"]))
+    base = int(f[f"{name}/base"])
+    return ((f[f"{name}/row_ptr"] - base).astype(np.int32), (f[f"{name}/col"] - base).astype(np.int32),
+            f[f"{name}/vals"])
+
+
+def spmm_row_err(got, ref, rp, col, vals, B, alpha, beta=0.0, C0=None):
+    """Per-row scaled error of an SpMM result: |got - ref| over
+    max(|ref|, |alpha| sum_j |a_ij| |B_j| + |beta| |C0|), elementwise."""
+    import oracle
+
+    k = B.shape[1]
+    scale = abs(alpha) * oracle.csr_spmm(rp, col, np.abs(vals), np.abs(B), k)
+    if C0 is not None:
+        scale = scale + abs(beta) * np.abs(C0)
+    den = np.maximum(np.abs(ref), scale)
+    den = np.where(den == 0, 1.0, den)
+    return float((np.abs(got - ref) / den).max())

@@ -13,6 +13,12 @@ Outputs:
   seeded inputs: SELL-C-sigma layouts from its csr2scs + gen_data_vectors
   (including C = 32, which the reference builds but never executes), and
   FP64 CSR / SELL SpMV results from its exec kernels.
+* ``ref_spmm.npz`` — C = alpha*A*B (+ beta*C0) from the reference's own
+  perflibs_spmm_exec_d on small seeded CSR and BSR matrices, k in
+  {4, 8, 32, 128}: k = 4 takes its repeated-SpMV route
+  (src/matmul.cpp:26-28,42-89), larger k its row-wise blocked loop
+  (src/compressed_sparse_rows.cpp:1699-1764), BSR its CSR view
+  (src/matmul.cpp:616-631).
 
 The GPU box never runs this script; tests read the fixtures.
 """
@@ -120,8 +126,67 @@ def small_cases():
     return out
 
 
+def spmm_cases():
+    """Seeded small SpMM inputs: (name, kind, dict of arrays, ks)."""
+    rng = np.random.default_rng(4321)
+    out = []
+    m, n, rp, c, v = W.stencil_27pt(5, seed=5)
+    out.append(("st27_5", "csr", dict(m=m, n=n, row_ptr=rp, col=c, vals=v, base=0), (4, 8, 32, 128)))
+    rp, c, v = W.random_csr(160, 220, 24, rng, empty_frac=0.15)
+    out.append(("rand160", "csr", dict(m=160, n=220, row_ptr=rp, col=c, vals=v, base=0), (4, 8, 32, 128)))
+    rp, c, v = W.random_csr(90, 70, 12, rng, base=1, empty_frac=0.2)
+    out.append(("rand90_b1", "csr", dict(m=90, n=70, row_ptr=rp, col=c, vals=v, base=1), (4, 8)))
+    for bs, mb, nb in ((4, 12, 15), (8, 7, 9)):
+        for layout in (90, 91):
+            rpb = np.zeros(mb + 1, np.int32)
+            cols = []
+            for i in range(mb):
+                cc = np.sort(rng.choice(nb, int(rng.integers(0, 5)), replace=False))
+                cols.append(cc)
+                rpb[i + 1] = rpb[i] + len(cc)
+            colb = np.concatenate(cols).astype(np.int32)
+            vb = rng.uniform(-1, 1, len(colb) * bs * bs)
+            vb[rng.random(len(vb)) < 0.25] = 0.0  # explicit zeros inside blocks
+            name = f"bsr{bs}_{'col' if layout == 90 else 'row'}"
+            out.append((name, "bsr", dict(m=mb * bs, n=nb * bs, bs=bs, layout=layout, row_ptr=rpb,
+                                          col=colb, vals=vb), (4, 8, 32)))
+    return out
+
+
+def spmm_fixtures():
+    """Reference SpMM outputs: per case and k, alpha = 1.5 with a null C, and
+    (k in {4, 32}) alpha = 0.75, beta = -0.5 with a dense C0."""
+    rng = np.random.default_rng(8765)
+    arrays = {}
+    for name, kind, d, ks in spmm_cases():
+        m, n = d["m"], d["n"]
+        kmax = max(ks)
+        B = rng.uniform(-1, 1, (n, kmax))
+        C0 = rng.uniform(-1, 1, (m, kmax))
+        for key, val in d.items():
+            arrays[f"{name}/{key}"] = np.asarray(val)
+        arrays[f"{name}/kind"] = np.array(0 if kind == "csr" else 1)
+        arrays[f"{name}/B"] = B
+        arrays[f"{name}/C0"] = C0
+        arrays[f"{name}/ks"] = np.array(ks, np.int32)
+        if kind == "csr":
+            A = oracle.RefMatrix.csr(m, n, d["row_ptr"], d["col"], d["vals"])
+        else:
+            A = oracle.RefMatrix.bsr(d["layout"], m, n, d["bs"], d["row_ptr"], d["col"], d["vals"])
+        for k in ks:
+            Bk = np.ascontiguousarray(B[:, :k])
+            arrays[f"{name}/C_k{k}"] = A.spmm(m, Bk, alpha=1.5)
+            if k in (4, 32):
+                C0k = np.ascontiguousarray(C0[:, :k])
+                arrays[f"{name}/Cb_k{k}"] = A.spmm(m, Bk, alpha=0.75, beta=-0.5, C0=C0k)
+        A.destroy()
+    np.savez_compressed(os.path.join(HERE, "ref_spmm.npz"), **arrays)
+    return len(arrays)
+
+
 def main():
     assert oracle.ref_available(), "build the reference oracle first: make -C oracle ref"
+    print("wrote", spmm_fixtures(), "SpMM arrays")
     with open(os.path.join(HERE, "reference_kats.json"), "w") as f:
         json.dump(KATS, f, indent=1)
     arrays = {}

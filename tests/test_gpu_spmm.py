@@ -7,6 +7,7 @@ import pytest
 import oracle
 import perf_libs_sparse_b200 as pls
 from perf_libs_sparse_b200 import workloads as W
+from tests.conftest import rel_err_rows
 
 pytestmark = pytest.mark.gpu
 
@@ -23,6 +24,14 @@ def scaled_err(got, ref, rp, c, v, B, alpha, beta, C0):
     den = np.maximum(np.abs(ref), sc)
     den[den == 0] = 1
     return (np.abs(got - ref) / den).max()
+
+
+def dense_scaled_err(got, ref, scale):
+    """Elementwise |got - ref| / max(|ref|, scale): the per-element form of
+    the scaled metric, for products checked against numpy."""
+    den = np.maximum(np.abs(ref), scale)
+    den = np.where(den == 0, 1.0, den)
+    return float((np.abs(got - ref) / den).max())
 
 
 def test_kat_matmul_variants(kats):
@@ -112,8 +121,9 @@ def test_identity_and_dense_products_vs_numpy(ta, tb):
     B = pls.SpMat.dense(pls.ROW_MAJOR, Bd.shape[0], Bd.shape[1], Bd.shape[1], Bd.reshape(-1))
     Cm = pls.SpMat.dense(pls.COL_MAJOR, m, n, m, C0.T.reshape(-1))
     assert pls.spmm_exec(ta, tb, 0.75, A, B, -0.5, Cm) == 0
-    np.testing.assert_allclose(Cm.export_dense(), 0.75 * T(Ad, ta) @ T(Bd, tb) - 0.5 * C0,
-                               atol=1e-12)
+    ref = 0.75 * T(Ad, ta) @ T(Bd, tb) - 0.5 * C0
+    scale = 0.75 * np.abs(T(Ad, ta)) @ np.abs(T(Bd, tb)) + 0.5 * np.abs(C0)
+    assert dense_scaled_err(Cm.export_dense(), ref, scale) <= 1e-12
     # identity x sparse (CSR, then BSR) and sparse x identity, beta != 0
     rp, c, v = W.random_csr(6, 6, 4, rng)
     S = _dense_of(6, 6, rp, c, v)
@@ -122,13 +132,14 @@ def test_identity_and_dense_products_vs_numpy(ta, tb):
                pls.SpMat.bsr(pls.ROW_MAJOR, 6, 6, 2, *oracle.csr2bsr(rp, c, v, 6, 6, 2, pls.ROW_MAJOR))):
         Cm = pls.SpMat.dense(pls.ROW_MAJOR, 6, 6, 6, C1.reshape(-1))
         assert pls.spmm_exec(ta, tb, 1.25, pls.SpMat.identity(6), Sm, 0.5, Cm) == 0
-        np.testing.assert_allclose(Cm.export_dense(), 1.25 * T(S, tb) + 0.5 * C1, atol=1e-12)
+        assert dense_scaled_err(Cm.export_dense(), 1.25 * T(S, tb) + 0.5 * C1,
+                                1.25 * np.abs(T(S, tb)) + 0.5 * np.abs(C1)) <= 1e-12
         Cm = pls.SpMat.dense(pls.ROW_MAJOR, 6, 6, 6, C1.reshape(-1))
         assert pls.spmm_exec(ta, tb, -2.0, Sm, pls.SpMat.identity(6), 0.0, Cm) == 0
-        np.testing.assert_allclose(Cm.export_dense(), -2.0 * T(S, ta), atol=1e-12)
+        assert dense_scaled_err(Cm.export_dense(), -2.0 * T(S, ta), 2.0 * np.abs(T(S, ta))) <= 1e-12
     Cm = pls.SpMat.dense(pls.ROW_MAJOR, 6, 6, 6, C1.reshape(-1))
     assert pls.spmm_exec(ta, tb, 3.0, pls.SpMat.identity(6), pls.SpMat.identity(6), 1.0, Cm) == 0
-    np.testing.assert_allclose(Cm.export_dense(), 3.0 * np.eye(6) + C1, atol=1e-12)
+    assert dense_scaled_err(Cm.export_dense(), 3.0 * np.eye(6) + C1, 3.0 * np.eye(6) + np.abs(C1)) <= 1e-12
 
 
 def test_kat_matrix_kernel_ops(kats):
@@ -198,7 +209,7 @@ def test_repeated_exec_with_beta_zero_overwrites():
     for _ in range(3):
         assert pls.spmm_exec(pls.OPERATION_NOTRANS, pls.OPERATION_NOTRANS, 1.0, A, B, 0.0, Cm) == 0
     ref = spmm_ref(rp, c, v, Bd, 1.0, 0.0, None)
-    np.testing.assert_allclose(Cm.export_dense(), ref, rtol=1e-12, atol=1e-12)
+    assert scaled_err(Cm.export_dense(), ref, rp, c, v, Bd, 1.0, 0.0, None) <= 1e-12
 
 
 def test_bsr_spmm_vs_oracle():
@@ -215,10 +226,11 @@ def test_bsr_spmm_vs_oracle():
                 Cm = pls.SpMat.null(m, k)
                 assert pls.spmm_exec(pls.OPERATION_NOTRANS, pls.OPERATION_NOTRANS, 1.0, A, B, 0.0, Cm) == 0
                 ref = spmm_ref(rp, c, v, Bd, 1.0, 0.0, None)
-                np.testing.assert_allclose(Cm.export_dense(), ref, rtol=1e-12, atol=1e-12)
+                assert scaled_err(Cm.export_dense(), ref, rp, c, v, Bd, 1.0, 0.0, None) <= 1e-12, (bs, layout, k)
                 # BSR SpMV
                 x = rng.uniform(-1, 1, n)
-                np.testing.assert_allclose(A.spmv(x), oracle.csr_spmv(rp, c, v, x), rtol=1e-12, atol=1e-12)
+                y_ref = oracle.csr_spmv(rp, c, v, x)
+                assert rel_err_rows(A.spmv(x), y_ref, oracle.csr_absdot(rp, c, v, x)).max() <= 1e-12
 
 
 @pytest.mark.parametrize("storage,tol", [(pls.STORAGE_NATIVE, 1e-12), (pls.STORAGE_FP32, 1e-5),
@@ -250,7 +262,8 @@ def test_device_pointer_spmm():
     Ct = torch.empty((1000, 32), dtype=torch.float64, device="cuda")
     A.spmm_dev(Bt.data_ptr(), 32, 32, Ct.data_ptr(), 32, 1.0, 0.0, torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()
-    np.testing.assert_allclose(Ct.cpu().numpy(), spmm_ref(rp, c, v, Bd, 1.0, 0.0, None), rtol=1e-12, atol=1e-12)
+    ref = spmm_ref(rp, c, v, Bd, 1.0, 0.0, None)
+    assert scaled_err(Ct.cpu().numpy(), ref, rp, c, v, Bd, 1.0, 0.0, None) <= 1e-12
 
 
 @pytest.mark.parametrize("dt", [np.float64, np.float32])

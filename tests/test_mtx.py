@@ -109,3 +109,54 @@ def test_driver_runs_on_laplacian(tmp_path):
     assert lines[0] == f"A: {m} x {n} nnz={len(ent)}"
     assert lines[1] == f"B: {n} x 1024" and lines[2] == f"C: {m} x 1024"
     assert re.fullmatch(r"iters=10 total_s=[0-9.]+ avg_s=[0-9.]+", lines[3])
+
+
+@pytest.mark.gpu
+def test_reference_driver_runs_on_gpu(tmp_path):
+    """The reference's own benchmark driver (bench/pl_bench_sparse_x_dense.c,
+    unchanged, compiled against include/perflibs_sparse.h and linked to this
+    library by `make -C oracle driver-check`) runs on the GPU: it reads a
+    Matrix Market file, fills B (n x 1024) from srand(1) / rand(), and runs
+    spmm_optimize + 10 spmm_exec_d. A preloaded tap (tests/ref_driver_tap.c)
+    writes the C of each exec; the last one must equal the FP64 oracle's
+    A*B within 1e-12 (scaled per element), with B rebuilt here from the same
+    C library's rand()."""
+    import ctypes
+
+    import oracle
+    from perf_libs_sparse_b200 import workloads as W
+    from tests.conftest import spmm_row_err
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = os.path.join(root, "oracle", "_build", "ref_driver_on_b200")
+    if not os.path.exists(exe):
+        pytest.skip("the reference driver was not built (make -C oracle driver-check)")
+    tap = tmp_path / "tap.so"
+    subprocess.run(["gcc", "-shared", "-fPIC", "-O2", f"-I{os.path.join(root, 'include')}",
+                    os.path.join(root, "tests", "ref_driver_tap.c"), "-o", str(tap), "-ldl"], check=True)
+    rng = np.random.default_rng(31)
+    m, n = 300, 260
+    rp, c, v = W.random_csr(m, n, 20, rng, empty_frac=0.1)
+    path = tmp_path / "r.mtx"
+    ent = [(i + 1, int(c[p]) + 1, f"{v[p]:.17g}") for i in range(m) for p in range(rp[i], rp[i + 1])]
+    _write(path, "%%MatrixMarket matrix coordinate real general", f"{m} {n} {len(ent)}", ent)
+    out_c = tmp_path / "c.bin"
+    env = dict(os.environ, LD_PRELOAD=str(tap), PERFLIBS_TAP_C=str(out_c),
+               LD_LIBRARY_PATH=os.path.dirname(pls.__file__) + os.pathsep + os.environ.get("LD_LIBRARY_PATH", ""))
+    r = subprocess.run([exe, str(path)], capture_output=True, text=True, timeout=300, env=env)
+    assert r.returncode == 0, r.stdout + r.stderr
+    lines = r.stdout.strip().splitlines()
+    assert lines[0] == f"A: {m} x {n} nnz={len(ent)}"
+    assert lines[2] == f"C: {m} x 1024"
+    assert re.fullmatch(r"iters=10 total_s=[0-9.]+ avg_s=[0-9.]+", lines[3])
+    raw = out_c.read_bytes()
+    mm, nn = np.frombuffer(raw[:8], np.int32)
+    assert (mm, nn) == (m, 1024)
+    got = np.frombuffer(raw[8:], np.float64).reshape(m, 1024)
+    libc = ctypes.CDLL(None)
+    libc.rand.restype = ctypes.c_int
+    libc.srand(1)
+    rand_max = 2147483647.0  # glibc RAND_MAX
+    B = np.array([2.0 * libc.rand() / rand_max - 1.0 for _ in range(n * 1024)]).reshape(n, 1024)
+    ref = oracle.csr_spmm(rp, c, v, B, 1024)
+    assert spmm_row_err(got, ref, rp, c, v, B, 1.0) <= 1e-12

@@ -192,3 +192,51 @@ def test_coo_csc_restatement_matches_reference():
         np.testing.assert_array_equal(o_rp, t_rp)
         np.testing.assert_array_equal(o_c, t_c)
         np.testing.assert_array_equal(np.sort(o_v), np.sort(t_v))
+
+
+def test_spmm_port_matches_reference_fixtures(ref_spmm):
+    """The restated SpMM (oracle.csr_spmm, the blocked row-wise loop of
+    src/compressed_sparse_rows.cpp:1699-1764) against the reference's own
+    perflibs_spmm_exec_d outputs (tests/golden/ref_spmm.npz): CSR with index
+    base 0 and 1, BSR bs 4 and 8 in both block layouts through its CSR view,
+    k in {4, 8, 32, 128} (k = 4 is the reference's repeated-SpMV route), with
+    and without beta. Per-row scaled error <= 1e-12: summation order is the
+    only freedom."""
+    from tests.conftest import spmm_case_csr, spmm_row_err
+
+    f = ref_spmm
+    names = sorted({k.split("/")[0] for k in f.files})
+    assert len(names) == 7
+    for name in names:
+        rp, col, vals = spmm_case_csr(f, name)
+        B, C0 = f[f"{name}/B"], f[f"{name}/C0"]
+        for k in (int(t) for t in f[f"{name}/ks"]):
+            Bk = np.ascontiguousarray(B[:, :k])
+            got = oracle.csr_spmm(rp, col, vals, Bk, k, alpha=1.5)
+            assert spmm_row_err(got, f[f"{name}/C_k{k}"], rp, col, vals, Bk, 1.5) <= 1e-12, (name, k)
+            if k >= 8:  # the blocked loop: the same order as the reference, bit for bit
+                np.testing.assert_array_equal(got, f[f"{name}/C_k{k}"], err_msg=f"{name} k={k}")
+            if f"{name}/Cb_k{k}" in f.files:
+                C0k = np.ascontiguousarray(C0[:, :k])
+                got = oracle.csr_spmm(rp, col, vals, Bk, k, Cmat=C0k, alpha=0.75, beta=-0.5)
+                assert spmm_row_err(got, f[f"{name}/Cb_k{k}"], rp, col, vals, Bk, 0.75, -0.5, C0k) <= 1e-12, (name, k)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference library not built here")
+def test_spmm_port_matches_reference_live():
+    """Fresh random CSR SpMMs, the port against the reference library run
+    here, k across the repeated-SpMV threshold."""
+    from perf_libs_sparse_b200 import workloads as W
+    from tests.conftest import spmm_row_err
+
+    rng = np.random.default_rng(77)
+    for t in range(12):
+        m, n = int(rng.integers(1, 200)), int(rng.integers(1, 200))
+        rp, c, v = W.random_csr(m, n, min(n, 30), rng)
+        k = int(rng.choice([1, 3, 4, 5, 8, 17, 64]))
+        B = rng.uniform(-1, 1, (n, k))
+        A = oracle.RefMatrix.csr(m, n, rp, c, v)
+        theirs = A.spmm(m, B, alpha=-1.25)
+        A.destroy()
+        ours = oracle.csr_spmm(rp, c, v, B, k, alpha=-1.25)
+        assert spmm_row_err(ours, theirs, rp, c, v, B, -1.25) <= 1e-12, (m, n, k)
