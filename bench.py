@@ -408,6 +408,8 @@ def c3_config(args, timer, sp, arms):
         A.set_storage({"native": pls.STORAGE_NATIVE, "fp32": pls.STORAGE_FP32,
                        "bf16": pls.STORAGE_BF16}[storage])
         A.set_stream(sp)
+        if getattr(args, "spmm_path", None) is not None:
+            A.set_spmm_path(args.spmm_path)
         assert A.optimize() == 0
         Bd = torch.tensor(B, dtype=tdt, device="cuda")
         Cd = torch.zeros((m, k), dtype=tdt, device="cuda")
@@ -769,6 +771,8 @@ def main():
                          "configuration alone")
     ap.add_argument("--k", type=int, default=32, help="right-hand sides for --workload c3")
     ap.add_argument("--storage", default="native", choices=["native", "fp32", "bf16"])
+    ap.add_argument("--spmm-path", type=int, default=None,
+                    help="--workload c3: force one SpMM kernel (perflibs_b200_spmat_set_spmm_path)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)

@@ -46,9 +46,10 @@ perflibs_status_t perflibs_b200_spmv_exec_s_dev(
  * library holds until exit; a matrix that needs more returns
  * PERFLIBS_STATUS_INPUT_PARAMETER_ERROR with the sizes in the handle's
  * error message. The first call on a device looks the arrays' addresses up
- * (cudaGetSymbolAddress), so make that first call before any stream
- * capture. All calls share the arrays: calls that overlap on the GPU race,
- * so serialise them (one stream, or events between streams). */
+ * (cudaGetSymbolAddress), and so does the first call after the device's
+ * context was re-created (cudaDeviceReset); make that first call before any
+ * stream capture. All calls share the arrays: calls that overlap on the GPU
+ * race, so serialise them (one stream, or events between streams). */
 perflibs_status_t perflibs_b200_spmv_exec_d_noalloc(double alpha,
                                                     perflibs_spmat_t A,
                                                     const double *x,
@@ -141,11 +142,17 @@ perflibs_status_t perflibs_b200_spmat_exec_info(perflibs_spmat_t A,
  * its rows are sorted without duplicate columns, and B and C rows are
  * 16-byte vectors (any storage mode): each thread computes 4
  * consecutive rows and loads each row of B once per run of consecutive
- * diagonals. set_spmm_path overrides the choice: -1 measured choice
- * (default), 0 row-group kernel, 1 staged kernel whenever it applies, 2
- * row-group kernel with shared entries whenever the lane shape allows (at
- * least 4 lanes per row of C), 3 diagonal-form kernel whenever it
- * applies. */
+ * diagonals. Where the diagonal form applies, a second diagonal-form
+ * kernel is a candidate too, with B's rows staged in shared memory by
+ * tensor-map (TMA) copies: for diagonals in groups whose centres are evenly
+ * spaced (the planes of a 3-D stencil, the lines of a 2-D one) or in one
+ * band, each CTA walks a chain of tiles and copies one new window of B per
+ * tile; the staged (tiled) kernel is then not timed. set_spmm_path
+ * overrides the choice: -1 measured choice (default), 0 row-group kernel,
+ * 1 staged kernel whenever it applies, 2 row-group kernel with shared
+ * entries whenever the lane shape allows (at least 4 lanes per row of C),
+ * 3 diagonal-form kernel whenever it applies, 4 diagonal form with
+ * TMA-staged B whenever it applies (else 3 when that applies). */
 perflibs_status_t perflibs_b200_spmat_set_spmm_path(perflibs_spmat_t A, int32_t path);
 
 /* Host-buffer SpMV (perflibs_spmv_exec_{s,d}) in row bands: the kernels of
@@ -166,7 +173,8 @@ perflibs_status_t perflibs_b200_spmat_host_bands_used(perflibs_spmat_t A, int32_
  * were built: the staged kernel does not apply), the B rows staged per
  * column tile over all blocks and the copy runs; the path the last SpMM
  * took (1 staged, 0 row-group, 2 row-group with shared entries, 3
- * diagonal form, -1 none yet); and the two timings of the
+ * diagonal form, 4 diagonal form with TMA-staged B, -1 none yet); and the
+ * two timings of the
  * measured choice in milliseconds (0 when not measured). Any output may be
  * NULL. */
 perflibs_status_t perflibs_b200_spmat_spmm_info(perflibs_spmat_t A, int32_t *tile_rows,

@@ -1734,7 +1734,7 @@ void perflibs_spmat_print_err(perflibs_spmat_t A) {
 // ---------------------------------------------------------- extensions
 
 perflibs_status_t perflibs_b200_spmat_set_spmm_path(perflibs_spmat_t A, int32_t path) {
-  if (!A || path < -1 || path > 3)
+  if (!A || path < -1 || path > 4)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
   A->csr.tiles.forced = path;
   A->csr.tiles.choice_sig = -1;

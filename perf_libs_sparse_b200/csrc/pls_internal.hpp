@@ -21,6 +21,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
@@ -30,6 +31,8 @@
 #include <vector>
 
 #include <nvtx3/nvToolsExt.h>
+
+#include "dia_plan.hpp"
 
 #include "../../include/perflibs_b200.h"
 #include "../../include/perflibs_sparse.h"
@@ -280,17 +283,18 @@ struct TileDev {
   // Measured choice between the SpMM kernels for the call signature
   // `choice_sig` (k, ldb, value and API types): 0 row group 64-bit offsets,
   // 2 row group 32-bit, 3 row group with shared entries, 1 staged, 4
-  // diagonal form, -1 not measured; with the staged and the best row-group
-  // timing (ms).
+  // diagonal form, 5 diagonal form with TMA-staged B, -1 not measured; with
+  // the staged and the best row-group timing (ms).
   int64_t choice_sig = -1;
   int choice = -1;
   float ms_staged = 0.f, ms_rows = 0.f;
   // Path forced by perflibs_b200_spmat_set_spmm_path: -1 measured choice,
   // 0 row group, 1 staged (when it applies), 2 row group with shared entries
-  // (when the lane shape allows them), 3 diagonal form (when it applies).
+  // (when the lane shape allows them), 3 diagonal form (when it applies), 4
+  // diagonal form with TMA-staged B (when it applies, else 3 when that does).
   int forced = -1;
   // Path of the last SpMM: 1 staged, 0 row group, 2 row group with shared
-  // entries, 3 diagonal form.
+  // entries, 3 diagonal form, 4 diagonal form with TMA-staged B.
   int last_path = -1;
 };
 
@@ -299,20 +303,33 @@ struct TileDev {
 // diagonals c - r = offs[d] (ascending); vals holds, for every block of
 // kDiaRows rows and every diagonal, the block's kDiaRows values in the
 // kernels' value type (an absent entry is a reserved NaN bit pattern the
-// kernel skips). state: 0 not examined, 1 built, -1 unsuitable.
-constexpr int kDiaRows = 4;
-constexpr int kDiaMax = 32;
+// kernel skips). The blocks continue kDiaPadRows rows past the last row,
+// all absent, so that a copy of any kDiaPadRows rows starting at a row of
+// the matrix stays inside the buffer (kDiaRows, kDiaMax and kDiaPadRows are
+// in dia_plan.hpp). state: 0 not examined, 1 built, -1 unsuitable.
 struct DiaDev {
   int state = 0;
   int nd = 0;
   int32_t offs[kDiaMax] = {};
   DevBuf vals;
+  // Per block of kDiaRows rows (padded like vals): bit d set when every row
+  // of the block stores an entry on diagonal d.
+  DevBuf full;
   // What was examined: vals_version, type and buffer of the kernels' values
   // (a change of any of them means examining the matrix again).
   uint64_t version = 0;
   Vt vt = Vt::F64;
   const void *src = nullptr;
+  // Set (mapped host memory) by the TMA-staged kernel when a copy did not
+  // land within its wait limit; reported by the next call.
+  HostFlag err;
 };
+
+// Bounded waits of the kernels that stage through mbarriers: the poll limit
+// (2^22, about a second) and, for failure-path tests only, bytes an mbarrier
+// expects beyond what is copied (perflibs_b200_testing_stage_fault).
+extern std::atomic<int> g_stage_wait_limit;
+extern std::atomic<int> g_stage_shortfall;
 
 struct CsrDev {
   DevBuf row_ptr, col, vals;  // vals in the API type (authoritative)
@@ -535,6 +552,14 @@ bool spmm_tiled(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64_t ldc
 template <class X>
 bool spmm_dia(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64_t ldc, int k,
               X alpha, X beta, cudaStream_t s, bool launch = true);
+// The diagonal form with B's rows staged in shared memory by tensor-map
+// copies, for diagonal forms whose diagonals fall into groups with evenly
+// spaced centres (planes of a 3-D stencil, lines of a 2-D one) or into one
+// band; false (nothing launched) when it does not apply. With launch =
+// false it only says whether it applies (building the diagonal form).
+template <class X>
+bool spmm_dia_tma(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64_t ldc, int k,
+                  X alpha, X beta, cudaStream_t s, bool launch = true);
 template <class X>
 void spmm_bsr(const BsrDev &b, const X *B, int64_t ldb, X *C, int64_t ldc,
               int k, X alpha, X beta, cudaStream_t s);

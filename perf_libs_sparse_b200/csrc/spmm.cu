@@ -170,7 +170,9 @@ static bool spmm_rows(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
 // a scratch C (beta = 0, CUDA events, one warm-up and two timed runs) and
 // keeps the fastest; later calls use the kept one. choice: 0 row group
 // 64-bit, 2 row group 32-bit, 3 row group with shared entries (32-bit
-// offsets when they fit), 1 staged, 4 diagonal form (spmm_dia.cu).
+// offsets when they fit), 1 staged, 4 diagonal form, 5 diagonal form with
+// TMA-staged B (spmm_dia.cu). Where the diagonal form applies the staged
+// kernel is not timed: it stages the same rows of B less compactly.
 template <class X>
 void spmm_csr(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
               int64_t ldc, int k, X alpha, X beta, cudaStream_t s) {
@@ -193,6 +195,14 @@ void spmm_csr(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
     t.last_path = dia ? 3 : 0;
     return;
   }
+  if (t.forced == 4) {
+    const bool tma = spmm_dia_tma<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s, true);
+    const bool dia = !tma && spmm_dia<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s, true);
+    if (!tma && !dia)
+      spmm_rows<X>(c, m, B, ldb, C, ldc, k, alpha, beta, fits32, false, s);
+    t.last_path = tma ? 4 : dia ? 3 : 0;
+    return;
+  }
   if (t.forced == 1) {
     const bool staged = spmm_tiled<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s, true);
     if (!staged)
@@ -201,14 +211,15 @@ void spmm_csr(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
     return;
   }
   if (t.choice_sig != sig) {
-    const bool staged_ok = spmm_tiled<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s, false);
     const bool dia_ok = spmm_dia<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s, false);
+    const bool tma_ok = dia_ok && spmm_dia_tma<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s, false);
+    const bool staged_ok = !dia_ok && spmm_tiled<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s, false);
     const int vec_s = rows_vec<X>(c, m, B, ldb, C, ldc, k, true);
     const bool shared_ok = shared_entries_fit(
         rows_shape(k, vec_s, (double)c.nnz / std::max<int32_t>(m, 1)));
     t.choice = 0;
     t.ms_rows = t.ms_staged = 0.f;
-    if (staged_ok || fits32 || shared_ok || dia_ok) {
+    if (staged_ok || fits32 || shared_ok || dia_ok || tma_ok) {
       DevBuf scratch;
       scratch.reserve(sizeof(X) * (size_t)m * k);
       X *sc = scratch.as<X>();
@@ -258,8 +269,16 @@ void spmm_csr(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
       if (dia_ok) {
         const float msd =
             time2([&] { spmm_dia<X>(c, m, B, ldb, sc, (int64_t)k, k, X(1), X(0), s, true); });
-        if (msd < best)
+        if (msd < best) {
+          best = msd;
           t.choice = 4;
+        }
+      }
+      if (tma_ok) {
+        const float mst =
+            time2([&] { spmm_dia_tma<X>(c, m, B, ldb, sc, (int64_t)k, k, X(1), X(0), s, true); });
+        if (mst < best)
+          t.choice = 5;
       }
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
@@ -272,6 +291,10 @@ void spmm_csr(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
   }
   if (t.choice == 4 && spmm_dia<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s, true)) {
     t.last_path = 3;
+    return;
+  }
+  if (t.choice == 5 && spmm_dia_tma<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s, true)) {
+    t.last_path = 4;
     return;
   }
   t.last_path = spmm_rows<X>(c, m, B, ldb, C, ldc, k, alpha, beta,

@@ -36,12 +36,11 @@
 #include "common.cuh"
 #include "pls_internal.hpp"
 #include "spmm_rows.cuh"
+#include "tma.cuh"
 
 namespace pls {
 
 namespace {
-
-constexpr int kDiaRun = 3;  // diagonals per run (longer runs are split)
 
 // Reserved bit patterns for "no entry": signalling NaNs with a payload.
 constexpr unsigned long long kAbsentD = 0x7FF0DEAD00000001ull;
@@ -139,6 +138,27 @@ __global__ void k_dia_scatter(int32_t m, DiaOffs offs, const int32_t *__restrict
     atomicOr(flag, bad);
 }
 
+// One thread per block of kDiaRows rows (including the padding blocks): bit
+// d of full[block] is set when every row of the block stores an entry on
+// diagonal d.
+template <class V>
+__global__ void k_dia_full(int64_t nblocks, int nd, const V *__restrict__ dv,
+                           uint32_t *__restrict__ full) {
+  const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nblocks)
+    return;
+  uint32_t bits = 0;
+  for (int d = 0; d < nd; ++d) {
+    bool all = true;
+#pragma unroll
+    for (int i = 0; i < kDiaRows; ++i)
+      all = all && !dia_absent(dv[(b * nd + d) * kDiaRows + i]);
+    if (all)
+      bits |= 1u << d;
+  }
+  full[b] = bits;
+}
+
 // The kDiaRows values of one block of rows on one diagonal (8, 16 or 32
 // bytes, aligned to their size).
 template <class V>
@@ -157,11 +177,58 @@ __device__ __forceinline__ void ld_rows_vals(const V *p, V (&a)[kDiaRows]) {
   }
 }
 
+// One run of len consecutive diagonals for a thread's kDiaRows rows: B's
+// rows br0 + j, j = 0 .. kDiaRows + len - 2, at bp + j * ldb (columns of the
+// thread's vector); the values of the run's diagonal l at ab + l * kDiaRows.
+// INSIDE: len == kDiaRun and the rows all lie inside B, so the loads are
+// neither checked nor predicated (otherwise rows outside [0, n) read as
+// zeros). CHECK: absent entries are skipped (without it the block must store
+// every diagonal). Either way each stored entry is one fma in ascending
+// diagonal order.
+template <bool INSIDE, bool CHECK, class V, class X, class Acc, int VEC>
+__device__ __forceinline__ void dia_run(const X *bp, int64_t ldb, int64_t br0, int64_t n,
+                                        int len, const V *ab, Acc (&acc)[kDiaRows][VEC]) {
+  constexpr int RB = kDiaRows;
+  constexpr bool FAST = INSIDE;
+  X bv[RB + kDiaRun - 1][VEC];
+#pragma unroll
+  for (int j = 0; j < RB + kDiaRun - 1; ++j) {
+    if (FAST || (j < RB + len - 1 && br0 + j >= 0 && br0 + j < n)) {
+      ld_vec<X, VEC>(bp + j * ldb, bv[j]);
+    } else {
+#pragma unroll
+      for (int v = 0; v < VEC; ++v)
+        bv[j][v] = X(0);
+    }
+  }
+#pragma unroll
+  for (int l = 0; l < kDiaRun; ++l) {
+    if (FAST || l < len) {
+      V a[RB];
+      ld_rows_vals<V>(ab + l * RB, a);
+#pragma unroll
+      for (int i = 0; i < RB; ++i)
+        if (!CHECK || !dia_absent(a[i])) {
+          const Acc ai = to_acc<Acc>(a[i]);
+#pragma unroll
+          for (int v = 0; v < VEC; ++v)
+            acc[i][v] = fma(ai, to_acc<Acc>(bv[i + l][v]), acc[i][v]);
+        }
+    }
+  }
+}
+
 // Threads: (block of kDiaRows rows) x (TK column vectors of VEC); a thread
-// loops over C's columns in steps of TK * VEC.
-template <class V, class X, int VEC>
+// loops over C's columns in steps of TK * VEC. MASK (threads that make more
+// than one pass over the columns): the block's full-diagonal mask is loaded
+// first and blocks that store every diagonal skip the absent checks; with
+// one pass that load's latency costs more than the checks (C3, FP64: 0.233
+// against 0.331 ms at k = 8, 0.725 against 0.849 ms at k = 32; at k = 128,
+// two passes, 2.21 against 2.43 ms).
+template <class V, class X, int VEC, bool MASK>
 __global__ void __launch_bounds__(256, 4)  // 64 registers: 4 blocks per SM
     k_spmm_dia(int32_t m, int32_t n, int nd, DiaRuns runs, const V *__restrict__ dv,
+               const uint32_t *__restrict__ dfull, uint32_t full_mask,
                const X *__restrict__ B, int64_t ldb, X *__restrict__ C, int64_t ldc, int k,
                int lg_tk, X alpha, X beta, int beta_nz) {
   constexpr int RB = kDiaRows;
@@ -173,6 +240,7 @@ __global__ void __launch_bounds__(256, 4)  // 64 registers: 4 blocks per SM
   if (r0 >= m)
     return;
   const V *ab = dv + rb * nd * RB;
+  const bool full = MASK && (__ldg(dfull + rb) & full_mask) == full_mask;
   for (int kk = tk * VEC; kk < k; kk += VEC << lg_tk) {
     Acc acc[RB][VEC];
 #pragma unroll
@@ -181,33 +249,17 @@ __global__ void __launch_bounds__(256, 4)  // 64 registers: 4 blocks per SM
       for (int v = 0; v < VEC; ++v)
         acc[i][v] = Acc(0);
     for (int q = 0; q < runs.n; ++q) {
-      const int o0 = runs.o0[q], len = runs.len[q], d0 = runs.d0[q];
-      X bv[RB + kDiaRun - 1][VEC];
-#pragma unroll
-      for (int j = 0; j < RB + kDiaRun - 1; ++j) {
-        const int64_t br = r0 + o0 + j;
-        if (j < RB + len - 1 && br >= 0 && br < n) {
-          ld_vec<X, VEC>(B + br * ldb + kk, bv[j]);
-        } else {
-#pragma unroll
-          for (int v = 0; v < VEC; ++v)
-            bv[j][v] = X(0);
-        }
-      }
-#pragma unroll
-      for (int l = 0; l < kDiaRun; ++l) {
-        if (l < len) {
-          V a[RB];
-          ld_rows_vals<V>(ab + (int64_t)(d0 + l) * RB, a);
-#pragma unroll
-          for (int i = 0; i < RB; ++i)
-            if (!dia_absent(a[i])) {
-              const Acc ai = to_acc<Acc>(a[i]);
-#pragma unroll
-              for (int v = 0; v < VEC; ++v)
-                acc[i][v] = fma(ai, to_acc<Acc>(bv[i + l][v]), acc[i][v]);
-            }
-        }
+      const int o0 = runs.o0[q], len = runs.len[q];
+      const int64_t br0 = r0 + o0;
+      const X *bp = B + br0 * ldb + kk;
+      const V *aq = ab + runs.d0[q] * RB;
+      if (len == kDiaRun && br0 >= 0 && br0 + RB + kDiaRun - 2 < n) {
+        if (MASK && full)
+          dia_run<true, false, V, X, Acc, VEC>(bp, ldb, br0, n, len, aq, acc);
+        else
+          dia_run<true, true, V, X, Acc, VEC>(bp, ldb, br0, n, len, aq, acc);
+      } else {
+        dia_run<false, true, V, X, Acc, VEC>(bp, ldb, br0, n, len, aq, acc);
       }
     }
 #pragma unroll
@@ -240,6 +292,7 @@ void dia_build(CsrDev &c, int32_t m, cudaStream_t s) {
   DiaDev &d = c.dia;
   d.state = -1;
   d.vals.release();
+  d.full.release();
   DevBuf key;
   key.reserve(8);
   PLS_CUDA(cudaMemsetAsync(key.p, 0, 8, s));
@@ -273,8 +326,9 @@ void dia_build(CsrDev &c, int32_t m, cudaStream_t s) {
   o.nd = nd;
   for (int i = 0; i < nd; ++i)
     o.o[i] = (int32_t)offs[i];
-  const int64_t count = div_up(m, kDiaRows) * nd * kDiaRows;
-  d.vals.reserve(sizeof(V) * count);
+  const int64_t count = div_up((int64_t)m + kDiaPadRows, kDiaRows) * nd * kDiaRows;
+  // 16 bytes of slack: the staged kernel's copies end on a 16-byte boundary.
+  d.vals.reserve(sizeof(V) * count + 16);
   k_dia_fill<V><<<(unsigned)div_up(count, 256), 256, 0, s>>>(count, d.vals.as<V>());
   DevBuf flag;
   flag.reserve(4);
@@ -290,6 +344,11 @@ void dia_build(CsrDev &c, int32_t m, cudaStream_t s) {
     d.vals.release();
     return;
   }
+  const int64_t nblocks = div_up((int64_t)m + kDiaPadRows, kDiaRows);
+  d.full.reserve(sizeof(uint32_t) * nblocks + 16);  // slack as for vals
+  k_dia_full<V><<<(unsigned)div_up(nblocks, 256), 256, 0, s>>>(nblocks, nd, d.vals.as<V>(),
+                                                              d.full.as<uint32_t>());
+  PLS_LAUNCH_CHECK();
   d.nd = nd;
   for (int i = 0; i < nd; ++i)
     d.offs[i] = o.o[i];
@@ -320,10 +379,417 @@ void dia_launch(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64
   while ((1 << lg_tk) < cols && lg_tk < 5)
     ++lg_tk;
   const int64_t threads = div_up(m, kDiaRows) << lg_tk;
-  k_spmm_dia<V, X, VEC><<<(unsigned)div_up(threads, 256), 256, 0, s>>>(
-      m, c.ncols, d.nd, runs, d.vals.as<V>(), B, ldb, C, ldc, k, lg_tk, alpha, beta,
-      beta != X(0));
+  const uint32_t full_mask = d.nd >= 32 ? 0xffffffffu : (1u << d.nd) - 1u;
+  const bool passes = cols > (1 << lg_tk);
+  auto kern = passes ? k_spmm_dia<V, X, VEC, true> : k_spmm_dia<V, X, VEC, false>;
+  kern<<<(unsigned)div_up(threads, 256), 256, 0, s>>>(
+      m, c.ncols, d.nd, runs, d.vals.as<V>(), d.full.as<uint32_t>(), full_mask, B, ldb, C, ldc,
+      k, lg_tk, alpha, beta, beta != X(0));
   PLS_LAUNCH_CHECK();
+}
+
+
+// ------------------------------------------- diagonal form, B staged by TMA
+//
+// The kernel above reads B through L1 from L2: on the 27-point stencil each
+// run of 3 diagonals loads its 6 rows of B once per 4 rows of C, so every
+// row of B crosses from L2 about 13 times per SpMM. Here B's rows are staged
+// in shared memory by tensor-map (TMA) copies and each crosses about 3
+// times.
+//
+// Groups and windows. The sorted diagonal offsets fall into G groups with
+// centres c_g = c_0 + g P, P rows apart (G = 3 planes of a 3-D stencil,
+// P = the plane size; lines of a 2-D stencil), each within h of its centre.
+// A tile is L consecutive rows of C starting at R, and a KS-column slice of
+// B and C; for group g it needs B's rows [R + c_g - h, R + c_g + L + h),
+// the window PW(t + g) of the chain of tiles R = b + t P. Consecutive tiles
+// of a chain share windows, so a CTA walks a chain: at tile t it holds
+// PW(t) .. PW(t + G - 1) in G shared-memory slots, and as soon as group 0
+// is done with PW(t) it issues the copy of PW(t + G) into that slot, which
+// lands while groups 1 .. G - 1 compute. One group (a band) is a chain of
+// consecutive tiles (P = L) with two slots, the next tile's window loading
+// while the current one computes.
+//
+// Values. The tile's L x nd values (the diagonal form's blocks of 4 rows,
+// contiguous for consecutive rows) arrive by one 1-D bulk copy into one of
+// two slabs, the next tile's while the current one computes.
+//
+// Threads. 256 threads: NV column lanes of one 16-byte vector each
+// (KS = NV * VEC columns) x 256 / NV row groups of kDiaRows rows, so
+// L = 1024 / NV. Per run of consecutive diagonals a thread reads its 4 + run
+// - 1 window rows once from shared memory. Entries are added per row in
+// ascending offset, one fma each, with the epilogue alpha * acc + beta * C:
+// the order and arithmetic of k_spmm_dia, so the results are the same bits.
+//
+// Work items are (segment of Z tiles of one chain, column slice), column
+// slice fastest so that the slices of a tile run together and its values
+// come from L2 after the first. Waits are bounded; a wait that runs out
+// sets the mapped error flag, waits (bounded) for the CTA's copies in flight
+// and ends the CTA, leaving its part of C unwritten; the host reports it on
+// the next call.
+
+// All threads wait for `bar`'s phase `parity`; true when every thread saw
+// it complete within the limit.
+__device__ __forceinline__ bool cta_wait(uint64_t *bar, uint32_t parity, int limit) {
+  const bool ok = tma::bar_wait_bounded(bar, parity, limit);
+  return __syncthreads_and(ok) != 0;
+}
+
+// Shared-memory loads by 32-bit shared address (a constant part of the
+// address folds into the instruction's offset).
+__device__ __forceinline__ void lds16(uint32_t a, double (&v)[2]) {
+  asm("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v[0]), "=d"(v[1]) : "r"(a));
+}
+__device__ __forceinline__ void lds16(uint32_t a, float (&v)[4]) {
+  asm("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+      : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3])
+      : "r"(a));
+}
+// The RB values of a thread's rows on one diagonal (RB * sizeof(V) bytes,
+// aligned to their size).
+template <class V, int RB>
+__device__ __forceinline__ void lds_vals(uint32_t a, V (&v)[RB]) {
+  constexpr int bytes = RB * (int)sizeof(V);
+  if constexpr (bytes == 4) {
+    uint32_t u;
+    asm("ld.shared.b32 %0, [%1];" : "=r"(u) : "r"(a));
+    memcpy(v, &u, 4);
+  } else if constexpr (bytes == 8) {
+    uint32_t u[2];
+    asm("ld.shared.v2.b32 {%0, %1}, [%2];" : "=r"(u[0]), "=r"(u[1]) : "r"(a));
+    memcpy(v, u, 8);
+  } else {
+#pragma unroll
+    for (int h = 0; h < bytes / 16; ++h) {
+      uint32_t u[4];
+      asm("ld.shared.v4.b32 {%0, %1, %2, %3}, [%4];"
+          : "=r"(u[0]), "=r"(u[1]), "=r"(u[2]), "=r"(u[3])
+          : "r"(a + 16 * h));
+      memcpy(reinterpret_cast<char *>(v) + 16 * h, u, 16);
+    }
+  }
+}
+
+// The products of one run of len diagonals for a thread's RB rows: window
+// rows j = 0 .. RB + len - 2 at wa + j * ROW (shared addresses), values of
+// the run's diagonal l at va + l * kDiaRows * sizeof(V). CHECK: skip absent
+// entries.
+template <bool CHECK, int LEN, class V, class X, class Acc, int VEC, int ROW, int RB>
+__device__ __forceinline__ void dia_tma_run(uint32_t wa, uint32_t va, int len,
+                                            Acc (&acc)[RB][VEC]) {
+  X bv[RB + kDiaRun - 1][VEC];
+#pragma unroll
+  for (int j = 0; j < RB + kDiaRun - 1; ++j)
+    if (j < RB + (LEN ? LEN : len) - 1)
+      lds16(wa + j * ROW, bv[j]);
+#pragma unroll
+  for (int l = 0; l < kDiaRun; ++l) {
+    if (l < (LEN ? LEN : len)) {
+      V av[RB];
+      lds_vals<V, RB>(va + l * kDiaRows * (int)sizeof(V), av);
+#pragma unroll
+      for (int i = 0; i < RB; ++i)
+        if (!CHECK || !dia_absent(av[i])) {
+          const Acc ai = to_acc<Acc>(av[i]);
+#pragma unroll
+          for (int v = 0; v < VEC; ++v)
+            acc[i][v] = fma(ai, to_acc<Acc>(bv[i + l][v]), acc[i][v]);
+        }
+    }
+  }
+}
+
+// One group's runs for a thread's RB rows: the thread's first window row at
+// shared address wrow (rows of ROW bytes), its values of diagonal 0 at
+// vrow. Full runs of kDiaRun diagonals take the unpredicated body.
+template <bool CHECK, class V, class X, class Acc, int VEC, int ROW, int RB>
+__device__ __forceinline__ void dia_tma_group(const DiaTmaArgs &a, int g, uint32_t wrow,
+                                              uint32_t vrow, Acc (&acc)[RB][VEC]) {
+  for (int r = a.grp_run0[g]; r < a.grp_run0[g + 1]; ++r) {
+    const int len = a.run_len[r];
+    const uint32_t wa = wrow + (uint32_t)a.run_q0[r] * ROW;
+    const uint32_t va = vrow + (uint32_t)a.run_d0[r] * (kDiaRows * (int)sizeof(V));
+    if (len == kDiaRun)
+      dia_tma_run<CHECK, kDiaRun, V, X, Acc, VEC, ROW, RB>(wa, va, len, acc);
+    else
+      dia_tma_run<CHECK, 0, V, X, Acc, VEC, ROW, RB>(wa, va, len, acc);
+  }
+}
+
+// Slab of one tile: its values, copied from the 16-byte boundary at or
+// below their first byte, then (from the next 16-byte boundary on) its
+// blocks' full-diagonal masks, copied the same way.
+struct DiaSlab {
+  int64_t v_lo, v_bytes, f_lo, f_bytes;
+  int v_skew, f_skew;  // bytes from the copies' starts to the tile's first value / mask
+  int64_t f_at;        // offset of the masks in the slab
+};
+
+template <class V>
+__device__ __forceinline__ DiaSlab dia_slab(int64_t R, int L, int nd) {
+  DiaSlab sl;
+  const int64_t v0 = R * nd * (int64_t)sizeof(V);
+  sl.v_lo = v0 & ~(int64_t)15;
+  sl.v_bytes = ((v0 + (int64_t)L * nd * (int64_t)sizeof(V) + 15) & ~(int64_t)15) - sl.v_lo;
+  sl.v_skew = (int)(v0 - sl.v_lo);
+  const int64_t f0 = (R / kDiaRows) * (int64_t)sizeof(uint32_t);
+  sl.f_lo = f0 & ~(int64_t)15;
+  sl.f_bytes = ((f0 + (int64_t)(L / kDiaRows) * 4 + 15) & ~(int64_t)15) - sl.f_lo;
+  sl.f_skew = (int)(f0 - sl.f_lo);
+  sl.f_at = ((int64_t)L * nd * (int64_t)sizeof(V) + 15) / 16 * 16 + 16;
+  return sl;
+}
+
+template <class V, class X, int NV, int RB>
+__global__ void __launch_bounds__(kDiaRows * kDiaTmaThreads / RB, 1)
+    k_spmm_dia_tma(const __grid_constant__ CUtensorMap tmB, const DiaTmaArgs a,
+                   const V *__restrict__ dv, const uint32_t *__restrict__ dfull,
+                   X *__restrict__ C, int64_t ldc, X alpha, X beta, int beta_nz,
+                   int *__restrict__ err) {
+  constexpr int VEC = 16 / (int)sizeof(X);
+  constexpr int KS = NV * VEC;
+  constexpr int NT = kDiaRows * kDiaTmaThreads / RB;
+  constexpr int L = NT / NV * RB;
+  static_assert(L == kDiaTmaThreads / NV * kDiaRows, "the tile of the launch plan");
+  static_assert(kDiaRows % RB == 0, "a thread's rows lie in one block");
+  using Acc = typename AccOf<V, X>::type;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t wbar[kDiaTmaMaxSlots];
+  __shared__ __align__(8) uint64_t vbar[2];
+  // Tensor copies land on 128-byte boundaries: the launch adds 128 bytes so
+  // that the slots can start at the first such boundary.
+  unsigned char *smem = smem_raw + ((128u - (tma::smem_addr(smem_raw) & 127u)) & 127u);
+  const int tid = threadIdx.x;
+  const int cl = tid % NV;
+  const int i0 = (tid / NV) * RB;
+  unsigned char *vbase = smem + (size_t)a.S * a.slot_bytes;
+  const uint32_t full_mask = a.nd >= 32 ? 0xffffffffu : (1u << a.nd) - 1u;
+  if (tid == 0) {
+    for (int s = 0; s < a.S; ++s)
+      tma::bar_init(&wbar[s]);
+    tma::bar_init(&vbar[0]);
+    tma::bar_init(&vbar[1]);
+    tma::bar_init_fence();
+  }
+  __syncthreads();
+  // Parity of the next phase of each barrier, and the copies issued but not
+  // yet waited for (the same in every thread).
+  uint32_t wph = 0, vph = 0, wpend = 0, vpend = 0;
+  const bool early = a.S > a.G;
+
+  for (int64_t item = blockIdx.x; item < a.n_items; item += gridDim.x) {
+    const int slice = (int)(item % a.n_slices);
+    const int64_t rest = item / a.n_slices;
+    const int chain = (int)(rest % a.n_chains);
+    const int seg = (int)(rest / a.n_chains);
+    const int k0 = slice * KS;
+    const int64_t b = (int64_t)chain * L;
+    const int rows_tile = (int)min((int64_t)L, (int64_t)a.P - b);
+    const int64_t tiles = b < a.m ? ((int64_t)a.m - b + a.P - 1) / a.P : 0;
+    const int t0 = seg * a.Z;
+    const int t1 = (int)min((int64_t)t0 + a.Z, tiles);
+    if (t0 >= t1)
+      continue;
+    auto issue_window = [&](int w) {  // thread 0
+      const int s = w % a.S;
+      const int64_t row0 = b + (int64_t)w * a.P + a.win0;
+      tma::bar_expect_tx(&wbar[s], (uint32_t)(a.slot_bytes + a.tx_extra));
+      for (int j = 0; j < a.NB; ++j)
+        tma::tensor_load_2d(smem + (size_t)s * a.slot_bytes + (size_t)j * a.BR * KS * sizeof(X),
+                            &tmB, k0, (int32_t)(row0 + (int64_t)j * a.BR), &wbar[s]);
+    };
+    auto issue_vals = [&](int t) {  // thread 0
+      const int s = t & 1;
+      const DiaSlab sl = dia_slab<V>(b + (int64_t)t * a.P, L, a.nd);
+      unsigned char *slab = vbase + (size_t)s * a.vslab_bytes;
+      tma::bar_expect_tx(&vbar[s], (uint32_t)(sl.v_bytes + sl.f_bytes));
+      tma::bulk_load(slab, reinterpret_cast<const char *>(dv) + sl.v_lo, (uint32_t)sl.v_bytes,
+                     &vbar[s]);
+      tma::bulk_load(slab + sl.f_at, reinterpret_cast<const char *>(dfull) + sl.f_lo,
+                     (uint32_t)sl.f_bytes, &vbar[s]);
+    };
+    if (tid == 0) {
+      for (int g = 0; g < a.G; ++g)
+        issue_window(t0 + g);
+      issue_vals(t0);
+    }
+    for (int g = 0; g < a.G; ++g)
+      wpend |= 1u << ((t0 + g) % a.S);
+    vpend |= 1u << (t0 & 1);
+
+    for (int t = t0; t < t1; ++t) {
+      const int64_t R = b + (int64_t)t * a.P;
+      if (t + 1 < t1) {
+        if (tid == 0) {
+          if (early)
+            issue_window(t + a.G);
+          issue_vals(t + 1);
+        }
+        if (early)
+          wpend |= 1u << ((t + a.G) % a.S);
+        vpend |= 1u << ((t + 1) & 1);
+      }
+      const int vs = t & 1;
+      if (!cta_wait(&vbar[vs], (vph >> vs) & 1u, a.wait_limit))
+        goto failed;
+      vph ^= 1u << vs;
+      vpend &= ~(1u << vs);
+      {
+        Acc acc[RB][VEC];
+#pragma unroll
+        for (int i = 0; i < RB; ++i)
+#pragma unroll
+          for (int v = 0; v < VEC; ++v)
+            acc[i][v] = Acc(0);
+        const DiaSlab sl = dia_slab<V>(R, L, a.nd);
+        const unsigned char *slab = vbase + (size_t)vs * a.vslab_bytes;
+        const uint32_t vrow =
+            tma::smem_addr(slab + sl.v_skew) +
+            (uint32_t)(((i0 / kDiaRows) * a.nd * kDiaRows + i0 % kDiaRows) * (int)sizeof(V));
+        const uint32_t blk_full =
+            reinterpret_cast<const uint32_t *>(slab + sl.f_at + sl.f_skew)[i0 / kDiaRows];
+        const bool checked = (blk_full & full_mask) != full_mask;
+        for (int g = 0; g < a.G; ++g) {
+          const int s = (t + g) % a.S;
+          if (t == t0 || g == a.G - 1) {  // the window's first use
+            if (!cta_wait(&wbar[s], (wph >> s) & 1u, a.wait_limit))
+              goto failed;
+            wph ^= 1u << s;
+            wpend &= ~(1u << s);
+          }
+          constexpr int ROW = KS * (int)sizeof(X);
+          const uint32_t wrow = tma::smem_addr(smem + (size_t)s * a.slot_bytes) +
+                                (uint32_t)(i0 * ROW + cl * 16);
+          if (checked)
+            dia_tma_group<true, V, X, Acc, VEC, ROW, RB>(a, g, wrow, vrow, acc);
+          else
+            dia_tma_group<false, V, X, Acc, VEC, ROW, RB>(a, g, wrow, vrow, acc);
+          if (g == 0 && !early && t + 1 < t1) {
+            __syncthreads();  // every thread is done with PW(t): its slot takes PW(t + G)
+            if (tid == 0)
+              issue_window(t + a.G);
+            wpend |= 1u << ((t + a.G) % a.S);
+          }
+        }
+        const int col = k0 + cl * VEC;
+        if (col < a.k) {
+#pragma unroll
+          for (int i = 0; i < RB; ++i) {
+            const int64_t row = R + i0 + i;
+            if (i0 + i < rows_tile && row < a.m) {
+              X *cp = C + row * ldc + col;
+              X out[VEC];
+              if (beta_nz) {
+                X old[VEC];
+                ld_vec_plain<X, VEC>(cp, old);
+#pragma unroll
+                for (int v = 0; v < VEC; ++v)
+                  out[v] = (X)acc[i][v] * alpha + beta * old[v];
+              } else {
+#pragma unroll
+                for (int v = 0; v < VEC; ++v)
+                  out[v] = (X)acc[i][v] * alpha;
+              }
+              st_vec<X, VEC>(cp, out);
+            }
+          }
+        }
+      }
+      __syncthreads();  // the values slab and the windows are free for the next copies
+    }
+  }
+  return;
+
+failed:
+  // A copy did not land in time: record it, give the CTA's copies in flight
+  // another bounded wait (its shared memory must outlive them) and stop.
+  if (tid == 0) {
+    *(volatile int *)err = 1;
+    __threadfence_system();
+    for (int s = 0; s < a.S; ++s)
+      if (wpend & (1u << s))
+        tma::bar_wait_bounded(&wbar[s], (wph >> s) & 1u, a.wait_limit);
+    for (int s = 0; s < 2; ++s)
+      if (vpend & (1u << s))
+        tma::bar_wait_bounded(&vbar[s], (vph >> s) & 1u, a.wait_limit);
+  }
+  __syncthreads();
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// to the driver library); null if the driver does not offer it.
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                   const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                   const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static const EncodeTiledFn fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (EncodeTiledFn) nullptr;
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
+template <class V, class X, int NV>
+void dia_tma_run(const DiaDev &d, const DiaTmaShape &sh, const CUtensorMap &map, X *C,
+                 int64_t ldc, X alpha, X beta, int sms, cudaStream_t s) {
+  constexpr int RB = kDiaTmaThreadRows;
+  constexpr int NT = kDiaRows * kDiaTmaThreads / RB;
+  auto kern = k_spmm_dia_tma<V, X, NV, RB>;
+  const size_t smem = sh.smem + 128;  // room to align the slots (see the kernel)
+  PLS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  PLS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
+  const unsigned grid =
+      (unsigned)std::min<int64_t>(sh.a.n_items, (int64_t)sms * std::max(per_sm, 1));
+  kern<<<grid, NT, smem, s>>>(map, sh.a, d.vals.as<V>(), d.full.as<uint32_t>(), C, ldc, alpha,
+                              beta, beta != X(0), d.err.dev);
+  PLS_LAUNCH_CHECK();
+}
+
+template <class V, class X>
+bool dia_tma_launch(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64_t ldc, int k,
+                    X alpha, X beta, cudaStream_t s, bool launch) {
+  DiaDev &d = c.dia;
+  int dev = 0, sms = 0;
+  PLS_CUDA(cudaGetDevice(&dev));
+  PLS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  DiaTmaShape sh = dia_tma_shape(d.offs, d.nd, m, k, (int)sizeof(X), (int)sizeof(V), sms);
+  const EncodeTiledFn enc = encode_tiled();
+  if (!sh.ok || !enc || c.ncols <= 0 || (uintptr_t)d.vals.p % 16)
+    return false;
+  // B as a 2-D tensor (k columns innermost, ncols rows of ldb elements),
+  // copied in boxes of KS columns x BR rows; rows outside [0, ncols) and
+  // columns past k read as zeros. A shape the driver refuses is not used.
+  constexpr int VEC = 16 / (int)sizeof(X);
+  CUtensorMap map;
+  const cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)c.ncols};
+  const cuuint64_t strides[1] = {(cuuint64_t)ldb * sizeof(X)};
+  const cuuint32_t box[2] = {(cuuint32_t)(sh.NV * VEC), (cuuint32_t)sh.a.BR};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = enc(&map, sizeof(X) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                         2, const_cast<X *>(B), dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    return false;
+  if (!launch)
+    return true;
+  if (!d.err.host)
+    d.err.alloc();
+  sh.a.tx_extra = g_stage_shortfall.load();
+  sh.a.wait_limit = g_stage_wait_limit.load();
+  switch (sh.NV) {
+  case 8: dia_tma_run<V, X, 8>(d, sh, map, C, ldc, alpha, beta, sms, s); break;
+  case 4: dia_tma_run<V, X, 4>(d, sh, map, C, ldc, alpha, beta, sms, s); break;
+  default: dia_tma_run<V, X, 2>(d, sh, map, C, ldc, alpha, beta, sms, s); break;
+  }
+  return true;
 }
 
 }  // namespace
@@ -377,5 +843,35 @@ template bool spmm_dia<float>(CsrDev &, int32_t, const float *, int64_t, float *
                               float, float, cudaStream_t, bool);
 template bool spmm_dia<double>(CsrDev &, int32_t, const double *, int64_t, double *, int64_t,
                                int, double, double, cudaStream_t, bool);
+
+
+template <class X>
+bool spmm_dia_tma(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64_t ldc, int k,
+                  X alpha, X beta, cudaStream_t s, bool launch) {
+  DiaDev &d = c.dia;
+  if (d.err.host && *(volatile int *)d.err.host) {
+    *(volatile int *)d.err.host = 0;
+    throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE,
+                "diagonal-form SpMM: a staged copy did not complete (reported by an earlier call)");
+  }
+  // The diagonal form itself (built or examined here) and its conditions.
+  if (!spmm_dia<X>(c, m, B, ldb, C, ldc, k, alpha, beta, s, false))
+    return false;
+  const Vt vt = c.evt();
+  if constexpr (sizeof(X) == 8) {
+    if (vt == Vt::F64)
+      return dia_tma_launch<double, X>(c, m, B, ldb, C, ldc, k, alpha, beta, s, launch);
+  }
+  if (vt == Vt::F32)
+    return dia_tma_launch<float, X>(c, m, B, ldb, C, ldc, k, alpha, beta, s, launch);
+  if (vt == Vt::BF16)
+    return dia_tma_launch<__nv_bfloat16, X>(c, m, B, ldb, C, ldc, k, alpha, beta, s, launch);
+  return false;
+}
+
+template bool spmm_dia_tma<float>(CsrDev &, int32_t, const float *, int64_t, float *, int64_t,
+                                  int, float, float, cudaStream_t, bool);
+template bool spmm_dia_tma<double>(CsrDev &, int32_t, const double *, int64_t, double *, int64_t,
+                                   int, double, double, cudaStream_t, bool);
 
 }  // namespace pls

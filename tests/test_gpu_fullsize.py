@@ -30,8 +30,8 @@ pytestmark = pytest.mark.gpu
 TOLS = {"native": 1e-12, "fp32": 1e-5, "bf16": 1e-2}
 STORAGE = {"native": pls.STORAGE_NATIVE, "fp32": pls.STORAGE_FP32, "bf16": pls.STORAGE_BF16}
 # SpMM kernels: -1 measured choice, 0 row group, 1 staged, 2 row group with
-# shared entries, 3 diagonal form.
-SPMM_PATHS = (-1, 0, 1, 2, 3)
+# shared entries, 3 diagonal form, 4 diagonal form with TMA-staged B.
+SPMM_PATHS = (-1, 0, 1, 2, 3, 4)
 
 
 def _spmv_err(y, rp, c, v, x):
@@ -145,9 +145,9 @@ def test_c3_stencil_spmm_full(c3, c3_refs, k, storage):
             den[den == 0] = 1
             worst = max(worst, float((np.abs(got - ref) / den).max()))
         assert worst <= TOLS[storage], (k, storage, path, worst)
-    # the row group, shared entries and diagonal kernels each ran once, and
-    # the staged kernel with FP64 / FP32 values
-    assert {0, 2, 3} <= ran, ran
+    # the row group, shared entries, diagonal and TMA-staged diagonal
+    # kernels each ran once, and the staged kernel with FP64 / FP32 values
+    assert {0, 2, 3, 4} <= ran, ran
     if storage != "bf16":
         assert 1 in ran, ran
     A.destroy()

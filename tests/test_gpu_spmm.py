@@ -367,25 +367,32 @@ def test_random_matrix_keeps_row_group_kernel():
 
 
 def test_spmm_measured_choice_matches_oracle():
-    """Default path: the first SpMM on a stencil times both kernels on
-    scratch output, keeps the faster, and the result matches the oracle
-    (beta != 0: the timing runs must not touch C)."""
+    """Default path: the first SpMM times the applicable kernels on scratch
+    output, keeps the fastest, and the result matches the oracle (beta != 0:
+    the timing runs must not touch C). On a stencil the diagonal forms are
+    timed and the staged kernel is not; on a band of 41 diagonals (beyond
+    the diagonal form's 32) the staged kernel is timed."""
     import torch
 
     rng = np.random.default_rng(11)
-    m, n, rp, c, v = W.stencil_27pt(24, seed=2)
-    A = pls.SpMat.csr(m, n, rp, c, v)
-    for k in (8, 32):
-        Bd = rng.uniform(-1, 1, (n, k))
-        C0 = rng.uniform(-1, 1, (m, k))
-        Bt, Ct = torch.tensor(Bd, device="cuda"), torch.tensor(C0, device="cuda")
-        s = torch.cuda.Stream()
-        A.spmm_dev(Bt.data_ptr(), k, k, Ct.data_ptr(), k, 0.75, 1.5, s.cuda_stream)
-        s.synchronize()
-        info = A.spmm_info()
-        assert info["path"] in (0, 1, 2) and info["ms_staged"] > 0 and info["ms_rows"] > 0, info
-        ref = spmm_ref(rp, c, v, Bd, 0.75, 1.5, C0)
-        assert scaled_err(Ct.cpu().numpy(), ref, rp, c, v, Bd, 0.75, 1.5, C0) <= 1e-12
+    cases = [(W.stencil_27pt(24, seed=2), False), (W.banded_csr(20000, 20, rng), True)]
+    for (m, n, rp, c, v), staged_timed in cases:
+        A = pls.SpMat.csr(m, n, rp, c, v)
+        for k in (8, 32):
+            Bd = rng.uniform(-1, 1, (n, k))
+            C0 = rng.uniform(-1, 1, (m, k))
+            Bt, Ct = torch.tensor(Bd, device="cuda"), torch.tensor(C0, device="cuda")
+            s = torch.cuda.Stream()
+            A.spmm_dev(Bt.data_ptr(), k, k, Ct.data_ptr(), k, 0.75, 1.5, s.cuda_stream)
+            s.synchronize()
+            info = A.spmm_info()
+            assert info["ms_rows"] > 0, info
+            if staged_timed:
+                assert info["path"] in (0, 1, 2) and info["ms_staged"] > 0, info
+            else:
+                assert info["path"] in (0, 2, 3, 4) and info["ms_staged"] == 0, info
+            ref = spmm_ref(rp, c, v, Bd, 0.75, 1.5, C0)
+            assert scaled_err(Ct.cpu().numpy(), ref, rp, c, v, Bd, 0.75, 1.5, C0) <= 1e-12
 
 
 @pytest.mark.parametrize("ta", [pls.OPERATION_NOTRANS, pls.OPERATION_TRANS])
@@ -480,6 +487,117 @@ def test_staged_wait_timeout_is_reported_and_recoverable():
     s.synchronize()
     ref = spmm_ref(rp, c, v, Bd, 1.0, 0.0, None)
     assert scaled_err(Ct.cpu().numpy(), ref, rp, c, v, Bd, 1.0, 0.0, None) <= 1e-12
+
+
+def test_dia_tma_wait_timeout_is_reported_and_recoverable():
+    """The same failure path for the diagonal form with TMA-staged B: its
+    window barriers expect 16 bytes more than the tensor copies bring, so
+    every CTA's bounded wait runs out with all copies landed; C is left
+    untouched, the next SpMM reports EXECUTION_FAILURE, and once the hook is
+    cleared the handle computes correctly."""
+    import torch
+
+    m, n, rp, c, v = W.stencil_27pt(16, seed=2)
+    k = 8
+    rng = np.random.default_rng(13)
+    Bd = rng.uniform(-1, 1, (n, k))
+    A = pls.SpMat.csr(m, n, rp, c, v)
+    A.set_spmm_path(4)
+    Bt = torch.tensor(Bd, device="cuda")
+    Ct = torch.full((m, k), 7.0, dtype=torch.float64, device="cuda")
+    s = torch.cuda.Stream()
+    L = pls.lib()
+    assert L.perflibs_b200_testing_stage_fault(16, 20000) == 0
+    try:
+        A.spmm_dev(Bt.data_ptr(), k, k, Ct.data_ptr(), k, 1.0, 0.0, s.cuda_stream)
+        s.synchronize()
+        assert A.spmm_info()["path"] == 4
+        assert torch.all(Ct == 7.0)
+        with pytest.raises(pls.PerflibsError) as e:
+            A.spmm_dev(Bt.data_ptr(), k, k, Ct.data_ptr(), k, 1.0, 0.0, s.cuda_stream)
+        assert e.value.status == pls.STATUS_EXECUTION_FAILURE
+    finally:
+        assert L.perflibs_b200_testing_stage_fault(0, 0) == 0
+    s.synchronize()
+    A.spmm_dev(Bt.data_ptr(), k, k, Ct.data_ptr(), k, 1.0, 0.0, s.cuda_stream)
+    s.synchronize()
+    assert A.spmm_info()["path"] == 4
+    ref = spmm_ref(rp, c, v, Bd, 1.0, 0.0, None)
+    assert scaled_err(Ct.cpu().numpy(), ref, rp, c, v, Bd, 1.0, 0.0, None) <= 1e-12
+
+
+@pytest.mark.parametrize("storage", [pls.STORAGE_NATIVE, pls.STORAGE_FP32, pls.STORAGE_BF16])
+def test_dia_tma_equals_diagonal_form_bitwise(storage):
+    """The diagonal form with TMA-staged B adds each row's entries in the
+    same order with the same arithmetic as the diagonal-form kernel, so the
+    two agree bit for bit: 27- and 7-point 3-D stencils (windows chained
+    over planes), 5- and 9-point 2-D stencils (over lines), bands and a
+    diagonal (one group); k from one 16-byte vector to several column
+    slices with a partial last one (the staged kernel runs from four vectors
+    on; narrower k may not fit its windows in shared memory, and then the
+    diagonal form runs); B with ldb > k; beta = 0 and beta != 0; and the
+    result matches the oracle within the storage mode's tolerance."""
+    import torch
+
+    from tests.conftest import rel_err_rows  # noqa: F401
+
+    rng = np.random.default_rng(21)
+    native = storage == pls.STORAGE_NATIVE
+    dt = np.float64 if native else np.float32
+    tdt = torch.float64 if native else torch.float32
+    tol = {pls.STORAGE_NATIVE: 1e-12, pls.STORAGE_FP32: 1e-5, pls.STORAGE_BF16: 1e-2}[storage]
+
+    def stencil(g, pts):
+        if pts == 27:
+            return W.stencil_27pt(g, seed=3)
+        n = g ** 3 if pts == 7 else g * g
+        idx = np.arange(n)
+        if pts == 7:
+            z, y, x = idx // (g * g), (idx // g) % g, idx % g
+            nb = [(-g * g, z > 0), (-g, y > 0), (-1, x > 0), (0, idx >= 0), (1, x < g - 1), (g, y < g - 1),
+                  (g * g, z < g - 1)]
+        else:
+            y, x = idx // g, idx % g
+            nb = [(dy * g + dx, (y + dy >= 0) & (y + dy < g) & (x + dx >= 0) & (x + dx < g))
+                  for dy in (-1, 0, 1) for dx in (-1, 0, 1)]
+        cols = np.stack([idx + o for o, _ in nb], 1)
+        mask = np.stack([mk for _, mk in nb], 1)
+        rp = np.zeros(n + 1, np.int32)
+        rp[1:] = np.cumsum(mask.sum(1))
+        return n, n, rp, cols[mask].astype(np.int32), rng.uniform(-1, 1, int(rp[-1]))
+
+    cases = [stencil(22, 27), stencil(30, 7), stencil(150, 9), W.laplacian_2d(200),
+             W.banded_csr(7001, 6, rng), W.banded_csr(513, 0, rng)]
+    for (m, n, rp, c, v) in cases:
+        A = pls.SpMat.csr(m, n, rp, c, v.astype(dt))
+        A.set_storage(storage)
+        for k in (4, 8, 16, 24, 40, 72, 136):
+            vec = 16 // np.dtype(dt).itemsize
+            if k % vec:
+                continue
+            for ldb in (k, k + 2 * vec):
+                Bd = rng.uniform(-1, 1, (n, ldb)).astype(dt)
+                C0 = rng.uniform(-1, 1, (m, k)).astype(dt)
+                Bt = torch.tensor(Bd, device="cuda")
+                for alpha, beta in ((1.5, 0.0), (-0.75, 0.5)):
+                    outs = {}
+                    for path in (3, 4):
+                        A.set_spmm_path(path)
+                        Ct = torch.tensor(C0, device="cuda")
+                        A.spmm_dev(Bt.data_ptr(), ldb, k, Ct.data_ptr(), k, alpha, beta)
+                        torch.cuda.synchronize()
+                        outs[path] = (Ct.cpu().numpy(), A.spmm_info()["path"])
+                    # path 4 falls back to the diagonal form when its plan does not fit
+                    # shared memory (k of one or two vectors on the 3-D stencil)
+                    assert outs[3][1] == 3 and outs[4][1] in (3, 4), (m, k, ldb, outs[3][1], outs[4][1])
+                    if k >= 4 * vec:
+                        assert outs[4][1] == 4, (m, k, ldb)
+                    np.testing.assert_array_equal(outs[4][0], outs[3][0], err_msg=f"m={m} k={k} ldb={ldb}")
+                    B64 = np.ascontiguousarray(Bd[:, :k].astype(np.float64))
+                    ref = spmm_ref(rp, c, v, B64, alpha, beta, C0.astype(np.float64) if beta else None)
+                    err = scaled_err(outs[4][0].astype(np.float64), ref, rp, c, v, B64, alpha, beta,
+                                     C0.astype(np.float64))
+                    assert err <= tol, (m, k, ldb, err)
 
 
 @pytest.mark.parametrize("dt", [np.float64, np.float32])
