@@ -501,6 +501,77 @@ def c4_config(args, timer, sp):
     return out
 
 
+def bsr8_config(args, timer, sp):
+    """BSR SpMM with 8 x 8 blocks and BF16 value storage (FP32 B and C, FP32
+    accumulation), the tensor-core kernel (tcgen05.mma kind::tf32) against the
+    FMA kernel: (1) a blocked random matrix, 32,768 block rows of 8 distinct
+    random block columns each (n = 262,144, 16.8 M stored values), k = 128,
+    seed 5; (2) the BSR instances of the C4 batch one by one. Errors against
+    the FP64 oracle of the FP32 values; tolerance 1e-2 (BF16 storage)."""
+    import torch
+
+    import oracle
+    import perf_libs_sparse_b200 as pls
+
+    rng = np.random.default_rng(5)
+    mb, per_row, k = 32768, 8, 128
+    rp = np.arange(0, (mb + 1) * per_row, per_row, dtype=np.int32)
+    col = np.concatenate([np.sort(rng.choice(mb, per_row, replace=False)) for _ in range(mb)]).astype(np.int32)
+    vals = rng.uniform(-1, 1, len(col) * 64).astype(np.float32)
+    n = mb * 8
+    A = pls.SpMat.bsr(pls.ROW_MAJOR, n, n, 8, rp, col, vals)
+    A.set_storage(pls.STORAGE_BF16)
+    A.set_stream(sp)
+    B = rng.uniform(-1, 1, (n, k)).astype(np.float32)
+    Bd = torch.tensor(B, device="cuda")
+    Cd = torch.zeros((n, k), dtype=torch.float32, device="cuda")
+    nbytes = len(col) * 64 * 2 + len(col) * 4 + (mb + 1) * 4 + 2 * n * k * 4
+    out = {"workload": f"BSR bs=8, {mb} block rows x {per_row} random blocks, n={n}, k={k}, BF16 values, "
+                       "FP32 B and C", "algorithmic_bytes_per_step": nbytes, "arms": {}}
+    crp, cc, cv = oracle.bsr2csr(rp, col, vals.astype(np.float64), 8, pls.ROW_MAJOR)
+    rows = np.arange(0, 16384)
+    for name, path in (("tensor_core", 5), ("fma", 0)):
+        A.set_spmm_path(path)
+        K = max(args.steps, 10)
+        ms = timer(lambda: A.spmm_dev(Bd.data_ptr(), k, k, Cd.data_ptr(), k, 1.0, 0.0, sp), K,
+                   max(args.warmup, 3))
+        torch.cuda.synchronize()
+        ran = A.spmm_info()["path"]
+        sub = (crp[:len(rows) + 1]).astype(np.int32)
+        p1 = int(crp[len(rows)])
+        ref = oracle.csr_spmm(sub, cc[:p1], cv[:p1], B.astype(np.float64), k)
+        scale = oracle.csr_spmm(sub, cc[:p1], np.abs(cv[:p1]), np.abs(B.astype(np.float64)), k)
+        got = Cd[:len(rows)].cpu().numpy().astype(np.float64)
+        den = np.maximum(np.abs(ref), scale)
+        den[den == 0] = 1
+        out["arms"][name] = {"path": ran, "ms_per_step": ms, "value": nbytes / ms / 1e6, "unit": "GB/s",
+                             "max_rel_err": float((np.abs(got - ref) / den).max()),
+                             "rows_checked": len(rows), "roofline": roofline(nbytes / ms / 1e6)}
+    A.destroy()
+    del Bd, Cd
+    # C4's BSR instances, one SpMM each, BF16 storage
+    inst = [d for d in W.batched_instances(512, seed=3) if d["kind"] == "bsr"]
+    tot = {5: 0.0, 0: 0.0}
+    worst = 0.0
+    for d in inst:
+        Ai = pls.SpMat.bsr(d["layout"], d["m"], d["n"], d["bs"], d["row_ptr"], d["col"], d["vals"])
+        Ai.set_storage(pls.STORAGE_BF16)
+        Ai.set_stream(sp)
+        Bi = torch.tensor(d["B"], device="cuda")
+        Ci = torch.zeros((d["m"], d["k"]), dtype=torch.float32, device="cuda")
+        for path in (5, 0):
+            Ai.set_spmm_path(path)
+            tot[path] += timer(lambda: Ai.spmm_dev(Bi.data_ptr(), d["k"], d["k"], Ci.data_ptr(), d["k"], 1.0, 0.0, sp),
+                               5, 2)
+        torch.cuda.synchronize()
+        Ai.destroy()
+    out["c4_bsr_instances"] = {"count": len(inst), "bs": sorted({d["bs"] for d in inst}),
+                               "ms_total_tensor_core": tot[5], "ms_total_fma": tot[0],
+                               "note": "one SpMM per instance (sum of per-instance times); the tensor-core "
+                                       "kernel applies to the bs = 8 instances, bs = 4 ones run the FMA kernel"}
+    return out
+
+
 def run_b200(args):
     import torch
 
@@ -687,6 +758,7 @@ def run_b200(args):
             "c3": c3_config(args, timer, sp, [(8, "native"), (32, "native"), (128, "native"),
                                               (32, "fp32"), (32, "bf16")]),
             "c4": c4_config(args, timer, sp),
+            "bsr8": bsr8_config(args, timer, sp),
         }
     if rank == 0 and world == 1 and not args.no_cpu:
         os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
@@ -717,6 +789,8 @@ def run_extra(args):
     timer = Timer(stream)
     if args.workload == "c1":
         sub = c1_config(args, timer, sp)
+    elif args.workload == "bsr8":
+        sub = bsr8_config(args, timer, sp)
     elif args.workload == "c3":
         sub = c3_config(args, timer, sp, [(args.k, args.storage)])["arms"][0]
     elif args.workload == "c4":
@@ -766,7 +840,7 @@ def emit(line, args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c3spmv", "c4"],
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c3spmv", "c4", "bsr8"],
                     help="c2 (default: the headline line, with c1 / c3 / c4 inside it) or one "
                          "configuration alone")
     ap.add_argument("--k", type=int, default=32, help="right-hand sides for --workload c3")

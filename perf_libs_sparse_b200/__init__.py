@@ -463,8 +463,8 @@ class SpMat:
     def spmm_info(self):
         """SpMM plan: tile_rows (0 = no staged tiles), staged_rows, runs,
         path of the last SpMM (1 staged, 0 row group, 2 row group with shared
-        entries, 3 diagonal form, 4 diagonal form with TMA-staged B, -1 none)
-        and the two
+        entries, 3 diagonal form, 4 diagonal form with TMA-staged B, 5 BSR on
+        the tensor cores, 6 BSR FMA kernel, -1 none) and the two
         timings of the measured choice (ms, 0 when not measured)."""
         r, u, n, pth = C.c_int32(), C.c_int64(), C.c_int64(), C.c_int32()
         ms_s, ms_r = C.c_float(), C.c_float()
@@ -477,8 +477,9 @@ class SpMat:
     def set_spmm_path(self, path):
         """-1 measured choice (default), 0 row-group kernel, 1 staged kernel,
         2 row-group kernel with shared entries, 3 diagonal-form kernel, 4
-        diagonal form with TMA-staged B (each where it applies; otherwise the
-        row-group kernel runs, or for 4 the diagonal form when it applies)."""
+        diagonal form with TMA-staged B, 5 BSR on the tensor cores (each where
+        it applies; otherwise the row-group kernel runs, or for 4 the diagonal
+        form when it applies, for 5 the BSR FMA kernel)."""
         _check(lib().perflibs_b200_spmat_set_spmm_path(self.h, path), "set_spmm_path")
 
     def set_host_bands(self, n_bands):

@@ -160,6 +160,7 @@ void prepare_values(Mat *A) {
       convert_values(b.vals.p, b.vt, b.vals_lo.p, t, nv, s);
       b.vt_lo = t;
       b.lo = true;
+      ++b.vals_version;
     }
   }
 }
@@ -1021,7 +1022,7 @@ perflibs_status_t spmm_impl(int transA, int transB, X alpha, Mat *A, Mat *B, X b
   if (ta)
     spmm_csr<X>(A->csrT, m, Bv, ldb, Cv, ldc, n, alpha, beta, s);
   else if (A->fmt == Fmt::BSR)
-    spmm_bsr<X>(A->bsr, Bv, ldb, Cv, ldc, n, alpha, beta, s);
+    spmm_bsr<X>(A->bsr, Bv, ldb, Cv, ldc, n, alpha, beta, s, A->csr.tiles);
   else
     spmm_csr<X>(A->csr, m, Bv, ldb, Cv, ldc, n, alpha, beta, s);
   PLS_CUDA(cudaStreamSynchronize(s));
@@ -1734,7 +1735,7 @@ void perflibs_spmat_print_err(perflibs_spmat_t A) {
 // ---------------------------------------------------------- extensions
 
 perflibs_status_t perflibs_b200_spmat_set_spmm_path(perflibs_spmat_t A, int32_t path) {
-  if (!A || path < -1 || path > 4)
+  if (!A || path < -1 || path > 5)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
   A->csr.tiles.forced = path;
   A->csr.tiles.choice_sig = -1;
@@ -1855,7 +1856,7 @@ static perflibs_status_t spmm_dev(X alpha, Mat *A, const X *B, int64_t ldb, int3
     prepare_values(A);
     cudaStream_t s = stream ? (cudaStream_t)stream : stream_of(A);
     if (A->fmt == Fmt::BSR)
-      spmm_bsr<X>(A->bsr, B, ldb, C, ldc, k, alpha, beta, s);
+      spmm_bsr<X>(A->bsr, B, ldb, C, ldc, k, alpha, beta, s, A->csr.tiles);
     else
       spmm_csr<X>(A->csr, A->m, B, ldb, C, ldc, k, alpha, beta, s);
     return PERFLIBS_STATUS_SUCCESS;

@@ -388,8 +388,20 @@ struct BsrDev {
   DevBuf vals_lo;
   Vt vt_lo = Vt::F64;
   bool lo = false;
+  uint64_t vals_version = 0;  // counts rebuilds of the kernels' values
   const void *ev() const { return lo ? vals_lo.p : vals.p; }
   Vt evt() const { return lo ? vt_lo : vt; }
+  // Tensor-core SpMM (spmm_bsr_tc.cu): the values as FP32 operand blocks
+  // (built from ev() at vals_version), its error flag, and the measured
+  // choice against the FMA kernel for the call signature tc_sig (0 FMA,
+  // 1 tensor cores) with both timings (ms).
+  DevBuf tc_vals;
+  const void *tc_vals_src = nullptr;
+  uint64_t tc_vals_version = ~0ull;
+  HostFlag tc_err;
+  int64_t tc_sig = -1;
+  int tc_choice = 0;
+  float ms_tc = 0.f, ms_fma = 0.f;
 };
 
 struct DenseDev {
@@ -560,9 +572,18 @@ bool spmm_dia(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64_t ldc, 
 template <class X>
 bool spmm_dia_tma(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64_t ldc, int k,
                   X alpha, X beta, cudaStream_t s, bool launch = true);
+// BSR SpMM: the FMA kernel, or for bs = 8 with BF16 values and FP32 B / C
+// the tensor-core kernel (spmm_bsr_tc.cu). `t` carries the forced path (5:
+// tensor cores whenever they apply; -1: the faster of the two, measured on
+// the first call of each signature) and receives the path taken (5 tensor
+// cores, 6 FMA) and, in ms_staged / ms_rows, the measured tensor-core / FMA
+// times.
 template <class X>
-void spmm_bsr(const BsrDev &b, const X *B, int64_t ldb, X *C, int64_t ldc,
-              int k, X alpha, X beta, cudaStream_t s);
+void spmm_bsr(BsrDev &b, const X *B, int64_t ldb, X *C, int64_t ldc, int k, X alpha, X beta,
+              cudaStream_t s, TileDev &t);
+// Tensor-core BSR SpMM; false (nothing launched) when it does not apply.
+bool spmm_bsr_tc(BsrDev &b, const float *B, int64_t ldb, float *C, int64_t ldc, int k,
+                 float alpha, float beta, cudaStream_t s, bool launch);
 
 // Layout helpers.
 template <class X>

@@ -387,8 +387,8 @@ __global__ void k_spmm_bsr_generic(int32_t mb, int bs, int layout,
 }
 
 template <class X>
-void spmm_bsr(const BsrDev &b, const X *B, int64_t ldb, X *C, int64_t ldc,
-              int k, X alpha, X beta, cudaStream_t s) {
+static void spmm_bsr_fma(const BsrDev &b, const X *B, int64_t ldb, X *C, int64_t ldc, int k,
+                         X alpha, X beta, cudaStream_t s) {
   if (b.mb == 0 || k == 0)
     return;
   const int bnz = beta != X(0);
@@ -421,15 +421,68 @@ void spmm_bsr(const BsrDev &b, const X *B, int64_t ldb, X *C, int64_t ldc,
   PLS_LAUNCH_CHECK();
 }
 
+// Kernel choice for a BSR SpMM: the tensor-core kernel where it applies
+// (bs = 8, BF16 values, FP32 B and C), forced (path 5) or measured against
+// the FMA kernel on the first call of each (k, ldb) signature (one warm-up
+// and two timed runs of each on a scratch C); the FMA kernel otherwise.
+template <class X>
+void spmm_bsr(BsrDev &b, const X *B, int64_t ldb, X *C, int64_t ldc, int k, X alpha, X beta,
+              cudaStream_t s, TileDev &t) {
+  if constexpr (sizeof(X) == 4) {
+    if (b.mb > 0 && k > 0 && (t.forced == 5 || t.forced == -1) &&
+        spmm_bsr_tc(b, B, ldb, C, ldc, k, alpha, beta, s, false)) {
+      bool tc = t.forced == 5;
+      if (!tc) {
+        const int64_t sig = ((int64_t)k << 32) ^ ldb;
+        if (b.tc_sig != sig) {
+          DevBuf scratch;
+          scratch.reserve(sizeof(float) * (size_t)b.mb * b.bs * k);
+          float *sc = scratch.as<float>();
+          cudaEvent_t e0, e1;
+          PLS_CUDA(cudaEventCreate(&e0));
+          PLS_CUDA(cudaEventCreate(&e1));
+          auto time2 = [&](auto &&run) {
+            run();
+            PLS_CUDA(cudaEventRecord(e0, s));
+            run();
+            run();
+            PLS_CUDA(cudaEventRecord(e1, s));
+            PLS_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            PLS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            return ms / 2;
+          };
+          b.ms_fma = time2([&] { spmm_bsr_fma<float>(b, B, ldb, sc, k, k, 1.f, 0.f, s); });
+          b.ms_tc = time2([&] { spmm_bsr_tc(b, B, ldb, sc, k, k, 1.f, 0.f, s, true); });
+          cudaEventDestroy(e0);
+          cudaEventDestroy(e1);
+          b.tc_choice = b.ms_tc < b.ms_fma ? 1 : 0;
+          b.tc_sig = sig;
+        }
+        tc = b.tc_choice == 1;
+        t.ms_staged = b.ms_tc;
+        t.ms_rows = b.ms_fma;
+        t.choice_sig = b.tc_sig | ((int64_t)1 << 62);  // timings valid for spmm_info
+      }
+      if (tc) {
+        spmm_bsr_tc(b, B, ldb, C, ldc, k, alpha, beta, s, true);
+        t.last_path = 5;
+        return;
+      }
+    }
+  }
+  spmm_bsr_fma<X>(b, B, ldb, C, ldc, k, alpha, beta, s);
+  t.last_path = 6;
+}
+
 template void spmm_csr<float>(CsrDev &, int32_t, const float *, int64_t,
                               float *, int64_t, int, float, float, cudaStream_t);
 template void spmm_csr<double>(CsrDev &, int32_t, const double *, int64_t,
                                double *, int64_t, int, double, double,
                                cudaStream_t);
-template void spmm_bsr<float>(const BsrDev &, const float *, int64_t, float *,
-                              int64_t, int, float, float, cudaStream_t);
-template void spmm_bsr<double>(const BsrDev &, const double *, int64_t,
-                               double *, int64_t, int, double, double,
-                               cudaStream_t);
+template void spmm_bsr<float>(BsrDev &, const float *, int64_t, float *, int64_t, int, float,
+                              float, cudaStream_t, TileDev &);
+template void spmm_bsr<double>(BsrDev &, const double *, int64_t, double *, int64_t, int, double,
+                               double, cudaStream_t, TileDev &);
 
 }  // namespace pls

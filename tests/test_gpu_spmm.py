@@ -707,3 +707,99 @@ def test_diagonal_form_spmm(dt):
     torch.cuda.synchronize()
     assert A.spmm_info()["path"] == 0
     A.destroy()
+
+
+def _random_bsr8(rng, mb, nb, max_blocks, layout, empty_frac=0.1):
+    """Random BSR with 8 x 8 blocks: 0 .. max_blocks distinct block columns
+    per block row (some rows empty), FP32 values U[-1, 1] with about 20% of
+    the entries explicit zeros."""
+    rp = np.zeros(mb + 1, np.int32)
+    cols = []
+    for i in range(mb):
+        cnt = 0 if rng.random() < empty_frac else int(rng.integers(1, max_blocks + 1))
+        c = np.sort(rng.choice(nb, min(cnt, nb), replace=False))
+        cols.append(c)
+        rp[i + 1] = rp[i] + len(c)
+    col = np.concatenate(cols).astype(np.int32)
+    vals = rng.uniform(-1, 1, len(col) * 64).astype(np.float32)
+    vals[rng.random(len(vals)) < 0.2] = 0.0
+    return rp, col, vals
+
+
+@pytest.mark.parametrize("layout", [pls.ROW_MAJOR, pls.COL_MAJOR])
+def test_bsr_tensor_core_spmm_vs_oracle(layout):
+    """The tensor-core BSR SpMM (tcgen05.mma kind::tf32, bs = 8, BF16 value
+    storage, FP32 B and C): every k from one column chunk of 128 to several
+    with a partial last one, B with ldb > k, beta = 0 and beta != 0, empty
+    block rows. Forced (path 5) it must run and match the FP64 oracle of the
+    FP32 values within the BF16 storage mode's 1e-2 (scaled per element),
+    as the FMA kernel does; the measured choice (path -1) picks one of the
+    two and is correct too."""
+    import torch
+
+    rng = np.random.default_rng(40 + layout)
+    mb, nb = 300, 260
+    rp, col, vals = _random_bsr8(rng, mb, nb, 12, layout)
+    m, n = mb * 8, nb * 8
+    crp, cc, cv = oracle.bsr2csr(rp, col, vals.astype(np.float64), 8, layout)
+    A = pls.SpMat.bsr(layout, m, n, 8, rp, col, vals)
+    A.set_storage(pls.STORAGE_BF16)
+    for k in (8, 64, 128, 200, 256):
+        for ldb in (k, k + 12):
+            Bd = rng.uniform(-1, 1, (n, ldb)).astype(np.float32)
+            C0 = rng.uniform(-1, 1, (m, k)).astype(np.float32)
+            Bt = torch.tensor(Bd, device="cuda")
+            B64 = np.ascontiguousarray(Bd[:, :k].astype(np.float64))
+            for alpha, beta in ((1.0, 0.0), (-0.5, 0.75)):
+                ref = spmm_ref(crp, cc, cv, B64, alpha, beta, C0.astype(np.float64) if beta else None)
+                for path, expect in ((5, 5), (0, 6), (-1, None)):
+                    A.set_spmm_path(path)
+                    Ct = torch.tensor(C0, device="cuda")
+                    A.spmm_dev(Bt.data_ptr(), ldb, k, Ct.data_ptr(), k, alpha, beta)
+                    torch.cuda.synchronize()
+                    ran = A.spmm_info()["path"]
+                    assert ran == expect if expect else ran in (5, 6), (k, ldb, path, ran)
+                    got = Ct.cpu().numpy().astype(np.float64)
+                    err = scaled_err(got, ref, crp, cc, cv, B64, alpha, beta, C0.astype(np.float64))
+                    assert err <= 1e-2, (k, ldb, path, err)
+
+
+def test_bsr_tensor_core_wait_timeout_is_reported_and_recoverable():
+    """Failure path of the tensor-core BSR kernel without a fault: with the
+    test hook armed, each CTA's first wait for a finished accumulator goes to
+    a barrier that nothing arrives on, so the bounded wait runs out; the
+    CTAs stop, wait for their MMAs in flight and free their tensor memory; C
+    is untouched, the next SpMM reports EXECUTION_FAILURE, and with the hook
+    cleared the handle computes correctly."""
+    import torch
+
+    rng = np.random.default_rng(77)
+    # no empty block rows: every CTA's first epilogue waits for an accumulator
+    rp, col, vals = _random_bsr8(rng, 64, 64, 4, pls.ROW_MAJOR, empty_frac=0.0)
+    A = pls.SpMat.bsr(pls.ROW_MAJOR, 512, 512, 8, rp, col, vals)
+    A.set_storage(pls.STORAGE_BF16)
+    A.set_spmm_path(5)
+    k = 64
+    Bd = rng.uniform(-1, 1, (512, k)).astype(np.float32)
+    Bt = torch.tensor(Bd, device="cuda")
+    Ct = torch.full((512, k), 7.0, dtype=torch.float32, device="cuda")
+    L = pls.lib()
+    assert L.perflibs_b200_testing_stage_fault(16, 20000) == 0
+    try:
+        A.spmm_dev(Bt.data_ptr(), k, k, Ct.data_ptr(), k, 1.0, 0.0)
+        torch.cuda.synchronize()
+        assert A.spmm_info()["path"] == 5
+        assert torch.all(Ct == 7.0)
+        with pytest.raises(pls.PerflibsError) as e:
+            A.spmm_dev(Bt.data_ptr(), k, k, Ct.data_ptr(), k, 1.0, 0.0)
+        assert e.value.status == pls.STATUS_EXECUTION_FAILURE
+    finally:
+        assert L.perflibs_b200_testing_stage_fault(0, 0) == 0
+    torch.cuda.synchronize()
+    A.spmm_dev(Bt.data_ptr(), k, k, Ct.data_ptr(), k, 1.0, 0.0)
+    torch.cuda.synchronize()
+    assert A.spmm_info()["path"] == 5
+    crp, cc, cv = oracle.bsr2csr(rp, col, vals.astype(np.float64), 8, pls.ROW_MAJOR)
+    B64 = Bd.astype(np.float64)
+    ref = spmm_ref(crp, cc, cv, B64, 1.0, 0.0, None)
+    assert scaled_err(Ct.cpu().numpy().astype(np.float64), ref, crp, cc, cv, B64, 1.0, 0.0, None) <= 1e-2
