@@ -324,12 +324,22 @@ class Timer:
         return max_over_ranks(ms, self.device) / K
 
 
+def timed_label(args):
+    """NVTX range around the timed steps of a configuration run alone
+    (--workload), which the ncu commands select with --nvtx-include timed/;
+    inside the default line only the C2 steps carry it."""
+    return "timed" if args.workload != "c2" else None
+
+
 def c1_config(args, timer, sp):
     """C1: plain FP64 CSR SpMV on the 5-point Laplacian 512^2 (21 MB). One
     step is one SpMV; steps go round R copies of the matrix, x and y
     (R * 21 MB > 2 x 126 MB of L2), so every step reads its inputs from HBM.
     The R-step rounds are captured in one CUDA graph and K steps are timed
-    under one event pair."""
+    under one event pair. The line is the plain CSR kernel (no tuning, the
+    configuration's definition); "tuned" is the same measurement after the
+    exhaustive autotuner (tuned once: the other copies share the structure,
+    so their optimize applies the cached result)."""
     import torch
 
     import perf_libs_sparse_b200 as pls
@@ -337,50 +347,59 @@ def c1_config(args, timer, sp):
     m, n, rp, c, v = W.laplacian_2d(512)
     x = W.uniform_vector(n, 0)
     nnz = int(rp[-1])
-    R = 12
-    mats, xs, ys = [], [], []
-    for _ in range(R):
-        A = pls.SpMat.csr(m, n, rp, c, v)
-        A.set_stream(sp)
-        A.hint(pls.HINT_SPMV_INVOCATIONS, pls.INVOCATIONS_SINGLE)  # plain CSR, no tuning
-        assert A.optimize() == 0
-        mats.append(A)
-        xs.append(torch.tensor(x, device="cuda"))
-        ys.append(torch.zeros(m, dtype=torch.float64, device="cuda"))
-
-    def round_():
-        for i in range(R):
-            mats[i].spmv_dev(xs[i].data_ptr(), ys[i].data_ptr(), 1.0, 0.0, sp)
-
-    graph = None
-    try:
-        round_()
-        torch.cuda.synchronize()
-        graph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(graph, stream=timer.stream, capture_error_mode="thread_local"):
-            round_()
-        torch.cuda.synchronize()
-        step = graph.replay
-    except Exception:
-        graph = None
-        step = round_
-    rounds = max(8, args.steps)
-    ms_round = timer(step, rounds, max(args.warmup, 3))
-    ms = ms_round / R
-    err, _ = spmv_rel_err(ys[0].cpu().numpy(), rp, c, v, x)
     b = W.algorithmic_bytes_spmv(m, n, nnz, 8, 8, False)
-    gbs = b / ms / 1e6
-    cfg = mats[0].config()
+    R = 12
+
+    def measure(invocations):
+        mats, xs, ys = [], [], []
+        for _ in range(R):
+            A = pls.SpMat.csr(m, n, rp, c, v)
+            A.set_stream(sp)
+            A.hint(pls.HINT_SPMV_INVOCATIONS, invocations)
+            assert A.optimize() == 0
+            mats.append(A)
+            xs.append(torch.tensor(x, device="cuda"))
+            ys.append(torch.zeros(m, dtype=torch.float64, device="cuda"))
+
+        def round_():
+            for i in range(R):
+                mats[i].spmv_dev(xs[i].data_ptr(), ys[i].data_ptr(), 1.0, 0.0, sp)
+
+        graph = None
+        try:
+            round_()
+            torch.cuda.synchronize()
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph, stream=timer.stream, capture_error_mode="thread_local"):
+                round_()
+            torch.cuda.synchronize()
+            step = graph.replay
+        except Exception:
+            graph = None
+            step = round_
+        rounds = max(8, args.steps)
+        ms = timer(step, rounds, max(args.warmup, 3), timed_label(args)) / R
+        err = max(spmv_rel_err(y.cpu().numpy(), rp, c, v, x)[0] for y in (ys[0], ys[-1]))
+        cfg = mats[0].config()
+        gbs = b / ms / 1e6
+        out = {"kernel": (f"CSR threads-per-row {cfg['tpr']}" if cfg["kind"] == pls.KIND_CSR
+                          else f"{KIND_NAMES[cfg['kind']]} C={cfg['C']} sigma={cfg['sigma']}"),
+               "value": gbs, "unit": "GB/s", "ms_per_step": ms, "steps": rounds * R,
+               "gflops": 2.0 * nnz / ms / 1e6, "max_rel_err": err, "tolerance": 1e-12,
+               "graph": graph is not None, "roofline": roofline(gbs)}
+        del graph
+        for A in mats:
+            A.destroy()
+        return out
+
+    plain = measure(pls.INVOCATIONS_SINGLE)
+    tuned = measure(pls.INVOCATIONS_MANY)
     out = {"workload": f"C1 5-point Laplacian 512x512 n={m} nnz={nnz}, plain FP64 CSR SpMV",
-           "kernel": f"CSR threads-per-row {cfg['tpr']}", "value": gbs, "unit": "GB/s",
-           "ms_per_step": ms, "steps": rounds * R, "gflops": 2.0 * nnz / ms / 1e6,
-           "max_rel_err": err, "tolerance": 1e-12,
+           **plain,
            "l2": f"{R} rotating copies of matrix, x and y ({R * b / 1e6:.0f} MB) "
-                 f"in {'one CUDA graph per round' if graph else 'direct launches'}",
-           "algorithmic_bytes_per_step": b, "roofline": roofline(gbs)}
-    del graph
-    for A in mats:
-        A.destroy()
+                 f"in {'one CUDA graph per round' if plain['graph'] else 'direct launches'}",
+           "algorithmic_bytes_per_step": b,
+           "tuned": tuned, "tuned_over_plain": plain["ms_per_step"] / tuned["ms_per_step"]}
     return out
 
 
@@ -419,7 +438,7 @@ def c3_config(args, timer, sp, arms):
         t_choice = time.perf_counter() - t0
         K = max(args.steps, 10)
         ms = timer(lambda: A.spmm_dev(Bd.data_ptr(), k, k, Cd.data_ptr(), k, 1.0, 0.0, sp),
-                   K, max(args.warmup, 3))
+                   K, max(args.warmup, 3), timed_label(args))
         torch.cuda.synchronize()
         full = k <= 32
         err = spmm_rel_err_rows(lambda r0, r1: Cd[r0:r1].cpu().numpy().astype(np.float64),
@@ -472,7 +491,7 @@ def c4_config(args, timer, sp):
     bt = pls.Batch(mats, ks, [b_.data_ptr() for b_ in Bs], ks, [c_.data_ptr() for c_ in Cs], ks, stream=sp)
     tile, _ = bt.tune()
     K = max(args.steps, 10)
-    ms = timer(lambda: bt.exec(1.0, 0.0), K, max(args.warmup, 3))
+    ms = timer(lambda: bt.exec(1.0, 0.0), K, max(args.warmup, 3), timed_label(args))
     torch.cuda.synchronize()
     worst = 0.0
     for d, Cd in zip(inst, Cs):
@@ -534,7 +553,7 @@ def bsr8_config(args, timer, sp):
         A.set_spmm_path(path)
         K = max(args.steps, 10)
         ms = timer(lambda: A.spmm_dev(Bd.data_ptr(), k, k, Cd.data_ptr(), k, 1.0, 0.0, sp), K,
-                   max(args.warmup, 3))
+                   max(args.warmup, 3), timed_label(args))
         torch.cuda.synchronize()
         ran = A.spmm_info()["path"]
         sub = (crp[:len(rows) + 1]).astype(np.int32)
@@ -776,8 +795,10 @@ def run_b200(args):
 
 def run_extra(args):
     """One configuration alone, as its own JSON line (N = 1): c1, c3 (k =
-    --k, storage --storage), c4, or c3spmv (FP64 SpMV, tuned, on C3's
-    matrix: the structured counterpart of C2). The default line carries
+    --k, storage --storage), c4, c3spmv (FP64 SpMV, tuned, on C3's
+    matrix: the structured counterpart of C2) or c2local (C2's row lengths
+    with every column drawn from 8192, so that x's gathers hit L1: what the
+    C2 kernel does without its L2 gathers). The default line carries
     c1 / c3 / c4 too; these lines are for profiling one kernel."""
     import torch
 
@@ -796,8 +817,17 @@ def run_extra(args):
     elif args.workload == "c4":
         sub = c4_config(args, timer, sp)
     else:
-        m, n, rp, c, v = W.stencil_27pt(128, seed=2)
-        x = W.uniform_vector(n, 2)
+        if args.workload == "c2local":
+            # C2's row lengths and uniform random columns, drawn from 8192
+            # columns: x (64 KB) stays in L1, so the gathers do not reach L2.
+            m, n, rp, c, v = W.zipf_rows(4_194_304, seed=1, ncols=8192)
+            x = W.uniform_vector(n, 1)
+            what = (f"C2's Zipf row lengths with columns from 8192 (x in L1) m={m} nnz={int(rp[-1])}, "
+                    "FP64 SpMV: the C2 kernel without its L2 gathers")
+        else:
+            m, n, rp, c, v = W.stencil_27pt(128, seed=2)
+            x = W.uniform_vector(n, 2)
+            what = "27-point stencil 128^3 n=2097152 nnz=55742968 (C3's matrix), FP64 SpMV"
         A = pls.SpMat.csr(m, n, rp, c, v)
         A.set_stream(sp)
         A.hint(pls.HINT_SPMV_INVOCATIONS, pls.INVOCATIONS_MANY)
@@ -810,12 +840,12 @@ def run_extra(args):
         yd = torch.zeros(m, dtype=torch.float64, device="cuda")
         K, Wm = args.steps, max(args.warmup, 3)
         ms_plain = timer(lambda: P.spmv_dev(xd.data_ptr(), yd.data_ptr(), 1.0, 0.0, sp), K, Wm)
-        ms = timer(lambda: A.spmv_dev(xd.data_ptr(), yd.data_ptr(), 1.0, 0.0, sp), K, Wm)
+        ms = timer(lambda: A.spmv_dev(xd.data_ptr(), yd.data_ptr(), 1.0, 0.0, sp), K, Wm, "timed")
         torch.cuda.synchronize()
         err, _ = spmv_rel_err(yd.cpu().numpy(), rp, c, v, x)
         b = W.algorithmic_bytes_spmv(m, n, int(rp[-1]), 8, 8, False)
         cfg = A.config()
-        sub = {"workload": "27-point stencil 128^3 n=2097152 nnz=55742968 (C3's matrix), FP64 SpMV",
+        sub = {"workload": what,
                "value": b / ms / 1e6, "unit": "GB/s", "ms_per_step": ms, "max_rel_err": err,
                "plain_csr": {"value": b / ms_plain / 1e6, "ms_per_step": ms_plain},
                "speedup_vs_plain_csr": ms_plain / ms, "format": KIND_NAMES[cfg["kind"]],
@@ -840,7 +870,8 @@ def emit(line, args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c3spmv", "c4", "bsr8"],
+    ap.add_argument("--workload", default="c2",
+                    choices=["c1", "c2", "c3", "c3spmv", "c2local", "c4", "bsr8"],
                     help="c2 (default: the headline line, with c1 / c3 / c4 inside it) or one "
                          "configuration alone")
     ap.add_argument("--k", type=int, default=32, help="right-hand sides for --workload c3")

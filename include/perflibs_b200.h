@@ -320,6 +320,15 @@ perflibs_status_t perflibs_b200_selector_predict(perflibs_b200_selector_t S,
  * must outlive the handle's optimize calls. */
 perflibs_status_t perflibs_b200_spmat_set_selector(perflibs_spmat_t A,
                                                    perflibs_b200_selector_t S);
+/* SpMM kernel selectors (5 classes each: 0 row-group kernel, 1 row group
+ * with shared entries, 2 staged, 3 diagonal form, 4 diagonal form with
+ * TMA-staged B) for k <= 16, 17..64 and > 64; S may be NULL and entries may
+ * be NULL (those k keep the measured choice). With one attached, the first
+ * CSR SpMM of a call signature runs the most probable kernel that applies,
+ * without timing the candidates. The selectors must outlive the handle's
+ * SpMM calls. */
+perflibs_status_t perflibs_b200_spmat_set_spmm_selectors(perflibs_spmat_t A,
+                                                         const perflibs_b200_selector_t *S);
 
 /* ---- batched uneven SpMM ---------------------------------------------------
  * Many independent products C_i = alpha*A_i*B_i + beta*C_i (FP32 CSR or BSR
@@ -332,8 +341,10 @@ perflibs_status_t perflibs_b200_spmat_set_selector(perflibs_spmat_t A,
  * side by side (one 8-byte load per entry; BSR instances expanded to scalar
  * rows, blocks in stored order), made at creation: values changed in the
  * handles afterwards (perflibs_spmat_update) are not seen until the batch is
- * created again. The copy takes 8 bytes of device memory per stored scalar
- * entry. */
+ * created again. Beside it the batch keeps the values alone (read by the
+ * staged items whose rows have consecutive columns), so the copies take 12
+ * bytes of device memory per stored scalar entry, plus 4 bytes per diagonal
+ * slot of the band items (see perflibs_b200_batch_staged_kinds). */
 typedef struct perflibs_b200_batch_s *perflibs_b200_batch_t;
 perflibs_status_t perflibs_b200_batch_create(
     perflibs_b200_batch_t *Bt, int32_t count, const perflibs_spmat_t *mats,
@@ -369,6 +380,18 @@ perflibs_status_t perflibs_b200_batch_set_staging(perflibs_b200_batch_t Bt,
 perflibs_status_t perflibs_b200_batch_stage_info(perflibs_b200_batch_t Bt,
                                                  int64_t *staged_items,
                                                  int32_t *on);
+/* Kinds of staged items. consecutive: items whose rows all have
+ * consecutive columns (c, c + 1, ...: full bands, the rows of block-diagonal
+ * blocks); the kernel reads such a row's first column and then its values
+ * alone, from a values-only copy of the entries made at creation. band: of
+ * those, the items whose entries fill at least 3/4 of the diagonals
+ * (column - row) their rows reach; their values are also kept
+ * diagonal-major (zeros where a row has no entry), and the kernel walks the
+ * diagonals of 4 rows at a time, one new row of B per diagonal. Either
+ * pointer may be NULL. */
+perflibs_status_t perflibs_b200_batch_staged_kinds(perflibs_b200_batch_t Bt,
+                                                   int64_t *consecutive,
+                                                   int64_t *band);
 perflibs_status_t perflibs_b200_batch_destroy(perflibs_b200_batch_t Bt);
 
 /* Library / device information: SM count, L2 bytes, device ordinal. */

@@ -638,6 +638,41 @@ perflibs_status_t spmv_exec_dev(int trans, X alpha, Mat *A, const X *x, X beta, 
 // than 5 right-hand sides run as one SpMV per column.
 constexpr int kSpmvRhsThreshold = 5;
 
+// The learned SpMM selector's kernel order for k, into the CSR tile state
+// (pred_n = 0 when no selector is attached for k's bucket: the candidates
+// are then timed). The handle's features are computed on the first
+// prediction; a prediction is kept while k stays in its bucket.
+void spmm_predict(Mat *A, int k) {
+  TileDev &t = A->csr.tiles;
+  const int b = spmm_bucket(k);
+  perflibs_b200_selector_t S = A->spmm_selector[b];
+  if (!S) {
+    t.pred_n = 0;
+    return;
+  }
+  if (t.pred_n > 0 && t.pred_bucket == b)
+    return;
+  if (!A->features_valid) {
+    compute_features(A, A->features);
+    A->features_valid = true;
+  }
+  float probs[kSpmmClasses];
+  int32_t cls = -1;
+  t.pred_n = 0;
+  if (selector_classes(S) != kSpmmClasses ||
+      perflibs_b200_selector_predict(S, A->features, 1, probs, &cls) != PERFLIBS_STATUS_SUCCESS)
+    return;
+  int order[kSpmmClasses];
+  for (int q = 0; q < kSpmmClasses; ++q)
+    order[q] = q;
+  std::stable_sort(order, order + kSpmmClasses, [&](int x, int y) { return probs[x] > probs[y]; });
+  for (int q = 0; q < kSpmmClasses; ++q)
+    t.pred_order[q] = order[q];
+  t.pred_n = kSpmmClasses;
+  t.pred_bucket = b;
+  t.choice_sig = -1;  // decide the kernel again from this order
+}
+
 template <class X> void make_dense_zero(Mat *C, Dt dt, int32_t m, int32_t n, int layout) {
   cudaStream_t s = stream_of(C);
   C->dt = dt;
@@ -1024,7 +1059,10 @@ perflibs_status_t spmm_impl(int transA, int transB, X alpha, Mat *A, Mat *B, X b
   else if (A->fmt == Fmt::BSR)
     spmm_bsr<X>(A->bsr, Bv, ldb, Cv, ldc, n, alpha, beta, s, A->csr.tiles);
   else
+  {
+    spmm_predict(A, n);
     spmm_csr<X>(A->csr, m, Bv, ldb, Cv, ldc, n, alpha, beta, s);
+  }
   PLS_CUDA(cudaStreamSynchronize(s));
   C->dense.is_zero = false;
   return PERFLIBS_STATUS_SUCCESS;
@@ -1858,7 +1896,10 @@ static perflibs_status_t spmm_dev(X alpha, Mat *A, const X *B, int64_t ldb, int3
     if (A->fmt == Fmt::BSR)
       spmm_bsr<X>(A->bsr, B, ldb, C, ldc, k, alpha, beta, s, A->csr.tiles);
     else
+    {
+      spmm_predict(A, k);
       spmm_csr<X>(A->csr, A->m, B, ldb, C, ldc, k, alpha, beta, s);
+    }
     return PERFLIBS_STATUS_SUCCESS;
   });
 }
@@ -2215,6 +2256,21 @@ perflibs_status_t perflibs_b200_tune_candidates(int32_t cap, int32_t *cfg4, int3
     }
   }
   *count = (int32_t)c.size();
+  return PERFLIBS_STATUS_SUCCESS;
+}
+
+perflibs_status_t perflibs_b200_spmat_set_spmm_selectors(perflibs_spmat_t A,
+                                                         const perflibs_b200_selector_t *S) {
+  if (!A)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  for (int b = 0; b < 3; ++b)
+    if (S && S[b] && selector_classes(S[b]) != kSpmmClasses)
+      return param_error(A, 2, "An SpMM selector must have 5 classes (the SpMM kernels).");
+  for (int b = 0; b < 3; ++b)
+    A->spmm_selector[b] = S ? S[b] : nullptr;
+  A->csr.tiles.pred_n = 0;
+  A->csr.tiles.pred_bucket = -1;
+  A->csr.tiles.choice_sig = -1;
   return PERFLIBS_STATUS_SUCCESS;
 }
 

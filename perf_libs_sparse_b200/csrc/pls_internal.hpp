@@ -293,6 +293,14 @@ struct TileDev {
   // (when the lane shape allows them), 3 diagonal form (when it applies), 4
   // diagonal form with TMA-staged B (when it applies, else 3 when that does).
   int forced = -1;
+  // Kernel order predicted by the learned SpMM selector for the current
+  // call's k (classes kSpmmClass*, most probable first; pred_n = 0 when no
+  // selector is attached): a new call signature takes the first kernel of
+  // the order that applies instead of timing the candidates.
+  int pred_order[5] = {};
+  int pred_n = 0;
+  int pred_bucket = -1;
+  bool predicted = false;  // the kept choice came from the selector
   // Path of the last SpMM: 1 staged, 0 row group, 2 row group with shared
   // entries, 3 diagonal form, 4 diagonal form with TMA-staged B.
   int last_path = -1;
@@ -475,6 +483,11 @@ struct perflibs_spmat_top_t {
   int tuner = PERFLIBS_B200_TUNE_EXHAUSTIVE;
   perflibs_b200_selector_t selector = nullptr;  // not owned
   int selector_class = -1;                      // last prediction
+  // SpMM kernel selectors for k <= 16, 17..64 and > 64 (not owned), and the
+  // handle's structure features (computed once, on the first prediction).
+  perflibs_b200_selector_t spmm_selector[3] = {nullptr, nullptr, nullptr};
+  float features[PERFLIBS_B200_NFEATURES] = {};
+  bool features_valid = false;
   bool forced = false;
   pls::SpmvConfig forced_cfg;
   pls::SpmvConfig cfg;  // active SpMV kernel configuration
@@ -631,6 +644,14 @@ int64_t update_csr_values(CsrDev &c, SellDev *sell, int32_t m, int32_t n,
                           int64_t n_updates, const int32_t *rows_host,
                           const int32_t *cols_host, const void *vals_host,
                           Dt dt, int32_t base, cudaStream_t s);
+
+// Classes of the learned SpMM selector: the CSR SpMM kernels.
+enum SpmmClass { kSpmmRows = 0, kSpmmShared = 1, kSpmmStaged = 2, kSpmmDia = 3, kSpmmDiaTma = 4,
+                 kSpmmClasses = 5 };
+// The SpMM selector bucket of k: 0 for k <= 16, 1 for 17..64, 2 above.
+inline int spmm_bucket(int k) { return k <= 16 ? 0 : (k <= 64 ? 1 : 2); }
+// Classes (outputs) of a selector.
+int selector_classes(perflibs_b200_selector_t S);
 
 // Statistics for the learned selector (PERFLIBS_B200_NFEATURES floats).
 void compute_features(const Mat *A, float *out);

@@ -246,6 +246,10 @@ void forward_backward(Sel *S, int B, const float *x, const float *T, Activations
 
 using namespace pls;
 
+namespace pls {
+int selector_classes(perflibs_b200_selector_t S) { return S ? S->K : 0; }
+}  // namespace pls
+
 extern "C" {
 
 perflibs_status_t perflibs_b200_selector_create(perflibs_b200_selector_t *out, int32_t K,

@@ -219,7 +219,33 @@ void spmm_csr(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
         rows_shape(k, vec_s, (double)c.nnz / std::max<int32_t>(m, 1)));
     t.choice = 0;
     t.ms_rows = t.ms_staged = 0.f;
-    if (staged_ok || fits32 || shared_ok || dia_ok || tma_ok) {
+    t.predicted = false;
+    if (t.pred_n > 0) {
+      // The learned selector's order: its first kernel that applies, untimed.
+      t.choice = fits32 ? 2 : 0;
+      for (int q = 0; q < t.pred_n; ++q) {
+        const int cls = t.pred_order[q];
+        if (cls == kSpmmRows)
+          break;
+        if (cls == kSpmmShared && shared_ok) {
+          t.choice = 3;
+          break;
+        }
+        if (cls == kSpmmStaged && staged_ok) {
+          t.choice = 1;
+          break;
+        }
+        if (cls == kSpmmDia && dia_ok) {
+          t.choice = 4;
+          break;
+        }
+        if (cls == kSpmmDiaTma && tma_ok) {
+          t.choice = 5;
+          break;
+        }
+      }
+      t.predicted = true;
+    } else if (staged_ok || fits32 || shared_ok || dia_ok || tma_ok) {
       DevBuf scratch;
       scratch.reserve(sizeof(X) * (size_t)m * k);
       X *sc = scratch.as<X>();

@@ -55,6 +55,7 @@ def _bind():
         "perflibs_b200_tune_candidates": [i32, vp, vp],
         "perflibs_b200_selector_create": [vp, i32, u64],
         "perflibs_b200_selector_destroy": [vp],
+        "perflibs_b200_spmat_set_spmm_selectors": [vp, vp],
         "perflibs_b200_selector_get_params": [vp, vp],
         "perflibs_b200_selector_set_params": [vp, vp],
         "perflibs_b200_selector_loss_grad": [vp, vp, vp, i32, vp, vp],
@@ -269,6 +270,174 @@ def create_from_device(m, n, row_ptr, col, vals) -> SpMat:
     return SpMat(h, np.float64)
 
 
+# ------------------------------------------------------------------ SpMM
+# The SpMM selector's classes (kSpmmClass in the library), the forced path
+# (perflibs_b200_spmat_set_spmm_path) that runs each, and the path code that
+# spmm_info reports when it did run; k of each bucket (k <= 16, 17..64, > 64)
+# in the corpus.
+SPMM_CLASSES = ("row group", "shared entries", "staged", "diagonal form", "diagonal form, TMA")
+SPMM_FORCE = (0, 2, 1, 3, 4)
+SPMM_KS = (8, 32, 128)
+SHIPPED_SPMM = os.path.join(os.path.dirname(os.path.abspath(__file__)), "selector_spmm_params.npz")
+
+
+def spmm_library_times(t: np.ndarray) -> np.ndarray:
+    """The candidate times the library's measured choice compares: the
+    staged kernel is not a candidate where the diagonal form applies
+    (infinite times are kernels that do not apply)."""
+    t = np.array(t, np.float64, copy=True)
+    dia = np.isfinite(t[..., 3])
+    t[..., 2] = np.where(dia, np.inf, t[..., 2])
+    return t
+
+
+def spmm_pick(probs: np.ndarray, times: np.ndarray) -> np.ndarray:
+    """The kernel the library runs from a prediction: the most probable
+    class that applies (finite time); the row-group kernel always does."""
+    order = np.argsort(-probs, axis=1, kind="stable")
+    out = np.zeros(len(probs), np.int64)
+    for i in range(len(probs)):
+        for c in order[i]:
+            if np.isfinite(times[i, c]):
+                out[i] = c
+                break
+    return out
+
+
+def time_spmm_kernels(A: SpMat, k: int, reps: int = 3) -> list:
+    """Milliseconds of one FP64 SpMM with k right-hand sides and each kernel
+    forced (SPMM_FORCE), inf for kernels that do not apply (the forced path
+    fell back to another); A.m and A.n are set by the caller."""
+    import torch
+
+    Bd = torch.randn((A.n, k), dtype=torch.float64, device="cuda")
+    Cd = torch.empty((A.m, k), dtype=torch.float64, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = []
+    for cls, path in enumerate(SPMM_FORCE):
+        A.set_spmm_path(path)
+        A.spmm_dev(Bd.data_ptr(), k, k, Cd.data_ptr(), k, 1.0, 0.0)
+        torch.cuda.synchronize()
+        if A.spmm_info()["path"] != path:
+            out.append(float("inf"))
+            continue
+        e0.record()
+        for _ in range(reps):
+            A.spmm_dev(Bd.data_ptr(), k, k, Cd.data_ptr(), k, 1.0, 0.0)
+        e1.record()
+        torch.cuda.synchronize()
+        out.append(e0.elapsed_time(e1) / reps)
+    A.set_spmm_path(-1)
+    del Bd, Cd
+    return out
+
+
+def build_spmm_corpus(n_mats: int, out_dir: str, seed: int = 4, log_every: int = 50,
+                      budget_s: float = 1e9):
+    """Features and forced-kernel SpMM times (k in SPMM_KS) for the corpus
+    matrices [0, n_mats) (the SpMV corpus's generators and seed), resumable;
+    stops after budget_s seconds."""
+    import torch
+
+    os.makedirs(out_dir, exist_ok=True)
+    ck = os.path.join(out_dir, "spmm_corpus.jsonl")
+    done = {}
+    if os.path.exists(ck):
+        with open(ck) as f:
+            for line in f:
+                d = json.loads(line)
+                done[d["idx"]] = d
+    t0 = time.time()
+    with open(ck, "a") as f:
+        for i in range(n_mats):
+            if i in done:
+                continue
+            if time.time() - t0 > budget_s:
+                break
+            fam, m, n, rp, col, vals = generate(i, seed)
+            A = create_from_device(m, n, rp, col, vals)
+            A.m, A.n = m, n
+            feat = features(A)
+            d = {"idx": i, "family": fam, "m": m, "n": n, "nnz": int(rp[-1].item()),
+                 "features": feat.tolist(), "ms": {str(k): time_spmm_kernels(A, k) for k in SPMM_KS}}
+            f.write(json.dumps(d, allow_nan=True) + "\n")
+            f.flush()
+            done[i] = d
+            A.destroy()
+            del rp, col, vals
+            torch.cuda.empty_cache()
+            if log_every and (i + 1) % log_every == 0:
+                print(f"spmm corpus {i + 1}/{n_mats} {time.time() - t0:.0f}s", flush=True)
+    return [done[i] for i in sorted(done)]
+
+
+def evaluate_spmm(corpus, n_train: int, out_dir: str, epochs=400, batch=64, lr=3e-3, seed=0):
+    """Train one 5-class selector per k bucket on the first n_train matrices
+    and report, on the rest, the regret t_selected / t_best - 1 against the
+    library's measured choice (the fastest applicable kernel) and the
+    first-call timing the prediction saves (the measured choice runs each
+    applicable kernel three times)."""
+    X = np.array([d["features"] for d in corpus], np.float32)
+    rep = {"n_train": int(n_train), "n_heldout": int(len(corpus) - n_train), "classes": list(SPMM_CLASSES),
+           "buckets": {}}
+    params = {}
+    for b, k in enumerate(SPMM_KS):
+        T = spmm_library_times(np.array([d["ms"][str(k)] for d in corpus], np.float64))
+        Tt = np.where(np.isfinite(T), T, np.nan)
+        best = np.nanmin(Tt, axis=1)
+        r = np.where(np.isfinite(T), T / best[:, None] - 1.0, np.inf)
+        w = np.exp(-r / SOFT_TAU)
+        targets = (w / w.sum(axis=1, keepdims=True)).astype(np.float32)
+        sel = Selector(len(SPMM_CLASSES), seed=seed + b)
+        t0 = time.time()
+        loss = sel.train(X[:n_train], targets[:n_train], epochs=epochs, batch=batch, lr=lr, seed=seed)
+        train_s = time.time() - t0
+        params[f"b{b}"] = sel.get_params()
+        probs, _ = sel.predict(X[n_train:])
+        Th = T[n_train:]
+        pick = spmm_pick(probs, Th)
+        chosen = Th[np.arange(len(Th)), pick]
+        regret = chosen / best[n_train:] - 1.0
+        rows_only = Th[:, 0] / best[n_train:] - 1.0
+        timing_cost = 3.0 * np.where(np.isfinite(Th), Th, 0.0).sum(axis=1)  # the measured choice's runs
+        rep["buckets"][str(k)] = {
+            "train_final_loss": float(loss), "train_seconds": train_s,
+            "regret_mean": float(regret.mean()), "regret_median": float(np.median(regret)),
+            "regret_p90": float(np.percentile(regret, 90)),
+            "top1_accuracy": float((pick == np.nanargmin(np.where(np.isfinite(Th), Th, np.nan), axis=1)).mean()),
+            "row_group_only_regret_mean": float(rows_only.mean()),
+            "first_call_timing_ms_saved_mean": float(timing_cost.mean()),
+            "first_call_timing_over_one_spmm_mean": float((timing_cost / chosen).mean()),
+            "best_class_counts": {SPMM_CLASSES[c]: int(v) for c, v in
+                                  zip(*np.unique(np.nanargmin(np.where(np.isfinite(Th), Th, np.nan), axis=1),
+                                                 return_counts=True))},
+        }
+    np.savez(os.path.join(out_dir, "selector_spmm_params.npz"), **params)
+    with open(os.path.join(out_dir, "spmm_report.json"), "w") as f:
+        json.dump(rep, f, indent=1)
+    return rep
+
+
+def default_spmm_selectors():
+    """The shipped SpMM selectors (k <= 16, 17..64, > 64), or None."""
+    if not os.path.exists(SHIPPED_SPMM):
+        return None
+    z = np.load(SHIPPED_SPMM)
+    out = []
+    for b in range(3):
+        S = Selector(len(SPMM_CLASSES))
+        S.set_params(z[f"b{b}"])
+        out.append(S)
+    return out
+
+
+def attach_spmm_selectors(A: SpMat, sels):
+    """Attach three SpMM selectors (or None) to a handle."""
+    L = _bind()
+    arr = (C.c_void_p * 3)(*[(s.h.value if s is not None else None) for s in (sels or [None] * 3)])
+    _check(L.perflibs_b200_spmat_set_spmm_selectors(A.h, arr), "set_spmm_selectors")
+
+
 def default_selector():
     """The shipped trained selector, or None when the package has none."""
     if not os.path.exists(SHIPPED):
@@ -388,7 +557,16 @@ def main():
     ap.add_argument("--out", default="selector_out")
     ap.add_argument("--seed", type=int, default=4)
     ap.add_argument("--epochs", type=int, default=400)
+    ap.add_argument("--spmm", action="store_true", help="the SpMM kernel selectors instead")
+    ap.add_argument("--budget-s", type=float, default=1e9, help="stop building the corpus after this")
     args = ap.parse_args()
+    if args.spmm:
+        corpus = build_spmm_corpus(args.n, args.out, args.seed, budget_s=args.budget_s)
+        if len(corpus) < args.n:
+            print(f"spmm corpus stopped at the time budget: {len(corpus)} of {args.n}")
+        n_train = args.train if args.train is not None else int(round(0.8 * len(corpus)))
+        print(json.dumps(evaluate_spmm(corpus, n_train, args.out, epochs=args.epochs)))
+        return
     corpus = build_corpus(args.n, args.out, args.seed)
     n_train = args.train if args.train is not None else int(round(0.8 * args.n))
     rep = evaluate(corpus, n_train, args.out, epochs=args.epochs)
