@@ -341,10 +341,8 @@ perflibs_status_t perflibs_b200_spmat_set_spmm_selectors(perflibs_spmat_t A,
  * side by side (one 8-byte load per entry; BSR instances expanded to scalar
  * rows, blocks in stored order), made at creation: values changed in the
  * handles afterwards (perflibs_spmat_update) are not seen until the batch is
- * created again. Beside it the batch keeps the values alone (read by the
- * staged items whose rows have consecutive columns), so the copies take 12
- * bytes of device memory per stored scalar entry, plus 4 bytes per diagonal
- * slot of the band items (see perflibs_b200_batch_staged_kinds). */
+ * created again. The copy takes 8 bytes of device memory per stored scalar
+ * entry. */
 typedef struct perflibs_b200_batch_s *perflibs_b200_batch_t;
 perflibs_status_t perflibs_b200_batch_create(
     perflibs_b200_batch_t *Bt, int32_t count, const perflibs_spmat_t *mats,
@@ -380,18 +378,6 @@ perflibs_status_t perflibs_b200_batch_set_staging(perflibs_b200_batch_t Bt,
 perflibs_status_t perflibs_b200_batch_stage_info(perflibs_b200_batch_t Bt,
                                                  int64_t *staged_items,
                                                  int32_t *on);
-/* Kinds of staged items. consecutive: items whose rows all have
- * consecutive columns (c, c + 1, ...: full bands, the rows of block-diagonal
- * blocks); the kernel reads such a row's first column and then its values
- * alone, from a values-only copy of the entries made at creation. band: of
- * those, the items whose entries fill at least 3/4 of the diagonals
- * (column - row) their rows reach; their values are also kept
- * diagonal-major (zeros where a row has no entry), and the kernel walks the
- * diagonals of 4 rows at a time, one new row of B per diagonal. Either
- * pointer may be NULL. */
-perflibs_status_t perflibs_b200_batch_staged_kinds(perflibs_b200_batch_t Bt,
-                                                   int64_t *consecutive,
-                                                   int64_t *band);
 perflibs_status_t perflibs_b200_batch_destroy(perflibs_b200_batch_t Bt);
 
 /* Library / device information: SM count, L2 bytes, device ordinal. */

@@ -525,7 +525,6 @@ class Batch:
                            "perflibs_b200_batch_info": [vp, vp, vp, vp],
                            "perflibs_b200_batch_set_staging": [vp, C.c_int32],
                            "perflibs_b200_batch_stage_info": [vp, vp, vp],
-                           "perflibs_b200_batch_staged_kinds": [vp, vp, vp],
                            "perflibs_b200_batch_destroy": [vp]}.items():
             getattr(L, name).argtypes = args
             getattr(L, name).restype = C.c_int
@@ -567,14 +566,6 @@ class Batch:
         n, on = C.c_int64(), C.c_int32()
         _check(lib().perflibs_b200_batch_stage_info(self.h, C.byref(n), C.byref(on)), "batch_stage_info")
         return {"staged_items": n.value, "staging": bool(on.value)}
-
-    def staged_kinds(self):
-        """{'consecutive': staged items whose rows have consecutive columns
-        (values read alone), 'band': of those, the items run diagonal by
-        diagonal from diagonal-major values}."""
-        n, b = C.c_int64(), C.c_int64()
-        _check(lib().perflibs_b200_batch_staged_kinds(self.h, C.byref(n), C.byref(b)), "batch_staged_kinds")
-        return {"consecutive": n.value, "band": b.value}
 
     def destroy(self):
         if self.h is not None and self.h.value:

@@ -26,11 +26,7 @@
 // takes the next staged item from a second counter; when none are left its
 // warps go on to the per-warp items. Which blocks are staged is decided at
 // creation from each block's column window; the tuner times the batch with
-// and without them. In a staged item a row's column lanes load its entries
-// together (one entry per lane, four per lane per round trip) and pass them
-// round by shuffles; where every row of the block has consecutive columns
-// (full bands, block-diagonal blocks) they load the values alone, from a
-// values-only copy, and count the columns up from the row's first.
+// and without them.
 #include <algorithm>
 #include <climits>
 #include <cstring>
@@ -50,7 +46,6 @@ struct InstDesc {
   const int32_t *col;  // the handle's arrays, read once at creation
   const float *val;
   const int2 *cv;      // the batch's packed (column, value) copy the kernel reads
-  const float *vv;     // the same entries' values alone (staged items of consecutive columns)
   const float *B;
   float *C;
   int64_t ldb, ldc;
@@ -65,28 +60,15 @@ struct Item {
 // A staged item: rows [row0, row1) of instance `inst`, whose entries all
 // have columns in [lo, lo + w), for C's columns [c0, c0 + ks) (ks <= 32).
 // The window sits in shared memory as w rows of 4 * tk floats (ks rounded
-// up to whole float4s, zero past ks). consec: every row's columns are
-// consecutive (c, c + 1, ...: full bands, the rows of block-diagonal
-// blocks), so the kernel reads the row's first column and then its values
-// alone.
-//
-// Band items (consecutive columns, and the block's rows fill at least 3/4
-// of the diagonals dmin .. dmin + ndiag - 1, diagonal = column - row): the
-// block's values are also kept diagonal-major, band[d][g][i] for diagonal d,
-// group g of 4 rows and row i of the group (zeros where a row has no entry),
-// starting at float `band`; -1 for other items.
+// up to whole float4s, zero past ks).
 struct SItem {
   int32_t inst, row0, row1, lo;
   int32_t w, c0, ks, tk;
-  int32_t consec, dmin, ndiag;
-  int32_t gaps;  // the stage keeps a gap row after every 4 window rows (band items, tk <= 2)
-  int64_t band;
 };
 
 constexpr int kBatchThreads = 256;
 constexpr int kStageFloats = 8192;  // 32 KB of shared memory per CTA
 constexpr int kStageCols = 32;      // widest column slice of a staged item
-constexpr int kBandMaxDiag = 4096;  // widest band of a band item
 
 // One item's rows with the instance's vector shape.
 template <class Rows, bool OFF32>
@@ -116,20 +98,12 @@ __device__ __forceinline__ void batch_rows(const Rows &A, const InstDesc &d, con
 // column lies in the window (the item was built from the minimum and
 // maximum column of its entries), so the stage reads stay inside
 // w * 4 tk floats.
-//
-// Band items with tk <= 2 keep window row r at stage row r + r / 4 (a gap
-// row after every 4): their lanes read rows 4 apart, which then fall in
-// different banks.
-__device__ __forceinline__ int stage_row(int r, bool gaps) { return gaps ? r + (r >> 2) : r; }
-
 __device__ __forceinline__ void staged_item(const SItem &w, const InstDesc &d,
-                                            float *__restrict__ stage,
-                                            const float *__restrict__ band, float alpha,
-                                            float beta, int beta_nz) {
+                                            float *__restrict__ stage, float alpha, float beta,
+                                            int beta_nz) {
   constexpr int warps = kBatchThreads / 32;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int TK = w.tk, KSP = 4 * w.tk;
-  const bool gaps = w.gaps != 0;
   if ((d.ldb & 3) == 0 && ((uintptr_t)d.B & 15) == 0) {
     // TK lanes per window row, a float4 each (c0 is a multiple of 32, so
     // every row segment starts on 16 bytes)
@@ -150,7 +124,7 @@ __device__ __forceinline__ void staged_item(const SItem &w, const InstDesc &d,
           v.z = c + 2 < w.ks ? __ldg(p + 2) : 0.f;
           v.w = 0.f;  // c + 3 >= ks here
         }
-        dst[stage_row(r, gaps) * TK] = v;
+        dst[r * TK] = v;
       }
     }
   } else {
@@ -162,17 +136,41 @@ __device__ __forceinline__ void staged_item(const SItem &w, const InstDesc &d,
       const float *src = d.B + (int64_t)w.lo * d.ldb + w.c0 + (in ? c : 0);
 #pragma unroll 4
       for (int r = warp * per + rs; r < w.w; r += warps * per)
-        stage[stage_row(r, gaps) * KSP + c] = in ? __ldg(src + (int64_t)r * d.ldb) : 0.f;
+        stage[r * KSP + c] = in ? __ldg(src + (int64_t)r * d.ldb) : 0.f;
     }
   }
   __syncthreads();
   const float4 *st4 = reinterpret_cast<const float4 *>(stage);
-  const int per = 32 / TK;  // rows per warp (lanes past per * TK only join the shuffles)
+  const int per = 32 / TK;  // rows per warp
   const int rs = lane / TK, tk = lane - rs * TK;
+  if (rs >= per)
+    return;
   const int kk = w.c0 + 4 * tk;  // this lane's first column of C
   const int kend = w.c0 + w.ks;
   const bool vec = d.path == 0 && kk + 4 <= kend;
-  const auto store = [&](int32_t row, const float4 &acc) {
+  for (int32_t row = w.row0 + warp * per + rs; row < w.row1; row += warps * per) {
+    const int32_t s = __ldg(d.rp + row), e = __ldg(d.rp + row + 1);
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    const auto add = [&](int2 t) {
+      const float4 b = st4[(t.x - w.lo) * TK + tk];
+      const float a = __int_as_float(t.y);
+      acc.x = fmaf(a, b.x, acc.x);
+      acc.y = fmaf(a, b.y, acc.y);
+      acc.z = fmaf(a, b.z, acc.z);
+      acc.w = fmaf(a, b.w, acc.w);
+    };
+    int32_t q = s;
+    for (; q + 4 <= e; q += 4) {
+      int2 t[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        t[u] = __ldg(d.cv + q + u);
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        add(t[u]);
+    }
+    for (; q < e; ++q)
+      add(__ldg(d.cv + q));
     float *crow = d.C + (int64_t)row * d.ldc + kk;
     const float sum[4] = {acc.x, acc.y, acc.z, acc.w};
     if (vec) {
@@ -199,143 +197,6 @@ __device__ __forceinline__ void staged_item(const SItem &w, const InstDesc &d,
           crow[v] = o;
         }
     }
-  };
-  if (w.band >= 0) {
-    // Band item: TK lanes per group of 4 consecutive rows, one diagonal d at
-    // a time (ascending, so each row adds its entries in stored order). Row
-    // i of the group at diagonal d reads window row base + d + i, so the
-    // lanes keep the 4 rows base + d .. base + d + 3 in registers and load
-    // one new row per diagonal; the group's 4 values on d are one float4.
-    if (rs >= per)
-      return;
-    const int32_t ng = (w.row1 - w.row0 + 3) / 4;
-    const float4 *bv = reinterpret_cast<const float4 *>(band + w.band);
-    const auto srow = [&](int32_t x) {  // x outside the window: a row no entry uses
-      x = min(max(x, 0), w.w - 1);
-      return st4[stage_row(x, gaps) * TK + tk];
-    };
-    for (int32_t g = warp * per + rs; g < ng; g += warps * per) {
-      const int32_t r4 = w.row0 + 4 * g;
-      int32_t dlo[4], dhi[4];  // row i stores diagonals [dlo, dhi) (from dmin)
-      int32_t dstart = INT32_MAX, dend = INT32_MIN;
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        dlo[i] = dhi[i] = 0;
-        if (r4 + i < w.row1) {
-          const int32_t s = __ldg(d.rp + r4 + i), e = __ldg(d.rp + r4 + i + 1);
-          if (e > s) {
-            dlo[i] = __ldg(&d.cv[s].x) - (r4 + i) - w.dmin;
-            dhi[i] = dlo[i] + (e - s);
-            dstart = min(dstart, dlo[i]);
-            dend = max(dend, dhi[i]);
-          }
-        }
-      }
-      float4 acc[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-        acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-      const auto fma4 = [](float a, const float4 &b, float4 &c) {
-        c.x = fmaf(a, b.x, c.x);
-        c.y = fmaf(a, b.y, c.y);
-        c.z = fmaf(a, b.z, c.z);
-        c.w = fmaf(a, b.w, c.w);
-      };
-      if (dstart < dend) {
-        const int32_t base = r4 + w.dmin - w.lo;
-        float4 b0 = srow(base + dstart), b1 = srow(base + dstart + 1), b2 = srow(base + dstart + 2);
-        for (int32_t dd = dstart; dd < dend; ++dd) {
-          const float4 b3 = srow(base + dd + 3);
-          const float4 a = __ldg(bv + (int64_t)dd * ng + g);
-          if (dd >= dlo[0] && dd < dhi[0])
-            fma4(a.x, b0, acc[0]);
-          if (dd >= dlo[1] && dd < dhi[1])
-            fma4(a.y, b1, acc[1]);
-          if (dd >= dlo[2] && dd < dhi[2])
-            fma4(a.z, b2, acc[2]);
-          if (dd >= dlo[3] && dd < dhi[3])
-            fma4(a.w, b3, acc[3]);
-          b0 = b1;
-          b1 = b2;
-          b2 = b3;
-        }
-      }
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-        if (r4 + i < w.row1)
-          store(r4 + i, acc[i]);
-    }
-    return;
-  }
-  // A row's TK lanes load 4 TK consecutive entries per round trip, lane tk
-  // entries tk, tk + TK, tk + 2 TK, tk + 3 TK, and hand them round with
-  // shuffles; every lane still adds its row's entries one by one in stored
-  // order. The warp runs to its longest row (shuffles take every lane).
-  for (int32_t r0 = w.row0 + warp * per; r0 < w.row1; r0 += warps * per) {
-    const int32_t row = r0 + rs;
-    const bool live = rs < per && row < w.row1;
-    int32_t s = 0, len = 0;
-    if (live) {
-      s = __ldg(d.rp + row);
-      len = __ldg(d.rp + row + 1) - s;
-    }
-    int32_t longest = len;
-    for (int o = 16; o > 0; o >>= 1)
-      longest = max(longest, __shfl_xor_sync(0xffffffffu, longest, o));
-    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-    const int src0 = rs < per ? rs * TK : 0;
-    const auto add = [&](float a, int32_t c) {
-      const float4 b = st4[(c - w.lo) * TK + tk];
-      acc.x = fmaf(a, b.x, acc.x);
-      acc.y = fmaf(a, b.y, acc.y);
-      acc.z = fmaf(a, b.z, acc.z);
-      acc.w = fmaf(a, b.w, acc.w);
-    };
-    if (w.consec) {
-      // Column of entry q = the row's first column + q: values alone.
-      const int32_t cfirst = len > 0 ? __ldg(&d.cv[s].x) : 0;
-      for (int32_t base = 0; base < longest; base += 4 * TK) {
-        float t[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int32_t q = base + u * TK + tk;
-          t[u] = q < len ? __ldg(d.vv + s + q) : 0.f;
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int32_t q0 = base + u * TK;
-          if (q0 >= longest)
-            break;
-          for (int j = 0; j < TK; ++j) {
-            const float a = __shfl_sync(0xffffffffu, t[u], src0 + j);
-            if (q0 + j < len)
-              add(a, cfirst + q0 + j);
-          }
-        }
-      }
-    }
-    for (int32_t base = 0; !w.consec && base < longest; base += 4 * TK) {
-      int2 t[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int32_t q = base + u * TK + tk;
-        t[u] = q < len ? __ldg(d.cv + s + q) : make_int2(0, 0);
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int32_t q0 = base + u * TK;
-        if (q0 >= longest)
-          break;
-        for (int j = 0; j < TK; ++j) {
-          const int32_t c = __shfl_sync(0xffffffffu, t[u].x, src0 + j);
-          const float a = __int_as_float(__shfl_sync(0xffffffffu, t[u].y, src0 + j));
-          if (q0 + j < len)
-            add(a, c);
-        }
-      }
-    }
-    if (live)
-      store(row, acc);
   }
 }
 
@@ -346,8 +207,8 @@ template <bool OFF32>
 __global__ void __launch_bounds__(kBatchThreads)
     k_batch_spmm(const InstDesc *__restrict__ inst, const Item *__restrict__ items,
                  int64_t n_items, const SItem *__restrict__ sitems, int64_t n_sitems,
-                 const float *__restrict__ band, unsigned long long *__restrict__ counters,
-                 float alpha, float beta, int beta_nz) {
+                 unsigned long long *__restrict__ counters, float alpha, float beta,
+                 int beta_nz) {
   extern __shared__ float4 stage4[];
   __shared__ unsigned long long s_ticket;
   if (n_sitems > 0) {
@@ -359,7 +220,7 @@ __global__ void __launch_bounds__(kBatchThreads)
       if (t >= (unsigned long long)n_sitems)
         break;  // every thread read the same ticket: the whole CTA leaves
       const SItem w = sitems[t];
-      staged_item(w, inst[w.inst], reinterpret_cast<float *>(stage4), band, alpha, beta, beta_nz);
+      staged_item(w, inst[w.inst], reinterpret_cast<float *>(stage4), alpha, beta, beta_nz);
       __syncthreads();  // the stage and s_ticket are reused by the next item
     }
   }
@@ -384,14 +245,11 @@ __global__ void __launch_bounds__(kBatchThreads)
 
 // The column window of each block of rs rows of one instance: x = smallest
 // column, y = largest (INT32_MAX / INT32_MIN for a block without entries),
-// z = the block's entries, w = 1 when every row's columns are consecutive
-// (each entry's column is the previous entry's plus one). One CTA of 256
-// threads per block.
+// z = the block's entries. One CTA of 256 threads per block.
 __global__ void __launch_bounds__(256)
     k_block_window(int32_t m, int32_t rs, const int32_t *__restrict__ rp,
-                   const int2 *__restrict__ cv, int4 *__restrict__ out,
-                   int2 *__restrict__ dspan) {
-  __shared__ int s_lo[8], s_hi[8], s_dlo[8], s_dhi[8];
+                   const int2 *__restrict__ cv, int4 *__restrict__ out) {
+  __shared__ int s_lo[8], s_hi[8];
   const int64_t r0 = (int64_t)blockIdx.x * rs;
   const int64_t r1 = r0 + rs < (int64_t)m ? r0 + rs : (int64_t)m;
   const int32_t p0 = rp[r0], p1 = rp[r1];
@@ -401,66 +259,21 @@ __global__ void __launch_bounds__(256)
     lo = min(lo, c);
     hi = max(hi, c);
   }
-  // consecutive columns, and the diagonals (column - row) the rows reach
-  int consec = 1, dlo = INT32_MAX, dhi = INT32_MIN;
-  for (int64_t r = r0 + threadIdx.x; r < r1; r += 256) {
-    const int32_t s = rp[r], e = rp[r + 1];
-    if (s == e)
-      continue;
-    dlo = min(dlo, (int)(cv[s].x - r));
-    dhi = max(dhi, (int)(cv[e - 1].x - r));
-    for (int32_t q = s + 1; q < e && consec; ++q)
-      if (cv[q].x != cv[q - 1].x + 1)
-        consec = 0;
-  }
-  consec = __syncthreads_and(consec);
   for (int o = 16; o > 0; o >>= 1) {
     lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
     hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-    dlo = min(dlo, __shfl_xor_sync(0xffffffffu, dlo, o));
-    dhi = max(dhi, __shfl_xor_sync(0xffffffffu, dhi, o));
   }
   if ((threadIdx.x & 31) == 0) {
     s_lo[threadIdx.x >> 5] = lo;
     s_hi[threadIdx.x >> 5] = hi;
-    s_dlo[threadIdx.x >> 5] = dlo;
-    s_dhi[threadIdx.x >> 5] = dhi;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     for (int i = 1; i < 8; ++i) {
       lo = min(lo, s_lo[i]);
       hi = max(hi, s_hi[i]);
-      dlo = min(dlo, s_dlo[i]);
-      dhi = max(dhi, s_dhi[i]);
     }
-    out[blockIdx.x] = make_int4(lo, hi, p1 - p0, consec);
-    dspan[blockIdx.x] = make_int2(dlo, dhi);
-  }
-}
-
-// Band values of one band block per CTA (rows [r0, r1) of instance with
-// row pointers rp and entries cv): entry (r, column c) goes to
-// band[off + ((c - r - dmin) * ng + (r - r0) / 4) * 4 + (r - r0) % 4],
-// ng = ceil((r1 - r0) / 4); the buffer was zeroed.
-struct BandBlock {
-  const int32_t *rp;
-  const int2 *cv;
-  int32_t r0, r1, dmin, pad;
-  int64_t off;
-};
-
-__global__ void __launch_bounds__(256)
-    k_band_fill(const BandBlock *__restrict__ blocks, float *__restrict__ band) {
-  const BandBlock b = blocks[blockIdx.x];
-  const int32_t ng = (b.r1 - b.r0 + 3) / 4;
-  for (int32_t r = b.r0 + (int32_t)threadIdx.x; r < b.r1; r += 256) {
-    const int32_t g = (r - b.r0) / 4, i = (r - b.r0) % 4;
-    for (int32_t q = b.rp[r]; q < b.rp[r + 1]; ++q) {
-      const int2 t = b.cv[q];
-      const int64_t d = (int64_t)t.x - r - b.dmin;
-      band[b.off + (d * ng + g) * 4 + i] = __int_as_float(t.y);
-    }
+    out[blockIdx.x] = make_int4(lo, hi, p1 - p0, 0);
   }
 }
 
@@ -469,12 +282,6 @@ __global__ void k_pack_cv(int64_t nnz, const int32_t *__restrict__ col,
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < nnz)
     cv[i] = make_int2(col[i], __float_as_int(val[i]));
-}
-
-__global__ void k_unpack_v(int64_t nnz, const int2 *__restrict__ cv, float *__restrict__ vv) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nnz)
-    vv[i] = __int_as_float(cv[i].y);
 }
 
 // A BSR instance as scalar CSR rows. Row i of block row br holds, block by
@@ -524,8 +331,6 @@ struct perflibs_b200_batch_s {
   std::vector<double> work_per_row;  // nonzeros per row x k (for ordering)
   pls::DevBuf inst, items, counter;
   pls::DevBuf packed;  // every instance's (column, value) pairs, packed at creation
-  pls::DevBuf values;  // the same entries' values alone
-  pls::DevBuf band;    // band items' values, diagonal-major (SItem::band)
   pls::DevBuf scalar_rp;  // row pointers of the BSR instances' scalar rows
   pls::DevBuf sitems;     // staged items, largest first
   // Per instance, the row ranges left to the per-warp items when staged
@@ -533,8 +338,6 @@ struct perflibs_b200_batch_s {
   std::vector<std::vector<std::pair<int32_t, int32_t>>> warp_ranges;
   int64_t n_items = 0;
   int64_t n_sitems = 0;  // staged items built at creation
-  int64_t n_consec = 0;  // of which rows of consecutive columns (values read alone)
-  int64_t n_band = 0;    // of which band items (diagonal-major values)
   bool staging = true;   // run them (else every row goes to per-warp items)
   int32_t tile = 0;
   int grid = 0;
@@ -599,11 +402,8 @@ void build_staged(Batch *B) {
   const int32_t count = (int32_t)B->host.size();
   B->warp_ranges.assign(count, {});
   std::vector<std::pair<double, SItem>> v;
-  DevBuf win, span;
+  DevBuf win;
   std::vector<int4> hw;
-  std::vector<int2> hs;
-  std::vector<BandBlock> bands;
-  int64_t band_floats = 0;
   for (int32_t i = 0; i < count; ++i) {
     const InstDesc &d = B->host[i];
     auto &ranges = B->warp_ranges[i];
@@ -624,15 +424,10 @@ void build_staged(Batch *B) {
     const int32_t rs = wmax / 2;
     const int64_t nblk = div_up((int64_t)d.m, (int64_t)rs);
     win.reserve(sizeof(int4) * nblk);
-    span.reserve(sizeof(int2) * nblk);
-    k_block_window<<<(unsigned)nblk, 256, 0, B->stream>>>(d.m, rs, d.rp, d.cv, win.as<int4>(),
-                                                         span.as<int2>());
+    k_block_window<<<(unsigned)nblk, 256, 0, B->stream>>>(d.m, rs, d.rp, d.cv, win.as<int4>());
     PLS_LAUNCH_CHECK();
     hw.resize(nblk);
-    hs.resize(nblk);
     PLS_CUDA(cudaMemcpyAsync(hw.data(), win.p, sizeof(int4) * nblk, cudaMemcpyDeviceToHost,
-                             B->stream));
-    PLS_CUDA(cudaMemcpyAsync(hs.data(), span.p, sizeof(int2) * nblk, cudaMemcpyDeviceToHost,
                              B->stream));
     PLS_CUDA(cudaStreamSynchronize(B->stream));
     for (int64_t j = 0; j < nblk; ++j) {
@@ -643,30 +438,9 @@ void build_staged(Batch *B) {
         to_warps(r0, r1);
         continue;
       }
-      // A band block: consecutive columns, and its entries fill at least
-      // 3/4 of the diagonals its rows reach. With gap rows (tk <= 2) the
-      // window must still fit the stage.
-      const int2 ds = hs[j];
-      const int64_t nd = (int64_t)ds.y - ds.x + 1, rows = r1 - r0, ng = div_up(rows, (int64_t)4);
-      const bool gaps = ksp0 <= 8;
-      const bool band = b.w && ds.x <= ds.y && nd <= kBandMaxDiag &&
-                        4 * (int64_t)b.z >= 3 * rows * nd &&
-                        (!gaps || (w + (w - 1) / 4) * ksp0 <= kStageFloats);
-      int64_t boff = -1;
-      if (band) {
-        boff = band_floats;
-        band_floats += ng * nd * 4;
-        bands.push_back(BandBlock{d.rp, d.cv, r0, r1, ds.x, 0, boff});
-      }
       for (int32_t c0 = 0; c0 < d.k; c0 += kStageCols) {
         const int32_t ks = std::min(kStageCols, d.k - c0);
-        const SItem it{i,  r0,
-                       r1, b.x,
-                       (int32_t)w, c0,
-                       ks, (int32_t)div_up(ks, 4),
-                       b.w, band ? ds.x : 0,
-                       band ? (int32_t)nd : 0, band && gaps ? 1 : 0,
-                       boff};
+        const SItem it{i, r0, r1, b.x, (int32_t)w, c0, ks, (int32_t)div_up(ks, 4)};
         v.push_back({(double)b.z * it.tk + (double)w * it.tk, it});
       }
     }
@@ -676,20 +450,6 @@ void build_staged(Batch *B) {
   for (size_t j = 0; j < v.size(); ++j)
     items[j] = v[j].second;
   B->n_sitems = (int64_t)items.size();
-  B->n_consec = std::count_if(items.begin(), items.end(), [](const SItem &x) { return x.consec != 0; });
-  B->n_band = std::count_if(items.begin(), items.end(), [](const SItem &x) { return x.band >= 0; });
-  // The band blocks' diagonal-major values (zeros where a row has no entry).
-  B->band.reserve(sizeof(float) * std::max<int64_t>(band_floats, 4));
-  if (!bands.empty()) {
-    PLS_CUDA(cudaMemsetAsync(B->band.p, 0, sizeof(float) * band_floats, B->stream));
-    DevBuf bb;
-    bb.reserve(sizeof(BandBlock) * bands.size());
-    PLS_CUDA(cudaMemcpyAsync(bb.p, bands.data(), sizeof(BandBlock) * bands.size(),
-                             cudaMemcpyHostToDevice, B->stream));
-    k_band_fill<<<(unsigned)bands.size(), 256, 0, B->stream>>>(bb.as<BandBlock>(), B->band.as<float>());
-    PLS_LAUNCH_CHECK();
-    PLS_CUDA(cudaStreamSynchronize(B->stream));
-  }
   B->sitems.reserve(sizeof(SItem) * std::max<size_t>(items.size(), 1));
   if (!items.empty())
     PLS_CUDA(cudaMemcpyAsync(B->sitems.p, items.data(), sizeof(SItem) * items.size(),
@@ -712,7 +472,7 @@ void capture(Batch *B, float alpha, float beta) {
     const size_t smem = n_s > 0 ? sizeof(float) * kStageFloats : 0;
     kern<<<B->grid, kBatchThreads, smem, s>>>(
         B->inst.as<InstDesc>(), B->items.as<Item>(), B->n_items, B->sitems.as<SItem>(), n_s,
-        B->band.as<float>(), B->counter.as<unsigned long long>(), alpha, beta, beta != 0.f);
+        B->counter.as<unsigned long long>(), alpha, beta, beta != 0.f);
   }
   PLS_CUDA(cudaStreamEndCapture(s, &g));
   PLS_CUDA(cudaGraphInstantiate(&B->graph, g, 0));
@@ -813,8 +573,6 @@ perflibs_status_t perflibs_b200_batch_create(perflibs_b200_batch_t *out, int32_t
         srows += (int64_t)d.m + 1;
     }
     B->packed.reserve(sizeof(int2) * std::max<int64_t>(packed, 1));
-    B->values.reserve(sizeof(float) * std::max<int64_t>(packed, 1));
-    const int64_t n_entries = packed;
     B->scalar_rp.reserve(sizeof(int32_t) * std::max<int64_t>(srows, 1));
     packed = srows = 0;
     for (int32_t i = 0; i < count; ++i) {
@@ -838,12 +596,8 @@ perflibs_status_t perflibs_b200_batch_create(perflibs_b200_batch_t *out, int32_t
           k_pack_cv<<<(unsigned)div_up(nnz, 256), 256, 0, B->stream>>>(nnz, d.col, d.val, cv);
         packed += nnz;
       }
-      d.vv = B->values.as<float>() + (cv - B->packed.as<int2>());
       d.cv = cv;
     }
-    if (n_entries > 0)
-      k_unpack_v<<<(unsigned)div_up(n_entries, 256), 256, 0, B->stream>>>(
-          n_entries, B->packed.as<int2>(), B->values.as<float>());
     PLS_LAUNCH_CHECK();
     B->inst.reserve(sizeof(InstDesc) * count);
     PLS_CUDA(cudaMemcpyAsync(B->inst.p, B->host.data(), sizeof(InstDesc) * count,
@@ -948,17 +702,6 @@ perflibs_status_t perflibs_b200_batch_stage_info(perflibs_b200_batch_t B, int64_
     *staged_items = B->n_sitems;
   if (on)
     *on = B->staging ? 1 : 0;
-  return PERFLIBS_STATUS_SUCCESS;
-}
-
-perflibs_status_t perflibs_b200_batch_staged_kinds(perflibs_b200_batch_t B, int64_t *consecutive,
-                                                  int64_t *band) {
-  if (!B)
-    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
-  if (consecutive)
-    *consecutive = B->n_consec;
-  if (band)
-    *band = B->n_band;
   return PERFLIBS_STATUS_SUCCESS;
 }
 

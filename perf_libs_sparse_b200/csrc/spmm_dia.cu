@@ -414,9 +414,9 @@ void dia_launch(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64
 // contiguous for consecutive rows) arrive by one 1-D bulk copy into one of
 // two slabs, the next tile's while the current one computes.
 //
-// Threads. 256 threads: NV column lanes of one 16-byte vector each
+// Threads. 256 consumer threads: NV column lanes of one 16-byte vector each
 // (KS = NV * VEC columns) x 256 / NV row groups of kDiaRows rows, so
-// L = 1024 / NV. Per run of consecutive diagonals a thread reads its 4 + run
+// L = 1024 / NV; and one producer warp that issues the copies. Per run of consecutive diagonals a thread reads its 4 + run
 // - 1 window rows once from shared memory. Entries are added per row in
 // ascending offset, one fma each, with the epilogue alpha * acc + beta * C:
 // the order and arithmetic of k_spmm_dia, so the results are the same bits.
@@ -424,16 +424,10 @@ void dia_launch(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64
 // Work items are (segment of Z tiles of one chain, column slice), column
 // slice fastest so that the slices of a tile run together and its values
 // come from L2 after the first. Waits are bounded; a wait that runs out
-// sets the mapped error flag, waits (bounded) for the CTA's copies in flight
-// and ends the CTA, leaving its part of C unwritten; the host reports it on
-// the next call.
-
-// All threads wait for `bar`'s phase `parity`; true when every thread saw
-// it complete within the limit.
-__device__ __forceinline__ bool cta_wait(uint64_t *bar, uint32_t parity, int limit) {
-  const bool ok = tma::bar_wait_bounded(bar, parity, limit);
-  return __syncthreads_and(ok) != 0;
-}
+// sets the mapped error flag and stops the warp (the producer stops when a
+// slot is not released in time, then waits, bounded, for the copies in
+// flight before the CTA ends), leaving part of C unwritten; the host
+// reports it on the next call.
 
 // Shared-memory loads by 32-bit shared address (a constant part of the
 // address folds into the instruction's offset).
@@ -540,8 +534,16 @@ __device__ __forceinline__ DiaSlab dia_slab(int64_t R, int L, int nd) {
   return sl;
 }
 
+// Warp roles. NT = kDiaRows * kDiaTmaThreads / RB consumer threads
+// compute; one more warp issues the copies (its lane 0). Each window slot
+// has a full barrier (its copy landed) and an empty barrier (every consumer
+// warp is done with the window it holds), and so has each values slab. A
+// consumer warp waits only for the copies it reads and releases each window
+// after its last use, so the warps of a CTA never meet at a CTA-wide
+// barrier while they work; the producer refills a slot as soon as it is
+// released.
 template <class V, class X, int NV, int RB>
-__global__ void __launch_bounds__(kDiaRows * kDiaTmaThreads / RB, 1)
+__global__ void __launch_bounds__(kDiaRows * kDiaTmaThreads / RB + 32, 1)
     k_spmm_dia_tma(const __grid_constant__ CUtensorMap tmB, const DiaTmaArgs a,
                    const V *__restrict__ dv, const uint32_t *__restrict__ dfull,
                    X *__restrict__ C, int64_t ldc, X alpha, X beta, int beta_nz,
@@ -549,92 +551,141 @@ __global__ void __launch_bounds__(kDiaRows * kDiaTmaThreads / RB, 1)
   constexpr int VEC = 16 / (int)sizeof(X);
   constexpr int KS = NV * VEC;
   constexpr int NT = kDiaRows * kDiaTmaThreads / RB;
+  constexpr int NCW = NT / 32;  // consumer warps
   constexpr int L = NT / NV * RB;
   static_assert(L == kDiaTmaThreads / NV * kDiaRows, "the tile of the launch plan");
   static_assert(kDiaRows % RB == 0, "a thread's rows lie in one block");
+  static_assert(NT % 32 == 0, "whole consumer warps");
   using Acc = typename AccOf<V, X>::type;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t wbar[kDiaTmaMaxSlots];
-  __shared__ __align__(8) uint64_t vbar[2];
+  __shared__ __align__(8) uint64_t wfull[kDiaTmaMaxSlots], wempty[kDiaTmaMaxSlots];
+  __shared__ __align__(8) uint64_t vfull[2], vempty[2];
   // Tensor copies land on 128-byte boundaries: the launch adds 128 bytes so
   // that the slots can start at the first such boundary.
   unsigned char *smem = smem_raw + ((128u - (tma::smem_addr(smem_raw) & 127u)) & 127u);
   const int tid = threadIdx.x;
-  const int cl = tid % NV;
-  const int i0 = (tid / NV) * RB;
   unsigned char *vbase = smem + (size_t)a.S * a.slot_bytes;
-  const uint32_t full_mask = a.nd >= 32 ? 0xffffffffu : (1u << a.nd) - 1u;
   if (tid == 0) {
-    for (int s = 0; s < a.S; ++s)
-      tma::bar_init(&wbar[s]);
-    tma::bar_init(&vbar[0]);
-    tma::bar_init(&vbar[1]);
+    for (int s = 0; s < a.S; ++s) {
+      tma::bar_init(&wfull[s]);
+      tma::bar_init_count(&wempty[s], NCW);
+    }
+    for (int s = 0; s < 2; ++s) {
+      tma::bar_init(&vfull[s]);
+      tma::bar_init_count(&vempty[s], NCW);
+    }
     tma::bar_init_fence();
   }
   __syncthreads();
-  // Parity of the next phase of each barrier, and the copies issued but not
-  // yet waited for (the same in every thread).
-  uint32_t wph = 0, vph = 0, wpend = 0, vpend = 0;
-  const bool early = a.S > a.G;
 
-  for (int64_t item = blockIdx.x; item < a.n_items; item += gridDim.x) {
+  // Position of work item `item`: column slice k0, chain start b, rows of a
+  // tile inside the chain's period, tiles [t0, t1). False when empty.
+  struct Pos {
+    int k0, rows_tile, t0, t1;
+    int64_t b;
+  };
+  const auto item_pos = [&](int64_t item, Pos &p) {
     const int slice = (int)(item % a.n_slices);
     const int64_t rest = item / a.n_slices;
     const int chain = (int)(rest % a.n_chains);
     const int seg = (int)(rest / a.n_chains);
-    const int k0 = slice * KS;
-    const int64_t b = (int64_t)chain * L;
-    const int rows_tile = (int)min((int64_t)L, (int64_t)a.P - b);
-    const int64_t tiles = b < a.m ? ((int64_t)a.m - b + a.P - 1) / a.P : 0;
-    const int t0 = seg * a.Z;
-    const int t1 = (int)min((int64_t)t0 + a.Z, tiles);
-    if (t0 >= t1)
-      continue;
-    auto issue_window = [&](int w) {  // thread 0
-      const int s = w % a.S;
-      const int64_t row0 = b + (int64_t)w * a.P + a.win0;
-      tma::bar_expect_tx(&wbar[s], (uint32_t)(a.slot_bytes + a.tx_extra));
-      for (int j = 0; j < a.NB; ++j)
-        tma::tensor_load_2d(smem + (size_t)s * a.slot_bytes + (size_t)j * a.BR * KS * sizeof(X),
-                            &tmB, k0, (int32_t)(row0 + (int64_t)j * a.BR), &wbar[s]);
-    };
-    auto issue_vals = [&](int t) {  // thread 0
-      const int s = t & 1;
-      const DiaSlab sl = dia_slab<V>(b + (int64_t)t * a.P, L, a.nd);
-      unsigned char *slab = vbase + (size_t)s * a.vslab_bytes;
-      tma::bar_expect_tx(&vbar[s], (uint32_t)(sl.v_bytes + sl.f_bytes));
-      tma::bulk_load(slab, reinterpret_cast<const char *>(dv) + sl.v_lo, (uint32_t)sl.v_bytes,
-                     &vbar[s]);
-      tma::bulk_load(slab + sl.f_at, reinterpret_cast<const char *>(dfull) + sl.f_lo,
-                     (uint32_t)sl.f_bytes, &vbar[s]);
-    };
-    if (tid == 0) {
-      for (int g = 0; g < a.G; ++g)
-        issue_window(t0 + g);
-      issue_vals(t0);
-    }
-    for (int g = 0; g < a.G; ++g)
-      wpend |= 1u << ((t0 + g) % a.S);
-    vpend |= 1u << (t0 & 1);
+    p.k0 = slice * KS;
+    p.b = (int64_t)chain * L;
+    p.rows_tile = (int)min((int64_t)L, (int64_t)a.P - p.b);
+    const int64_t tiles = p.b < a.m ? ((int64_t)a.m - p.b + a.P - 1) / a.P : 0;
+    p.t0 = (int)((int64_t)seg * a.Z);
+    p.t1 = (int)min((int64_t)p.t0 + a.Z, tiles);
+    return p.t0 < p.t1;
+  };
 
-    for (int t = t0; t < t1; ++t) {
-      const int64_t R = b + (int64_t)t * a.P;
-      if (t + 1 < t1) {
-        if (tid == 0) {
-          if (early)
-            issue_window(t + a.G);
-          issue_vals(t + 1);
+  if (tid >= NT) {
+    // ---- producer (lane 0 of the last warp) ----
+    if (tid == NT) {
+      int nw[kDiaTmaMaxSlots], nv[2] = {0, 0};  // copies issued into each slot / slab
+      for (int s = 0; s < kDiaTmaMaxSlots; ++s)
+        nw[s] = 0;
+      bool ok = true;
+      for (int64_t item = blockIdx.x; ok && item < a.n_items; item += gridDim.x) {
+        Pos p;
+        if (!item_pos(item, p))
+          continue;
+        const auto issue_window = [&](int w) {
+          const int s = w % a.S;
+          if (nw[s] > 0 && !tma::bar_wait_bounded(&wempty[s], (uint32_t)(nw[s] - 1) & 1u, a.wait_limit))
+            return false;
+          ++nw[s];
+          const int64_t row0 = p.b + (int64_t)w * a.P + a.win0;
+          tma::bar_expect_tx(&wfull[s], (uint32_t)(a.slot_bytes + a.tx_extra));
+          for (int j = 0; j < a.NB; ++j)
+            tma::tensor_load_2d(smem + (size_t)s * a.slot_bytes + (size_t)j * a.BR * KS * sizeof(X),
+                                &tmB, p.k0, (int32_t)(row0 + (int64_t)j * a.BR), &wfull[s]);
+          return true;
+        };
+        const auto issue_vals = [&](int t) {
+          const int s = t & 1;
+          if (nv[s] > 0 && !tma::bar_wait_bounded(&vempty[s], (uint32_t)(nv[s] - 1) & 1u, a.wait_limit))
+            return false;
+          ++nv[s];
+          const DiaSlab sl = dia_slab<V>(p.b + (int64_t)t * a.P, L, a.nd);
+          unsigned char *slab = vbase + (size_t)s * a.vslab_bytes;
+          tma::bar_expect_tx(&vfull[s], (uint32_t)(sl.v_bytes + sl.f_bytes));
+          tma::bulk_load(slab, reinterpret_cast<const char *>(dv) + sl.v_lo, (uint32_t)sl.v_bytes,
+                         &vfull[s]);
+          tma::bulk_load(slab + sl.f_at, reinterpret_cast<const char *>(dfull) + sl.f_lo,
+                         (uint32_t)sl.f_bytes, &vfull[s]);
+          return true;
+        };
+        // Tile t reads values(t) and windows t .. t + G - 1, in that order
+        // of need; window w's slot held window w - S, released by tile w - S.
+        ok = issue_vals(p.t0);
+        for (int g = 0; ok && g < a.G; ++g)
+          ok = issue_window(p.t0 + g);
+        for (int t = p.t0 + 1; ok && t < p.t1; ++t) {
+          ok = issue_vals(t);
+          if (ok)
+            ok = issue_window(t + a.G - 1);
         }
-        if (early)
-          wpend |= 1u << ((t + a.G) % a.S);
-        vpend |= 1u << ((t + 1) & 1);
       }
-      const int vs = t & 1;
-      if (!cta_wait(&vbar[vs], (vph >> vs) & 1u, a.wait_limit))
-        goto failed;
-      vph ^= 1u << vs;
-      vpend &= ~(1u << vs);
-      {
+      if (!ok) {
+        // A slot was not released in time: record it and give the copies
+        // in flight a bounded wait (the shared memory must outlive them).
+        *(volatile int *)err = 1;
+        __threadfence_system();
+      }
+      for (int s = 0; s < a.S; ++s)
+        if (nw[s] > 0)
+          tma::bar_wait_bounded(&wfull[s], (uint32_t)(nw[s] - 1) & 1u, a.wait_limit);
+      for (int s = 0; s < 2; ++s)
+        if (nv[s] > 0)
+          tma::bar_wait_bounded(&vfull[s], (uint32_t)(nv[s] - 1) & 1u, a.wait_limit);
+    }
+  } else {
+    // ---- consumers ----
+    const int lane = tid & 31;
+    const int cl = tid % NV;
+    const int i0 = (tid / NV) * RB;
+    const uint32_t full_mask = a.nd >= 32 ? 0xffffffffu : (1u << a.nd) - 1u;
+    uint32_t wph = 0, vph = 0;  // parity of the next phase of each full barrier
+    bool ok = true;
+    // A warp-wide bounded wait (the whole warp takes the same decision).
+    const auto wait = [&](uint64_t *bar, uint32_t parity) {
+      return __all_sync(0xffffffffu, tma::bar_wait_bounded(bar, parity, a.wait_limit)) != 0;
+    };
+    const auto release = [&](uint64_t *bar) {
+      __syncwarp();
+      if (lane == 0)
+        tma::bar_arrive(bar);
+    };
+    for (int64_t item = blockIdx.x; ok && item < a.n_items; item += gridDim.x) {
+      Pos p;
+      if (!item_pos(item, p))
+        continue;
+      for (int t = p.t0; t < p.t1; ++t) {
+        const int64_t R = p.b + (int64_t)t * a.P;
+        const int vs = t & 1;
+        if (!(ok = wait(&vfull[vs], (vph >> vs) & 1u)))
+          break;
+        vph ^= 1u << vs;
         Acc acc[RB][VEC];
 #pragma unroll
         for (int i = 0; i < RB; ++i)
@@ -651,11 +702,10 @@ __global__ void __launch_bounds__(kDiaRows * kDiaTmaThreads / RB, 1)
         const bool checked = (blk_full & full_mask) != full_mask;
         for (int g = 0; g < a.G; ++g) {
           const int s = (t + g) % a.S;
-          if (t == t0 || g == a.G - 1) {  // the window's first use
-            if (!cta_wait(&wbar[s], (wph >> s) & 1u, a.wait_limit))
-              goto failed;
+          if (t == p.t0 || g == a.G - 1) {  // the window's first use in this item
+            if (!(ok = wait(&wfull[s], (wph >> s) & 1u)))
+              break;
             wph ^= 1u << s;
-            wpend &= ~(1u << s);
           }
           constexpr int ROW = KS * (int)sizeof(X);
           const uint32_t wrow = tma::smem_addr(smem + (size_t)s * a.slot_bytes) +
@@ -664,19 +714,20 @@ __global__ void __launch_bounds__(kDiaRows * kDiaTmaThreads / RB, 1)
             dia_tma_group<true, V, X, Acc, VEC, ROW, RB>(a, g, wrow, vrow, acc);
           else
             dia_tma_group<false, V, X, Acc, VEC, ROW, RB>(a, g, wrow, vrow, acc);
-          if (g == 0 && !early && t + 1 < t1) {
-            __syncthreads();  // every thread is done with PW(t): its slot takes PW(t + G)
-            if (tid == 0)
-              issue_window(t + a.G);
-            wpend |= 1u << ((t + a.G) % a.S);
-          }
+          // Window t ends its use with group 0 of tile t; on the item's last
+          // tile every window it holds ends its use.
+          if (g == 0 || t == p.t1 - 1)
+            release(&wempty[s]);
         }
-        const int col = k0 + cl * VEC;
+        if (!ok)
+          break;
+        release(&vempty[vs]);
+        const int col = p.k0 + cl * VEC;
         if (col < a.k) {
 #pragma unroll
           for (int i = 0; i < RB; ++i) {
             const int64_t row = R + i0 + i;
-            if (i0 + i < rows_tile && row < a.m) {
+            if (i0 + i < p.rows_tile && row < a.m) {
               X *cp = C + row * ldc + col;
               X out[VEC];
               if (beta_nz) {
@@ -695,23 +746,13 @@ __global__ void __launch_bounds__(kDiaRows * kDiaTmaThreads / RB, 1)
           }
         }
       }
-      __syncthreads();  // the values slab and the windows are free for the next copies
     }
-  }
-  return;
-
-failed:
-  // A copy did not land in time: record it, give the CTA's copies in flight
-  // another bounded wait (its shared memory must outlive them) and stop.
-  if (tid == 0) {
-    *(volatile int *)err = 1;
-    __threadfence_system();
-    for (int s = 0; s < a.S; ++s)
-      if (wpend & (1u << s))
-        tma::bar_wait_bounded(&wbar[s], (wph >> s) & 1u, a.wait_limit);
-    for (int s = 0; s < 2; ++s)
-      if (vpend & (1u << s))
-        tma::bar_wait_bounded(&vbar[s], (vph >> s) & 1u, a.wait_limit);
+    if (!ok && lane == 0) {
+      // A copy did not land in time: record it; this warp stops (the
+      // producer drains the copies in flight before the CTA ends).
+      *(volatile int *)err = 1;
+      __threadfence_system();
+    }
   }
   __syncthreads();
 }
@@ -739,7 +780,7 @@ template <class V, class X, int NV>
 void dia_tma_run(const DiaDev &d, const DiaTmaShape &sh, const CUtensorMap &map, X *C,
                  int64_t ldc, X alpha, X beta, int sms, cudaStream_t s) {
   constexpr int RB = kDiaTmaThreadRows;
-  constexpr int NT = kDiaRows * kDiaTmaThreads / RB;
+  constexpr int NT = kDiaRows * kDiaTmaThreads / RB + 32;  // consumers + the producer warp
   auto kern = k_spmm_dia_tma<V, X, NV, RB>;
   const size_t smem = sh.smem + 128;  // room to align the slots (see the kernel)
   PLS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -173,17 +173,6 @@ def test_batch_staged_items_against_oracle_and_per_warp_items():
         mats.append(pls.SpMat.bsr(pls.ROW_MAJOR, nb * bs, nb * bs, bs, rp, col, blocks.reshape(-1)))
         descs.append(dict(kind="bsr", row_ptr=rp, col=col, vals=blocks.reshape(-1), bs=bs,
                           layout=pls.ROW_MAJOR, m=nb * bs, n=nb * bs, k=k, ldb=k, ldc=k))
-    # A band with every other column dropped: narrow windows (staged) whose
-    # rows' columns are not consecutive (the general staged reader).
-    n, hb = 3000, 24
-    rp, c, v = _banded(n, hb, rng)
-    keep = (c % 2) == 0
-    rows = np.repeat(np.arange(n), np.diff(rp))
-    rp = np.zeros(n + 1, np.int32)
-    rp[1:] = np.cumsum(np.bincount(rows[keep], minlength=n))
-    c, v = c[keep], v[keep]
-    mats.append(pls.SpMat.csr(n, n, rp, c, v))
-    descs.append(dict(kind="csr", row_ptr=rp, col=c, vals=v, m=n, n=n, k=20, ldb=20, ldc=20))
     m = 5000
     rp, c, v = W.random_csr(m, m, 10, rng)
     v = v.astype(np.float32)
@@ -203,12 +192,6 @@ def test_batch_staged_items_against_oracle_and_per_warp_items():
                    [cm.data_ptr() for cm in Cs], [d["ldc"] for d in descs], stream=s.cuda_stream)
     info = bt.stage_info()
     assert info["staged_items"] > 0 and info["staging"]
-    # the bands and the block-diagonal blocks have consecutive columns, the
-    # band with every other column does not; the full bands (not the
-    # block-diagonal blocks, which fill 8 of 15 diagonals) are band items,
-    # with gap rows in the stage for k <= 8
-    kinds = bt.staged_kinds()
-    assert 0 < kinds["band"] < kinds["consecutive"] < info["staged_items"], kinds
 
     def check(alpha, beta):
         for cm, c0 in zip(Cs, C0s):
