@@ -312,19 +312,22 @@ def time_spmm_kernels(A: SpMat, k: int, reps: int = 3) -> list:
 
     Bd = torch.randn((A.n, k), dtype=torch.float64, device="cuda")
     Cd = torch.empty((A.m, k), dtype=torch.float64, device="cuda")
+    # the SpMMs and both events on one stream, so that the events bracket them
+    st = torch.cuda.current_stream()
+    sp = st.cuda_stream
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     out = []
     for cls, path in enumerate(SPMM_FORCE):
         A.set_spmm_path(path)
-        A.spmm_dev(Bd.data_ptr(), k, k, Cd.data_ptr(), k, 1.0, 0.0)
+        A.spmm_dev(Bd.data_ptr(), k, k, Cd.data_ptr(), k, 1.0, 0.0, sp)
         torch.cuda.synchronize()
         if A.spmm_info()["path"] != path:
             out.append(float("inf"))
             continue
-        e0.record()
+        e0.record(st)
         for _ in range(reps):
-            A.spmm_dev(Bd.data_ptr(), k, k, Cd.data_ptr(), k, 1.0, 0.0)
-        e1.record()
+            A.spmm_dev(Bd.data_ptr(), k, k, Cd.data_ptr(), k, 1.0, 0.0, sp)
+        e1.record(st)
         torch.cuda.synchronize()
         out.append(e0.elapsed_time(e1) / reps)
     A.set_spmm_path(-1)
