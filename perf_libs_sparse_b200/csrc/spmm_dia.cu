@@ -757,25 +757,6 @@ __global__ void __launch_bounds__(kDiaRows * kDiaTmaThreads / RB + 32, 1)
   __syncthreads();
 }
 
-// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
-// to the driver library); null if the driver does not offer it.
-using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
-                                   const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
-                                   const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-EncodeTiledFn encode_tiled() {
-  static const EncodeTiledFn fn = [] {
-    void *p = nullptr;
-    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
-            cudaSuccess ||
-        q != cudaDriverEntryPointSuccess)
-      return (EncodeTiledFn) nullptr;
-    return reinterpret_cast<EncodeTiledFn>(p);
-  }();
-  return fn;
-}
-
 template <class V, class X, int NV>
 void dia_tma_run(const DiaDev &d, const DiaTmaShape &sh, const CUtensorMap &map, X *C,
                  int64_t ldc, X alpha, X beta, int sms, cudaStream_t s) {
@@ -801,7 +782,7 @@ bool dia_tma_launch(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64_t
   PLS_CUDA(cudaGetDevice(&dev));
   PLS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   DiaTmaShape sh = dia_tma_shape(d.offs, d.nd, m, k, (int)sizeof(X), (int)sizeof(V), sms);
-  const EncodeTiledFn enc = encode_tiled();
+  const tma::EncodeTiledFn enc = tma::encode_tiled();
   if (!sh.ok || !enc || c.ncols <= 0 || (uintptr_t)d.vals.p % 16)
     return false;
   // B as a 2-D tensor (k columns innermost, ncols rows of ldb elements),

@@ -312,8 +312,12 @@ def time_spmm_kernels(A: SpMat, k: int, reps: int = 3) -> list:
 
     Bd = torch.randn((A.n, k), dtype=torch.float64, device="cuda")
     Cd = torch.empty((A.m, k), dtype=torch.float64, device="cuda")
-    # the SpMMs and both events on one stream, so that the events bracket them
-    st = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    # The SpMMs and both events on one explicit stream, so that the events
+    # bracket them: a null stream handle would send the SpMMs to the
+    # handle's own stream, which the legacy default stream's events do not
+    # order against.
+    st = torch.cuda.Stream()
     sp = st.cuda_stream
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     out = []
