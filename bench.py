@@ -145,12 +145,17 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
-def load_traffic(workload: str):
+def load_traffic(workload: str, kernel: str):
+    """DRAM bytes (read + write) of one launch of the configuration's
+    dominant kernel, from the ncu capture summarised in
+    profiles/traffic.json, or None when that file holds no capture of this
+    kernel and layout (`kernel` names both, as the file records them)."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(p):
         with open(p) as f:
-            d = json.load(f)
-        return d.get(workload)
+            d = json.load(f).get(workload)
+        if isinstance(d, dict) and d.get("kernel") == kernel:
+            return d.get("bytes")
     return None
 
 
@@ -382,11 +387,13 @@ def c1_config(args, timer, sp):
         err = max(spmv_rel_err(y.cpu().numpy(), rp, c, v, x)[0] for y in (ys[0], ys[-1]))
         cfg = mats[0].config()
         gbs = b / ms / 1e6
-        out = {"kernel": (f"CSR threads-per-row {cfg['tpr']}" if cfg["kind"] == pls.KIND_CSR
-                          else f"{KIND_NAMES[cfg['kind']]} C={cfg['C']} sigma={cfg['sigma']}"),
+        kname = (f"CSR threads-per-row {cfg['tpr']}" if cfg["kind"] == pls.KIND_CSR
+                 else f"{KIND_NAMES[cfg['kind']]} C={cfg['C']} sigma={cfg['sigma']}")
+        out = {"kernel": kname,
                "value": gbs, "unit": "GB/s", "ms_per_step": ms, "steps": rounds * R,
                "gflops": 2.0 * nnz / ms / 1e6, "max_rel_err": err, "tolerance": 1e-12,
-               "graph": graph is not None, "roofline": roofline(gbs)}
+               "graph": graph is not None,
+               "roofline": roofline(gbs, load_traffic("c1_spmv_fp64", kname))}
         del graph
         for A in mats:
             A.destroy()
@@ -411,6 +418,7 @@ def c3_config(args, timer, sp, arms):
     import torch
 
     import perf_libs_sparse_b200 as pls
+    from perf_libs_sparse_b200 import selector as selmod
 
     m, n, rp, c, v = W.stencil_27pt(128, seed=2)
     nnz = int(rp[-1])
@@ -448,6 +456,31 @@ def c3_config(args, timer, sp, arms):
         b = W.algorithmic_bytes_spmm(m, n, nnz, k, sv, sb, False)
         gbs = b / ms / 1e6
         info = A.spmm_info()
+        # The learned SpMM kernel selector on the same call: its first SpMM
+        # runs the predicted kernel without timing the candidates.
+        sel = None
+        sels = selmod.default_spmm_selectors()
+        if sels is not None and getattr(args, "spmm_path", None) is None:
+            As = pls.SpMat.csr(m, n, rp, c, v.astype(dt))
+            As.set_storage({"native": pls.STORAGE_NATIVE, "fp32": pls.STORAGE_FP32,
+                            "bf16": pls.STORAGE_BF16}[storage])
+            As.set_stream(sp)
+            selmod.attach_spmm_selectors(As, sels)
+            assert As.optimize() == 0
+            t0 = time.perf_counter()
+            As.spmm_dev(Bd.data_ptr(), k, k, Cd.data_ptr(), k, 1.0, 0.0, sp)
+            torch.cuda.synchronize()
+            t_pred = time.perf_counter() - t0
+            pth = As.spmm_info()["path"]
+            sel = {"kernel": SPMM_PATHS.get(pth, str(pth)), "same_as_measured": pth == info["path"],
+                   "first_call_s": t_pred}
+            if pth != info["path"]:
+                ms_p = timer(lambda: As.spmm_dev(Bd.data_ptr(), k, k, Cd.data_ptr(), k, 1.0, 0.0, sp),
+                             K, max(args.warmup, 3))
+                sel.update({"ms_per_step": ms_p, "regret_vs_measured": ms_p / ms - 1.0})
+            else:
+                sel["regret_vs_measured"] = 0.0
+            As.destroy()
         out["arms"].append({
             "k": k, "storage": storage,
             "dtype": {"native": "f64", "fp32": "f32 values, B and C; f32 accumulate",
@@ -457,8 +490,9 @@ def c3_config(args, timer, sp, arms):
             "tolerance": {"native": 1e-12, "fp32": 1e-5, "bf16": 1e-2}[storage],
             "rows_checked": "all" if full else "8 blocks of 16384 rows",
             "kernel": SPMM_PATHS.get(info["path"], str(info["path"])),
-            "first_call_s": t_choice, "algorithmic_bytes_per_step": b,
-            "roofline": roofline(gbs)})
+            "first_call_s": t_choice, "selector": sel, "algorithmic_bytes_per_step": b,
+            "roofline": roofline(gbs, load_traffic(f"c3_spmm_k{k}_{storage}",
+                                                   SPMM_PATHS.get(info["path"], "")))})
         del Bd, Cd
         A.destroy()
     return out
@@ -507,13 +541,15 @@ def c4_config(args, timer, sp):
         worst = max(worst, float((np.abs(Cd.cpu().numpy().astype(np.float64) - ref) / den).max()))
     b = sum(W.algorithmic_bytes_spmm(d["m"], d["n"], W.instance_nnz(d), d["k"], 4, 4, False) for d in inst)
     gbs = b / ms / 1e6
+    si = bt.stage_info()
+    ktag = f"k_batch_spmm tile={tile} staging={bool(si.get('staging'))}"
     out = {"workload": "C4 512 uneven FP32 instances (banded / random / BSR bs 4-8), n in [1024, 65536], "
                        "k in [1, 64], one persistent launch per step",
            "value": gbs, "unit": "GB/s", "ms_per_step": ms, "steps": K, "max_rel_err": worst,
            "tolerance": 1e-5, "rows_checked": "all instances, all rows",
-           "tile_rows": tile, **bt.info(), **bt.stage_info(),
+           "tile_rows": tile, **bt.info(), **si,
            "rows_total": int(sum(d["m"] for d in inst)), "algorithmic_bytes_per_step": b,
-           "roofline": roofline(gbs)}
+           "roofline": roofline(gbs, load_traffic("c4_batch_fp32", ktag))}
     bt.destroy()
     for A in mats:
         A.destroy()
@@ -763,7 +799,8 @@ def run_b200(args):
         "e2e": {"value": replica_gbs(bytes_step, e2e_s, world), "unit": "GB/s",
                 "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": m * 8, "ms_per_step": e2e_s * 1e3,
                 "row_bands": e2e_bands, "max_rel_err": e2e_err},
-        "roofline": roofline(achieved, load_traffic("c2_spmv_fp64")),
+        "roofline": roofline(achieved, load_traffic(
+            "c2_spmv_fp64", f"k_sell C={cfg['C']} sigma={cfg['sigma']}" if cfg["kind"] == 1 else "")),
         "gpu_launches": K * kernels_per_step,
         "clocks": clk.summary(),
     }
@@ -796,7 +833,8 @@ def run_b200(args):
 def run_extra(args):
     """One configuration alone, as its own JSON line (N = 1): c1, c3 (k =
     --k, storage --storage), c4, c3spmv (FP64 SpMV, tuned, on C3's
-    matrix: the structured counterpart of C2) or c2local (C2's row lengths
+    matrix: the structured counterpart of C2), lap2d (FP64 SpMV, tuned, on
+    the 5-point Laplacian 4096^2) or c2local (C2's row lengths
     with every column drawn from 8192, so that x's gathers hit L1: what the
     C2 kernel does without its L2 gathers). The default line carries
     c1 / c3 / c4 too; these lines are for profiling one kernel."""
@@ -824,6 +862,12 @@ def run_extra(args):
             x = W.uniform_vector(n, 1)
             what = (f"C2's Zipf row lengths with columns from 8192 (x in L1) m={m} nnz={int(rp[-1])}, "
                     "FP64 SpMV: the C2 kernel without its L2 gathers")
+        elif args.workload == "lap2d":
+            # the C1 operator on a 4096 x 4096 grid: a structured SpMV large
+            # enough (0.3 GB) to stream at HBM speed
+            m, n, rp, c, v = W.laplacian_2d(4096)
+            x = W.uniform_vector(n, 0)
+            what = f"5-point Laplacian 4096^2 n={m} nnz={int(rp[-1])}, FP64 SpMV"
         else:
             m, n, rp, c, v = W.stencil_27pt(128, seed=2)
             x = W.uniform_vector(n, 2)
@@ -831,6 +875,11 @@ def run_extra(args):
         A = pls.SpMat.csr(m, n, rp, c, v)
         A.set_stream(sp)
         A.hint(pls.HINT_SPMV_INVOCATIONS, pls.INVOCATIONS_MANY)
+        if args.sell_config:
+            # a given SELL layout instead of the tuner's pick (to compare one
+            # layout across matrices)
+            C_, sigma = (int(t) for t in args.sell_config.split(","))
+            assert A.force_config(pls.KIND_SELL, C_, sigma, 0) == 0
         assert A.optimize() == 0
         P = pls.SpMat.csr(m, n, rp, c, v)
         P.set_stream(sp)
@@ -871,10 +920,12 @@ def emit(line, args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="c2",
-                    choices=["c1", "c2", "c3", "c3spmv", "c2local", "c4", "bsr8"],
+                    choices=["c1", "c2", "c3", "c3spmv", "c2local", "lap2d", "c4", "bsr8"],
                     help="c2 (default: the headline line, with c1 / c3 / c4 inside it) or one "
                          "configuration alone")
     ap.add_argument("--k", type=int, default=32, help="right-hand sides for --workload c3")
+    ap.add_argument("--sell-config", default=None,
+                    help="C,sigma: SELL layout for --workload c2local / c3spmv instead of the tuner's")
     ap.add_argument("--storage", default="native", choices=["native", "fp32", "bf16"])
     ap.add_argument("--spmm-path", type=int, default=None,
                     help="--workload c3: force one SpMM kernel (perflibs_b200_spmat_set_spmm_path)")

@@ -10,6 +10,7 @@
 //
 // BSR: a warp per block row, lanes over C's columns; each lane keeps bs
 // accumulators (one per scalar row of the block row).
+#include <cstring>
 #include <type_traits>
 
 #include "common.cuh"
@@ -380,6 +381,110 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// bs values of one block row (row-major blocks) or block column
+// (column-major blocks), loaded as whole vectors: bs * sizeof(V) bytes, at an
+// offset that is a multiple of that size.
+template <int BS, class V>
+__device__ __forceinline__ void ld_block_line(const V *p, V (&a)[BS]) {
+  constexpr int bytes = BS * (int)sizeof(V);
+  if constexpr (bytes >= 16) {
+#pragma unroll
+    for (int h = 0; h < bytes / 16; ++h) {
+      const uint4 t = __ldg(reinterpret_cast<const uint4 *>(p) + h);
+      memcpy(reinterpret_cast<char *>(a) + 16 * h, &t, 16);
+    }
+  } else if constexpr (bytes == 8) {
+    const uint2 t = __ldg(reinterpret_cast<const uint2 *>(p));
+    memcpy(a, &t, 8);
+  } else {
+    static_assert(bytes == 4, "block lines of 4, 8 or a multiple of 16 bytes");
+    const unsigned t = __ldg(reinterpret_cast<const unsigned *>(p));
+    memcpy(a, &t, 4);
+  }
+}
+
+// Block size 2 / 4 / 8 with 16-byte vectors of B and C: TK = 2^lg_tk lanes
+// per block row, each owning one vector of VEC columns per pass, 32 / TK
+// block rows per warp. Per block, a lane loads its vector of the block's BS
+// rows of B (independent 16-byte loads, issued together) and the block's
+// values a line at a time (the same addresses across the block row's
+// lanes), then adds, for every row i of the block, a_ij * B_j in ascending
+// j: per element of C the order of the scalar kernel above, blocks in stored
+// order and columns of a block ascending, so the results are the same bits.
+template <int BS, bool RM, class V, class X, int VEC>
+__global__ void __launch_bounds__(256)
+    k_spmm_bsr_vec(int32_t mb, const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+                   const V *__restrict__ val, const X *__restrict__ B, int64_t ldb,
+                   X *__restrict__ C, int64_t ldc, int k, int lg_tk, X alpha, X beta,
+                   int beta_nz) {
+  using Acc = typename AccOf<V, X>::type;
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t br = g >> lg_tk;
+  if (br >= mb)
+    return;
+  const int tk = (int)(g & ((1 << lg_tk) - 1));
+  const int32_t b0 = __ldg(rp + br), b1 = __ldg(rp + br + 1);
+  for (int kk = tk * VEC; kk < k; kk += VEC << lg_tk) {
+    Acc acc[BS][VEC];
+#pragma unroll
+    for (int i = 0; i < BS; ++i)
+#pragma unroll
+      for (int v = 0; v < VEC; ++v)
+        acc[i][v] = Acc(0);
+    for (int32_t b = b0; b < b1; ++b) {
+      const X *bb = B + (int64_t)__ldg(col + b) * BS * ldb + kk;
+      X bv[BS][VEC];
+#pragma unroll
+      for (int j = 0; j < BS; ++j)
+        ld_vec<X, VEC>(bb + (int64_t)j * ldb, bv[j]);
+      const V *ab = val + (int64_t)b * BS * BS;
+      if constexpr (RM) {
+#pragma unroll
+        for (int i = 0; i < BS; ++i) {
+          V a[BS];
+          ld_block_line<BS, V>(ab + i * BS, a);
+#pragma unroll
+          for (int j = 0; j < BS; ++j) {
+            const Acc aij = to_acc<Acc>(a[j]);
+#pragma unroll
+            for (int v = 0; v < VEC; ++v)
+              acc[i][v] = fma(aij, to_acc<Acc>(bv[j][v]), acc[i][v]);
+          }
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < BS; ++j) {
+          V a[BS];
+          ld_block_line<BS, V>(ab + j * BS, a);
+#pragma unroll
+          for (int i = 0; i < BS; ++i) {
+            const Acc aij = to_acc<Acc>(a[i]);
+#pragma unroll
+            for (int v = 0; v < VEC; ++v)
+              acc[i][v] = fma(aij, to_acc<Acc>(bv[j][v]), acc[i][v]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < BS; ++i) {
+      X *cp = C + (br * BS + i) * ldc + kk;
+      X o[VEC];
+#pragma unroll
+      for (int v = 0; v < VEC; ++v)
+        o[v] = (X)acc[i][v] * alpha;
+      if (beta_nz) {  // the scalar kernel's epilogue, element for element
+        X old[VEC];
+        ld_vec_plain<X, VEC>(cp, old);
+#pragma unroll
+        for (int v = 0; v < VEC; ++v)
+          o[v] += beta * old[v];
+      }
+      st_vec<X, VEC>(cp, o);
+    }
+  }
+}
+
 // Any block size: a thread per (scalar row, column).
 template <class V, class X>
 __global__ void k_spmm_bsr_generic(int32_t mb, int bs, int layout,
@@ -423,6 +528,31 @@ static void spmm_bsr_fma(const BsrDev &b, const X *B, int64_t ldb, X *C, int64_t
     if constexpr (std::is_same_v<X, float> && std::is_same_v<V, double>) {
       throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE, "FP64 storage with FP32 API");
     } else {
+      constexpr int VEC = 16 / (int)sizeof(X);
+      if ((b.bs == 2 || b.bs == 4 || b.bs == 8) && k % VEC == 0 && ldb % VEC == 0 &&
+          ldc % VEC == 0 && (uintptr_t)B % 16 == 0 && (uintptr_t)C % 16 == 0) {
+        const int cols = k / VEC;
+        int lg_tk = 0;
+        while ((1 << lg_tk) < cols && lg_tk < 5)
+          ++lg_tk;
+        const unsigned grid = (unsigned)div_up((int64_t)b.mb << lg_tk, 256);
+        const bool rm = b.layout == PERFLIBS_ROW_MAJOR;
+        auto go = [&](auto bs_tag, auto rm_tag) {
+          constexpr int BS = decltype(bs_tag)::value;
+          constexpr bool RM = decltype(rm_tag)::value;
+          k_spmm_bsr_vec<BS, RM, V, X, VEC><<<grid, 256, 0, s>>>(
+              b.mb, b.row_ptr.as<int32_t>(), b.col.as<int32_t>(), (const V *)b.ev(), B, ldb, C,
+              ldc, k, lg_tk, alpha, beta, bnz);
+        };
+        using T = std::true_type;
+        using F = std::false_type;
+        switch (b.bs) {
+        case 2: rm ? go(std::integral_constant<int, 2>{}, T{}) : go(std::integral_constant<int, 2>{}, F{}); break;
+        case 4: rm ? go(std::integral_constant<int, 4>{}, T{}) : go(std::integral_constant<int, 4>{}, F{}); break;
+        default: rm ? go(std::integral_constant<int, 8>{}, T{}) : go(std::integral_constant<int, 8>{}, F{}); break;
+        }
+        return;
+      }
       const unsigned blocks = (unsigned)div_up(b.mb, 8);
       switch (b.bs) {
       case 2:
