@@ -373,8 +373,8 @@ __global__ void __launch_bounds__(256)
       for (int i = 0; i < BS; ++i) {
         X *cp = C + (br * BS + i) * ldc + j;
         X o = (X)acc[i] * alpha;
-        if (beta_nz)
-          o += beta * *cp;
+        if (beta_nz)  // an explicit fma: the vector kernel below rounds the same way
+          o = fma(beta, *cp, o);
         *cp = o;
       }
     }
@@ -478,7 +478,7 @@ __global__ void __launch_bounds__(256)
         ld_vec_plain<X, VEC>(cp, old);
 #pragma unroll
         for (int v = 0; v < VEC; ++v)
-          o[v] += beta * old[v];
+          o[v] = fma(beta, old[v], o[v]);
       }
       st_vec<X, VEC>(cp, o);
     }

@@ -222,6 +222,20 @@ __device__ __forceinline__ void dia_run(const X *bp, int64_t ldb, int64_t br0, i
   }
 }
 
+// Line patches. On a grid stencil the diagonals come in runs one grid line
+// (Ly rows) apart, so the runs of row r at offset +Ly read the rows of B that
+// the runs of row r + Ly read at offset 0. A CTA of consecutive rows shares
+// only the overlap inside each run through L1; the rows Ly away belong to
+// other CTAs on other SMs, and each brings B's rows from L2 again. Where the
+// host finds such a line stride (the smallest gap of at least 16 rows
+// between consecutive run centres), each CTA instead takes a patch of
+// kDiaLines lines x (its row blocks / kDiaLines) consecutive row blocks, so
+// the lines it holds read each other's rows of B from L1. The patches tile
+// the first patch_rbs row blocks (whole groups of kDiaLines lines); the rest
+// keep consecutive row blocks. Every thread computes the same block of rows
+// either way, so the results do not change.
+constexpr int kDiaLines = 4;
+
 // Threads: (block of kDiaRows rows) x (TK column vectors of VEC); a thread
 // loops over C's columns in steps of TK * VEC. MASK (threads that make more
 // than one pass over the columns): the block's full-diagonal mask is loaded
@@ -234,11 +248,19 @@ __global__ void __launch_bounds__(256, 4)  // 64 registers: 4 blocks per SM
     k_spmm_dia(int32_t m, int32_t n, int nd, DiaRuns runs, const V *__restrict__ dv,
                const uint32_t *__restrict__ dfull, uint32_t full_mask,
                const X *__restrict__ B, int64_t ldb, X *__restrict__ C, int64_t ldc, int k,
-               int lg_tk, X alpha, X beta, int beta_nz) {
+               int lg_tk, int64_t patch_rbs, int32_t ly_rb, int lg_seg, X alpha, X beta,
+               int beta_nz) {
   constexpr int RB = kDiaRows;
   using Acc = typename AccOf<V, X>::type;
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t rb = g >> lg_tk;
+  int64_t rb = g >> lg_tk;
+  if (((int64_t)blockIdx.x * blockDim.x >> lg_tk) < patch_rbs) {
+    // this CTA's patch: line group lg, segment xs of 2^lg_seg row blocks
+    const int64_t nseg = ly_rb >> lg_seg;
+    const int64_t lg = blockIdx.x / nseg, xs = blockIdx.x - lg * nseg;
+    const int t = (int)(threadIdx.x >> lg_tk);
+    rb = (lg * kDiaLines + (t >> lg_seg)) * ly_rb + (xs << lg_seg) + (t & ((1 << lg_seg) - 1));
+  }
   const int tk = (int)(g & ((1 << lg_tk) - 1));
   const int64_t r0 = rb * RB;
   if (r0 >= m)
@@ -382,13 +404,34 @@ void dia_launch(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64
   int lg_tk = 0;
   while ((1 << lg_tk) < cols && lg_tk < 5)
     ++lg_tk;
-  const int64_t threads = div_up(m, kDiaRows) << lg_tk;
+  const int64_t nrb = div_up(m, kDiaRows);
+  const int64_t threads = nrb << lg_tk;
   const uint32_t full_mask = d.nd >= 32 ? 0xffffffffu : (1u << d.nd) - 1u;
   const bool passes = cols > (1 << lg_tk);
+  // Line patches (see kDiaLines): the line stride from the run centres, in
+  // row blocks, a whole number of segments of (256 threads >> lg_tk) /
+  // kDiaLines row blocks.
+  int64_t patch_rbs = 0;
+  int32_t ly_rb = 0;
+  const int lg_seg = 8 - lg_tk - 2;  // log2(row blocks per CTA / kDiaLines)
+  {
+    int64_t ly = 0;
+    for (int q = 1; q < runs.n; ++q) {
+      const int64_t gap = ((int64_t)runs.o0[q] + (runs.len[q] - 1) / 2) -
+                          ((int64_t)runs.o0[q - 1] + (runs.len[q - 1] - 1) / 2);
+      if (gap >= 16 && (ly == 0 || gap < ly))
+        ly = gap;
+    }
+    if (lg_seg >= 0 && ly > 0 && ly % kDiaRows == 0 && ly / kDiaRows <= INT32_MAX &&
+        (ly / kDiaRows) % (1 << lg_seg) == 0) {
+      ly_rb = (int32_t)(ly / kDiaRows);
+      patch_rbs = nrb / ((int64_t)kDiaLines * ly_rb) * ((int64_t)kDiaLines * ly_rb);
+    }
+  }
   auto kern = passes ? k_spmm_dia<V, X, VEC, true> : k_spmm_dia<V, X, VEC, false>;
   kern<<<(unsigned)div_up(threads, 256), 256, 0, s>>>(
       m, c.ncols, d.nd, runs, d.vals.as<V>(), d.full.as<uint32_t>(), full_mask, B, ldb, C, ldc,
-      k, lg_tk, alpha, beta, beta != X(0));
+      k, lg_tk, patch_rbs, ly_rb, lg_seg, alpha, beta, beta != X(0));
   PLS_LAUNCH_CHECK();
 }
 

@@ -233,6 +233,61 @@ def test_bsr_spmm_vs_oracle():
                 assert rel_err_rows(A.spmv(x), y_ref, oracle.csr_absdot(rp, c, v, x)).max() <= 1e-12
 
 
+@pytest.mark.parametrize("dtype,storage", [(np.float64, pls.STORAGE_NATIVE), (np.float64, pls.STORAGE_FP32),
+                                           (np.float32, pls.STORAGE_NATIVE), (np.float32, pls.STORAGE_BF16)])
+def test_bsr_vector_kernel_equals_scalar_kernel_bitwise(dtype, storage):
+    """The BSR FMA kernel with 16-byte vectors of B and C (ldb, ldc multiples
+    of the vector) adds each element of C's products in the same order, with
+    the same epilogue, as the scalar kernel that runs when the strides are
+    not: the same bits, for block sizes 2 / 4 / 8, both block layouts, k
+    from one vector to several passes, beta = 0 and beta != 0, empty block
+    rows. Both also match the FP64 oracle."""
+    import torch
+
+    rng = np.random.default_rng(70)
+    vec = 16 // np.dtype(dtype).itemsize
+    tol = {pls.STORAGE_NATIVE: 1e-12 if dtype == np.float64 else 1e-5, pls.STORAGE_FP32: 1e-5,
+           pls.STORAGE_BF16: 1e-2}[storage]
+    tdt = torch.float64 if dtype == np.float64 else torch.float32
+    for bs in (2, 4, 8):
+        for layout in (pls.ROW_MAJOR, pls.COL_MAJOR):
+            mb, nb = 150, 130
+            rp = np.zeros(mb + 1, np.int32)
+            cols = []
+            for i in range(mb):
+                cnt = 0 if i % 11 == 0 else int(rng.integers(1, 7))
+                cols.append(np.sort(rng.choice(nb, cnt, replace=False)))
+                rp[i + 1] = rp[i] + cnt
+            col = np.concatenate(cols).astype(np.int32)
+            vals = rng.uniform(-1, 1, len(col) * bs * bs).astype(dtype)
+            m, n = mb * bs, nb * bs
+            crp, cc, cv = oracle.bsr2csr(rp, col, vals.astype(np.float64), bs, layout)
+            A = pls.SpMat.bsr(layout, m, n, bs, rp, col, vals)
+            A.set_storage(storage)
+            A.set_spmm_path(0)  # the FMA kernel (not the tensor-core one) at bs 8 with BF16 values
+            for k in (vec, 8 * vec, 48 * vec):
+                Bd = rng.uniform(-1, 1, (n, k)).astype(dtype)
+                C0 = rng.uniform(-1, 1, (m, k)).astype(dtype)
+                B64 = Bd.astype(np.float64)
+                for alpha, beta in ((1.0, 0.0), (0.75, -1.5)):
+                    outs = []
+                    for pad in (0, 1):  # ld = k: vector kernel; ld = k + 1: scalar kernel
+                        ld = k + pad
+                        Bt = torch.zeros((n, ld), dtype=tdt, device="cuda")
+                        Bt[:, :k] = torch.tensor(Bd, device="cuda")
+                        Ct = torch.zeros((m, ld), dtype=tdt, device="cuda")
+                        Ct[:, :k] = torch.tensor(C0, device="cuda")
+                        A.spmm_dev(Bt.data_ptr(), ld, k, Ct.data_ptr(), ld, alpha, beta)
+                        torch.cuda.synchronize()
+                        assert A.spmm_info()["path"] == 6
+                        outs.append(Ct[:, :k].cpu().numpy())
+                    np.testing.assert_array_equal(outs[0], outs[1], err_msg=str((bs, layout, k, beta)))
+                    ref = spmm_ref(crp, cc, cv, B64, alpha, beta, C0.astype(np.float64) if beta else None)
+                    err = scaled_err(outs[0].astype(np.float64), ref, crp, cc, cv, B64, alpha, beta,
+                                     C0.astype(np.float64))
+                    assert err <= tol, (bs, layout, k, beta, err)
+
+
 @pytest.mark.parametrize("storage,tol", [(pls.STORAGE_NATIVE, 1e-12), (pls.STORAGE_FP32, 1e-5),
                                          (pls.STORAGE_BF16, 1e-2)])
 def test_stencil_spmm_storage_modes(storage, tol):
