@@ -163,16 +163,19 @@ __global__ void k_dia_full(int64_t nblocks, int nd, const V *__restrict__ dv,
   full[b] = bits;
 }
 
-// The kDiaRows values of one block of rows on one diagonal (8, 16 or 32
-// bytes, aligned to their size).
-template <class V>
-__device__ __forceinline__ void ld_rows_vals(const V *p, V (&a)[kDiaRows]) {
-  constexpr int bytes = kDiaRows * (int)sizeof(V);
-  static_assert(bytes == 8 || bytes % 16 == 0, "value blocks load as whole vectors");
-  if constexpr (bytes == 8) {
+// The RB values of a thread's rows on one diagonal (RB * sizeof(V) bytes:
+// 4, 8 or a multiple of 16, aligned to their size).
+template <int RB, class V>
+__device__ __forceinline__ void ld_rows_vals(const V *p, V (&a)[RB]) {
+  constexpr int bytes = RB * (int)sizeof(V);
+  if constexpr (bytes == 4) {
+    const unsigned t = __ldg(reinterpret_cast<const unsigned *>(p));
+    memcpy(a, &t, 4);
+  } else if constexpr (bytes == 8) {
     const uint2 t = __ldg(reinterpret_cast<const uint2 *>(p));
     memcpy(a, &t, 8);
   } else {
+    static_assert(bytes % 16 == 0, "value lines load as whole vectors");
 #pragma unroll
     for (int i = 0; i < bytes / 16; ++i) {
       const uint4 t = __ldg(reinterpret_cast<const uint4 *>(p) + i);
@@ -181,18 +184,18 @@ __device__ __forceinline__ void ld_rows_vals(const V *p, V (&a)[kDiaRows]) {
   }
 }
 
-// One run of len consecutive diagonals for a thread's kDiaRows rows: B's
-// rows br0 + j, j = 0 .. kDiaRows + len - 2, at bp + j * ldb (columns of the
-// thread's vector); the values of the run's diagonal l at ab + l * kDiaRows.
+// One run of len consecutive diagonals for a thread's RB rows: B's rows
+// br0 + j, j = 0 .. RB + len - 2, at bp + j * ldb (columns of the thread's
+// vector); the values of the run's diagonal l at ab + l * kDiaRows (the
+// thread's RB of its block's kDiaRows values).
 // INSIDE: len == kDiaRun and the rows all lie inside B, so the loads are
 // neither checked nor predicated (otherwise rows outside [0, n) read as
 // zeros). CHECK: absent entries are skipped (without it the block must store
 // every diagonal). Either way each stored entry is one fma in ascending
 // diagonal order.
-template <bool INSIDE, bool CHECK, class V, class X, class Acc, int VEC>
+template <bool INSIDE, bool CHECK, int RB, class V, class X, class Acc, int VEC>
 __device__ __forceinline__ void dia_run(const X *bp, int64_t ldb, int64_t br0, int64_t n,
-                                        int len, const V *ab, Acc (&acc)[kDiaRows][VEC]) {
-  constexpr int RB = kDiaRows;
+                                        int len, const V *ab, Acc (&acc)[RB][VEC]) {
   constexpr bool FAST = INSIDE;
   X bv[RB + kDiaRun - 1][VEC];
 #pragma unroll
@@ -209,7 +212,7 @@ __device__ __forceinline__ void dia_run(const X *bp, int64_t ldb, int64_t br0, i
   for (int l = 0; l < kDiaRun; ++l) {
     if (FAST || l < len) {
       V a[RB];
-      ld_rows_vals<V>(ab + l * RB, a);
+      ld_rows_vals<RB, V>(ab + l * kDiaRows, a);
 #pragma unroll
       for (int i = 0; i < RB; ++i)
         if (!CHECK || !dia_absent(a[i])) {
@@ -229,43 +232,50 @@ __device__ __forceinline__ void dia_run(const X *bp, int64_t ldb, int64_t br0, i
 // other CTAs on other SMs, and each brings B's rows from L2 again. Where the
 // host finds such a line stride (the smallest gap of at least 16 rows
 // between consecutive run centres), each CTA instead takes a patch of
-// kDiaLines lines x (its row blocks / kDiaLines) consecutive row blocks, so
-// the lines it holds read each other's rows of B from L1. The patches tile
-// the first patch_rbs row blocks (whole groups of kDiaLines lines); the rest
-// keep consecutive row blocks. Every thread computes the same block of rows
-// either way, so the results do not change.
+// kDiaLines lines x (its units / kDiaLines) consecutive units (a unit is a
+// thread's rows), so the lines it holds read each other's rows of B from
+// L1. The patches tile the first patch_units units (whole groups of
+// kDiaLines lines); the rest keep consecutive units. Every thread computes
+// the same rows either way, so the results do not change.
 constexpr int kDiaLines = 4;
 
-// Threads: (block of kDiaRows rows) x (TK column vectors of VEC); a thread
-// loops over C's columns in steps of TK * VEC. MASK (threads that make more
-// than one pass over the columns): the block's full-diagonal mask is loaded
-// first and blocks that store every diagonal skip the absent checks; with
-// one pass that load's latency costs more than the checks (C3, FP64: 0.233
-// against 0.331 ms at k = 8, 0.725 against 0.849 ms at k = 32; at k = 128,
-// two passes, 2.21 against 2.43 ms).
-template <class V, class X, int VEC, bool MASK>
-__global__ void __launch_bounds__(256, 4)  // 64 registers: 4 blocks per SM
+// Rows per thread. Each thread owns kDiaThreadRows consecutive rows of one
+// block of kDiaRows (a unit) and one 16-byte vector of C's columns.
+constexpr int kDiaThreadRows = 4;
+
+// Threads: (unit of RB rows) x (TK column vectors of VEC); a thread loops
+// over C's columns in steps of TK * VEC. MASK (threads that make more than
+// one pass over the columns): the block's full-diagonal mask is loaded first
+// and blocks that store every diagonal skip the absent checks; with one pass
+// that load's latency costs more than the checks (C3, FP64: 0.233 against
+// 0.331 ms at k = 8, 0.725 against 0.849 ms at k = 32; at k = 128, two
+// passes, 2.21 against 2.43 ms). Units are consecutive, or line patches of
+// 2^lg_seg units per line (patch_units of them, ly_u units per line).
+template <class V, class X, int VEC, bool MASK, int RB>
+__global__ void __launch_bounds__(256, RB == kDiaRows ? 4 : 6)
     k_spmm_dia(int32_t m, int32_t n, int nd, DiaRuns runs, const V *__restrict__ dv,
                const uint32_t *__restrict__ dfull, uint32_t full_mask,
                const X *__restrict__ B, int64_t ldb, X *__restrict__ C, int64_t ldc, int k,
-               int lg_tk, int64_t patch_rbs, int32_t ly_rb, int lg_seg, X alpha, X beta,
+               int lg_tk, int64_t patch_units, int32_t ly_u, int lg_seg, X alpha, X beta,
                int beta_nz) {
-  constexpr int RB = kDiaRows;
+  static_assert(kDiaRows % RB == 0, "a thread's rows lie in one block");
+  constexpr int SUB = kDiaRows / RB;  // units per block
   using Acc = typename AccOf<V, X>::type;
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  int64_t rb = g >> lg_tk;
-  if (((int64_t)blockIdx.x * blockDim.x >> lg_tk) < patch_rbs) {
-    // this CTA's patch: line group lg, segment xs of 2^lg_seg row blocks
-    const int64_t nseg = ly_rb >> lg_seg;
+  int64_t u = g >> lg_tk;
+  if (((int64_t)blockIdx.x * blockDim.x >> lg_tk) < patch_units) {
+    // this CTA's patch: line group lg, segment xs of 2^lg_seg units
+    const int64_t nseg = ly_u >> lg_seg;
     const int64_t lg = blockIdx.x / nseg, xs = blockIdx.x - lg * nseg;
     const int t = (int)(threadIdx.x >> lg_tk);
-    rb = (lg * kDiaLines + (t >> lg_seg)) * ly_rb + (xs << lg_seg) + (t & ((1 << lg_seg) - 1));
+    u = (lg * kDiaLines + (t >> lg_seg)) * ly_u + (xs << lg_seg) + (t & ((1 << lg_seg) - 1));
   }
   const int tk = (int)(g & ((1 << lg_tk) - 1));
-  const int64_t r0 = rb * RB;
+  const int64_t r0 = u * RB;
   if (r0 >= m)
     return;
-  const V *ab = dv + rb * nd * RB;
+  const int64_t rb = u / SUB;  // the unit's block
+  const V *ab = dv + rb * nd * kDiaRows + (u % SUB) * RB;
   const bool full = MASK && (__ldg(dfull + rb) & full_mask) == full_mask;
   for (int kk = tk * VEC; kk < k; kk += VEC << lg_tk) {
     Acc acc[RB][VEC];
@@ -278,14 +288,14 @@ __global__ void __launch_bounds__(256, 4)  // 64 registers: 4 blocks per SM
       const int o0 = runs.o0[q], len = runs.len[q];
       const int64_t br0 = r0 + o0;
       const X *bp = B + br0 * ldb + kk;
-      const V *aq = ab + runs.d0[q] * RB;
+      const V *aq = ab + runs.d0[q] * kDiaRows;
       if (len == kDiaRun && br0 >= 0 && br0 + RB + kDiaRun - 2 < n) {
         if (MASK && full)
-          dia_run<true, false, V, X, Acc, VEC>(bp, ldb, br0, n, len, aq, acc);
+          dia_run<true, false, RB, V, X, Acc, VEC>(bp, ldb, br0, n, len, aq, acc);
         else
-          dia_run<true, true, V, X, Acc, VEC>(bp, ldb, br0, n, len, aq, acc);
+          dia_run<true, true, RB, V, X, Acc, VEC>(bp, ldb, br0, n, len, aq, acc);
       } else {
-        dia_run<false, true, V, X, Acc, VEC>(bp, ldb, br0, n, len, aq, acc);
+        dia_run<false, true, RB, V, X, Acc, VEC>(bp, ldb, br0, n, len, aq, acc);
       }
     }
 #pragma unroll
@@ -404,16 +414,17 @@ void dia_launch(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64
   int lg_tk = 0;
   while ((1 << lg_tk) < cols && lg_tk < 5)
     ++lg_tk;
-  const int64_t nrb = div_up(m, kDiaRows);
-  const int64_t threads = nrb << lg_tk;
+  constexpr int RB = kDiaThreadRows;
+  const int64_t nunits = div_up(m, RB);
+  const int64_t threads = nunits << lg_tk;
   const uint32_t full_mask = d.nd >= 32 ? 0xffffffffu : (1u << d.nd) - 1u;
   const bool passes = cols > (1 << lg_tk);
   // Line patches (see kDiaLines): the line stride from the run centres, in
-  // row blocks, a whole number of segments of (256 threads >> lg_tk) /
-  // kDiaLines row blocks.
-  int64_t patch_rbs = 0;
-  int32_t ly_rb = 0;
-  const int lg_seg = 8 - lg_tk - 2;  // log2(row blocks per CTA / kDiaLines)
+  // units of RB rows, a whole number of segments of (256 threads >> lg_tk) /
+  // kDiaLines units.
+  int64_t patch_units = 0;
+  int32_t ly_u = 0;
+  const int lg_seg = 8 - lg_tk - 2;  // log2(units per CTA / kDiaLines)
   {
     int64_t ly = 0;
     for (int q = 1; q < runs.n; ++q) {
@@ -422,16 +433,16 @@ void dia_launch(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64
       if (gap >= 16 && (ly == 0 || gap < ly))
         ly = gap;
     }
-    if (lg_seg >= 0 && ly > 0 && ly % kDiaRows == 0 && ly / kDiaRows <= INT32_MAX &&
-        (ly / kDiaRows) % (1 << lg_seg) == 0) {
-      ly_rb = (int32_t)(ly / kDiaRows);
-      patch_rbs = nrb / ((int64_t)kDiaLines * ly_rb) * ((int64_t)kDiaLines * ly_rb);
+    if (lg_seg >= 0 && ly > 0 && ly % RB == 0 && ly / RB <= INT32_MAX &&
+        (ly / RB) % (1 << lg_seg) == 0) {
+      ly_u = (int32_t)(ly / RB);
+      patch_units = nunits / ((int64_t)kDiaLines * ly_u) * ((int64_t)kDiaLines * ly_u);
     }
   }
-  auto kern = passes ? k_spmm_dia<V, X, VEC, true> : k_spmm_dia<V, X, VEC, false>;
+  auto kern = passes ? k_spmm_dia<V, X, VEC, true, RB> : k_spmm_dia<V, X, VEC, false, RB>;
   kern<<<(unsigned)div_up(threads, 256), 256, 0, s>>>(
       m, c.ncols, d.nd, runs, d.vals.as<V>(), d.full.as<uint32_t>(), full_mask, B, ldb, C, ldc,
-      k, lg_tk, patch_rbs, ly_rb, lg_seg, alpha, beta, beta != X(0));
+      k, lg_tk, patch_units, ly_u, lg_seg, alpha, beta, beta != X(0));
   PLS_LAUNCH_CHECK();
 }
 
