@@ -48,6 +48,84 @@ struct DiaTmaArgs {
 
 inline int64_t plan_div_up(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+#ifdef __CUDACC__
+#define PLS_PLAN_HD __host__ __device__
+#else
+#define PLS_PLAN_HD
+#endif
+
+// Runs of consecutive diagonals (at most kDiaRun each) over the ascending
+// offsets: run q starts at offset o0[q], diagonal d0[q], and has len[q]
+// diagonals.
+struct DiaRuns {
+  int n = 0;
+  int o0[kDiaMax], len[kDiaMax], d0[kDiaMax];
+};
+
+inline DiaRuns dia_runs(const int32_t *offs, int nd) {
+  DiaRuns r{};
+  for (int i = 0; i < nd;) {
+    int len = 1;
+    while (i + len < nd && len < kDiaRun && offs[i + len] == offs[i] + len)
+      ++len;
+    r.o0[r.n] = offs[i];
+    r.len[r.n] = len;
+    r.d0[r.n] = i;
+    ++r.n;
+    i += len;
+  }
+  return r;
+}
+
+// Line patches of the diagonal-form SpMM (k_spmm_dia). On a grid stencil
+// the runs come one grid line (Ly rows) apart, so the runs of row r at
+// offset +Ly read the rows of B that row r + Ly reads at offset 0. Where the
+// run centres show such a stride (the smallest gap of at least 16 rows
+// between consecutive centres), each CTA takes kDiaLines lines x (its units
+// / kDiaLines) consecutive units (a unit is one thread's rb rows) instead of
+// consecutive units, so the lines it holds read each other's rows of B from
+// L1. The patches tile the first `units` units (whole groups of kDiaLines
+// lines, ly_u units per line, segments of 2^lg_seg units); the rest keep
+// consecutive units. 256-thread CTAs, 2^lg_tk threads per unit.
+constexpr int kDiaLines = 4;
+
+struct DiaPatchPlan {
+  int64_t units = 0;  // units covered by patches (0: none)
+  int32_t ly_u = 0;   // units per grid line
+  int lg_seg = 0;     // log2(units per CTA / kDiaLines)
+};
+
+inline DiaPatchPlan dia_patch_plan(const DiaRuns &runs, int rb, int64_t nunits, int lg_tk) {
+  DiaPatchPlan p;
+  p.lg_seg = 8 - lg_tk - 2;
+  int64_t ly = 0;
+  for (int q = 1; q < runs.n; ++q) {
+    const int64_t gap = ((int64_t)runs.o0[q] + (runs.len[q] - 1) / 2) -
+                        ((int64_t)runs.o0[q - 1] + (runs.len[q - 1] - 1) / 2);
+    if (gap >= 16 && (ly == 0 || gap < ly))
+      ly = gap;
+  }
+  if (p.lg_seg >= 0 && ly > 0 && ly % rb == 0 && ly / rb <= INT32_MAX &&
+      (ly / rb) % ((int64_t)1 << p.lg_seg) == 0) {
+    p.ly_u = (int32_t)(ly / rb);
+    p.units = nunits / ((int64_t)kDiaLines * p.ly_u) * ((int64_t)kDiaLines * p.ly_u);
+  }
+  return p;
+}
+
+// The unit that thread `tid` (of 256) of CTA `block` computes.
+PLS_PLAN_HD inline int64_t dia_patch_unit(int64_t block, int tid, int lg_tk,
+                                          const DiaPatchPlan &p) {
+  const int64_t u = (block * 256 + tid) >> lg_tk;
+  if ((block * 256 >> lg_tk) >= p.units)
+    return u;
+  const int64_t nseg = p.ly_u >> p.lg_seg;
+  const int64_t lg = block / nseg, xs = block - lg * nseg;
+  const int t = tid >> lg_tk;
+  return (lg * kDiaLines + (t >> p.lg_seg)) * p.ly_u + (xs << p.lg_seg) +
+         (t & ((1 << p.lg_seg) - 1));
+}
+
 inline int64_t floor_mid(int64_t lo, int64_t hi) {
   const int64_t s = lo + hi;
   return s >= 0 ? s / 2 : -((-s + 1) / 2);

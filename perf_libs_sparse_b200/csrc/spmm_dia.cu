@@ -69,11 +69,6 @@ template <> __device__ __forceinline__ __nv_bfloat16 dia_absent_value<__nv_bfloa
   return __ushort_as_bfloat16(kAbsentH);
 }
 
-struct DiaRuns {
-  int n;
-  int o0[kDiaMax], len[kDiaMax], d0[kDiaMax];
-};
-
 struct DiaOffs {
   int nd;
   int32_t o[kDiaMax];
@@ -225,19 +220,7 @@ __device__ __forceinline__ void dia_run(const X *bp, int64_t ldb, int64_t br0, i
   }
 }
 
-// Line patches. On a grid stencil the diagonals come in runs one grid line
-// (Ly rows) apart, so the runs of row r at offset +Ly read the rows of B that
-// the runs of row r + Ly read at offset 0. A CTA of consecutive rows shares
-// only the overlap inside each run through L1; the rows Ly away belong to
-// other CTAs on other SMs, and each brings B's rows from L2 again. Where the
-// host finds such a line stride (the smallest gap of at least 16 rows
-// between consecutive run centres), each CTA instead takes a patch of
-// kDiaLines lines x (its units / kDiaLines) consecutive units (a unit is a
-// thread's rows), so the lines it holds read each other's rows of B from
-// L1. The patches tile the first patch_units units (whole groups of
-// kDiaLines lines); the rest keep consecutive units. Every thread computes
-// the same rows either way, so the results do not change.
-constexpr int kDiaLines = 4;
+// Line patches: dia_patch_plan / dia_patch_unit in dia_plan.hpp.
 
 // Rows per thread. Each thread owns kDiaThreadRows consecutive rows of one
 // block of kDiaRows (a unit) and one 16-byte vector of C's columns.
@@ -249,28 +232,19 @@ constexpr int kDiaThreadRows = 4;
 // and blocks that store every diagonal skip the absent checks; with one pass
 // that load's latency costs more than the checks (C3, FP64: 0.233 against
 // 0.331 ms at k = 8, 0.725 against 0.849 ms at k = 32; at k = 128, two
-// passes, 2.21 against 2.43 ms). Units are consecutive, or line patches of
-// 2^lg_seg units per line (patch_units of them, ly_u units per line).
+// passes, 2.21 against 2.43 ms). A thread's unit comes from the line-patch
+// plan (dia_patch_unit).
 template <class V, class X, int VEC, bool MASK, int RB>
 __global__ void __launch_bounds__(256, RB == kDiaRows ? 4 : 6)
     k_spmm_dia(int32_t m, int32_t n, int nd, DiaRuns runs, const V *__restrict__ dv,
                const uint32_t *__restrict__ dfull, uint32_t full_mask,
                const X *__restrict__ B, int64_t ldb, X *__restrict__ C, int64_t ldc, int k,
-               int lg_tk, int64_t patch_units, int32_t ly_u, int lg_seg, X alpha, X beta,
-               int beta_nz) {
+               int lg_tk, DiaPatchPlan patch, X alpha, X beta, int beta_nz) {
   static_assert(kDiaRows % RB == 0, "a thread's rows lie in one block");
   constexpr int SUB = kDiaRows / RB;  // units per block
   using Acc = typename AccOf<V, X>::type;
-  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  int64_t u = g >> lg_tk;
-  if (((int64_t)blockIdx.x * blockDim.x >> lg_tk) < patch_units) {
-    // this CTA's patch: line group lg, segment xs of 2^lg_seg units
-    const int64_t nseg = ly_u >> lg_seg;
-    const int64_t lg = blockIdx.x / nseg, xs = blockIdx.x - lg * nseg;
-    const int t = (int)(threadIdx.x >> lg_tk);
-    u = (lg * kDiaLines + (t >> lg_seg)) * ly_u + (xs << lg_seg) + (t & ((1 << lg_seg) - 1));
-  }
-  const int tk = (int)(g & ((1 << lg_tk) - 1));
+  const int64_t u = dia_patch_unit(blockIdx.x, (int)threadIdx.x, lg_tk, patch);
+  const int tk = (int)(threadIdx.x & ((1 << lg_tk) - 1));
   const int64_t r0 = u * RB;
   if (r0 >= m)
     return;
@@ -399,17 +373,7 @@ void dia_launch(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64
                 X alpha, X beta, cudaStream_t s) {
   constexpr int VEC = 16 / (int)sizeof(X);
   const DiaDev &d = c.dia;
-  DiaRuns runs{};
-  for (int i = 0; i < d.nd;) {
-    int len = 1;
-    while (i + len < d.nd && len < kDiaRun && d.offs[i + len] == d.offs[i] + len)
-      ++len;
-    runs.o0[runs.n] = d.offs[i];
-    runs.len[runs.n] = len;
-    runs.d0[runs.n] = i;
-    ++runs.n;
-    i += len;
-  }
+  const DiaRuns runs = dia_runs(d.offs, d.nd);
   const int cols = k / VEC;
   int lg_tk = 0;
   while ((1 << lg_tk) < cols && lg_tk < 5)
@@ -419,30 +383,11 @@ void dia_launch(const CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C, int64
   const int64_t threads = nunits << lg_tk;
   const uint32_t full_mask = d.nd >= 32 ? 0xffffffffu : (1u << d.nd) - 1u;
   const bool passes = cols > (1 << lg_tk);
-  // Line patches (see kDiaLines): the line stride from the run centres, in
-  // units of RB rows, a whole number of segments of (256 threads >> lg_tk) /
-  // kDiaLines units.
-  int64_t patch_units = 0;
-  int32_t ly_u = 0;
-  const int lg_seg = 8 - lg_tk - 2;  // log2(units per CTA / kDiaLines)
-  {
-    int64_t ly = 0;
-    for (int q = 1; q < runs.n; ++q) {
-      const int64_t gap = ((int64_t)runs.o0[q] + (runs.len[q] - 1) / 2) -
-                          ((int64_t)runs.o0[q - 1] + (runs.len[q - 1] - 1) / 2);
-      if (gap >= 16 && (ly == 0 || gap < ly))
-        ly = gap;
-    }
-    if (lg_seg >= 0 && ly > 0 && ly % RB == 0 && ly / RB <= INT32_MAX &&
-        (ly / RB) % (1 << lg_seg) == 0) {
-      ly_u = (int32_t)(ly / RB);
-      patch_units = nunits / ((int64_t)kDiaLines * ly_u) * ((int64_t)kDiaLines * ly_u);
-    }
-  }
+  const DiaPatchPlan patch = dia_patch_plan(runs, RB, nunits, lg_tk);
   auto kern = passes ? k_spmm_dia<V, X, VEC, true, RB> : k_spmm_dia<V, X, VEC, false, RB>;
   kern<<<(unsigned)div_up(threads, 256), 256, 0, s>>>(
       m, c.ncols, d.nd, runs, d.vals.as<V>(), d.full.as<uint32_t>(), full_mask, B, ldb, C, ldc,
-      k, lg_tk, patch_units, ly_u, lg_seg, alpha, beta, beta != X(0));
+      k, lg_tk, patch, alpha, beta, beta != X(0));
   PLS_LAUNCH_CHECK();
 }
 

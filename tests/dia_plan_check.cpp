@@ -16,6 +16,10 @@
 //     padded diagonal-form buffer;
 //   * every element of C (row < m, column < k) is written exactly once;
 //   * shared memory fits one CTA.
+// It also replays the line-patch plan of the kernel that reads B through L1
+// (k_spmm_dia: dia_patch_plan / dia_patch_unit in the same header) over
+// every CTA and thread: every unit of rows is computed exactly once, and
+// each patch CTA holds whole line segments.
 // Prints "ok <cases>" or the first violation (exit status 1).
 #include <cstdio>
 #include <cstdlib>
@@ -261,6 +265,50 @@ static bool replay(const Case &cs, int k, int xb, int vb, int sms) {
   return true;
 }
 
+// The line-patch plan of the diagonal-form kernel that reads B through L1
+// (k_spmm_dia): over every CTA and thread of the launch, every unit of rb
+// rows below the row count is computed by exactly one thread group, units at
+// or past it only by the consecutive tail (where the kernel's row guard
+// drops them), and each patch CTA holds kDiaLines whole line segments of the
+// detected line stride. Returns whether patches applied.
+static bool replay_patches(const Case &cs, int lg_tk, int rb) {
+  const DiaRuns runs = dia_runs(cs.offs.data(), (int)cs.offs.size());
+  const int64_t nunits = plan_div_up(cs.m, rb);
+  const DiaPatchPlan p = dia_patch_plan(runs, rb, nunits, lg_tk);
+  CHECK(p.units % (256 >> lg_tk) == 0 && p.units <= nunits, "%s lg_tk=%d: %lld patch units",
+        cs.name.c_str(), lg_tk, (long long)p.units);
+  const int64_t grid = plan_div_up(nunits << lg_tk, 256);
+  std::vector<unsigned char> seen((size_t)nunits, 0);
+  for (int64_t b = 0; b < grid; ++b) {
+    int64_t first = -1;
+    for (int tid = 0; tid < 256; tid += 1 << lg_tk) {
+      const int64_t u = dia_patch_unit(b, tid, lg_tk, p);
+      const bool in_patch = (b * 256 >> lg_tk) < p.units;
+      if (u >= nunits) {
+        CHECK(!in_patch, "%s lg_tk=%d: patch unit %lld past %lld", cs.name.c_str(), lg_tk, (long long)u,
+              (long long)nunits);
+        continue;
+      }
+      CHECK(u >= 0 && seen[(size_t)u] == 0, "%s lg_tk=%d: unit %lld twice", cs.name.c_str(), lg_tk,
+            (long long)u);
+      seen[(size_t)u] = 1;
+      if (in_patch) {
+        // thread group t of the CTA: line t >> lg_seg of the patch, the
+        // (t & (seg - 1))-th unit of the segment
+        const int t = tid >> lg_tk, seg = 1 << p.lg_seg;
+        if (t == 0)
+          first = u;
+        CHECK(u == first + (int64_t)(t / seg) * p.ly_u + t % seg, "%s lg_tk=%d: patch shape",
+              cs.name.c_str(), lg_tk);
+      }
+    }
+  }
+  for (int64_t u = 0; u < nunits; ++u)
+    CHECK(seen[(size_t)u] == 1, "%s lg_tk=%d: unit %lld not computed", cs.name.c_str(), lg_tk,
+          (long long)u);
+  return p.units > 0;
+}
+
 int main() {
   std::vector<Case> cases = {
       {"27pt-128", 128 * 128 * 128, stencil3d(128, true), {8, 32, 128}},
@@ -304,6 +352,21 @@ int main() {
   for (int k : {8, 32, 128})
     for (int vb : {4, 2})
       CHECK(dia_tma_shape(c3.offs.data(), (int)c3.offs.size(), c3.m, k, 4, vb, 148).ok, "C3 k=%d FP32", k);
-  std::printf("ok %d of %d configurations applied and replayed\n", applied, tried);
+  int patched = 0, ptried = 0;
+  for (const Case &cs : cases)
+    for (int lg_tk = 0; lg_tk <= 5; ++lg_tk)
+      for (int rb : {4, 2}) {
+        ++ptried;
+        patched += replay_patches(cs, lg_tk, rb) ? 1 : 0;
+      }
+  // The C3 matrix gets patches at the lane counts of k = 8 / 32 / 128 (FP64).
+  for (int lg_tk : {2, 4, 5}) {
+    const DiaRuns r = dia_runs(c3.offs.data(), (int)c3.offs.size());
+    CHECK(dia_patch_plan(r, kDiaRows, plan_div_up(c3.m, kDiaRows), lg_tk).units ==
+              plan_div_up(c3.m, kDiaRows),
+          "C3 line patches, lg_tk=%d", lg_tk);
+  }
+  std::printf("ok %d of %d configurations applied and replayed; line patches in %d of %d\n",
+              applied, tried, patched, ptried);
   return 0;
 }

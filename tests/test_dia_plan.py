@@ -8,7 +8,9 @@ stencils, bands, the 27-point 128^3 matrix of the benchmark), column counts
 and element sizes: every copy must fit and be aligned, every copy must be
 waited for once before its first read and never overwritten while read,
 every read must hit the B row its entry needs, and every element of C must
-be written exactly once."""
+be written exactly once. It also replays the line-patch assignment of the
+diagonal-form kernel that reads B through L1 (every unit of rows computed
+exactly once, for every lane count and both unit sizes)."""
 import os
 import shutil
 import subprocess
