@@ -655,6 +655,61 @@ def test_dia_tma_equals_diagonal_form_bitwise(storage):
                     assert err <= tol, (m, k, ldb, err)
 
 
+def _laplacian_rect(nx, ny, rng):
+    """5-point operator on an nx x ny grid (rows of nx points: the line stride
+    is nx), random values, sorted columns."""
+    n = nx * ny
+    i = np.arange(n, dtype=np.int64)
+    r, c = i // nx, i % nx
+    offs = [(-nx, r > 0), (-1, c > 0), (0, np.ones(n, bool)), (1, c < nx - 1), (nx, r < ny - 1)]
+    cols = np.stack([i + o for o, _ in offs], 1)
+    mask = np.stack([mk for _, mk in offs], 1)
+    counts = mask.sum(1)
+    rp = np.zeros(n + 1, np.int32)
+    rp[1:] = np.cumsum(counts)
+    col = cols[mask].astype(np.int32)
+    return n, n, rp, col, rng.uniform(-1, 1, len(col))
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+def test_diagonal_form_line_patches_equal_row_group_bitwise(dt):
+    """Grids whose line stride lets the diagonal-form kernel give each CTA a
+    patch of 4 grid lines (64-point lines; a 27-point stencil on 32^3 and
+    64^3), with a tail of units past the last whole group of lines (37 and 41
+    lines): with beta = 0 the kernel must equal the row-group kernel bit for
+    bit at every column count (1, several or many lanes per unit, one or two
+    passes), so every row is computed once by the right thread, and match the
+    oracle."""
+    import torch
+
+    rng = np.random.default_rng(23)
+    vec = 16 // np.dtype(dt).itemsize
+    tol = 1e-12 if dt == np.float64 else 1e-5
+    cases = [_laplacian_rect(64, 37, rng), _laplacian_rect(64, 41, rng), W.stencil_27pt(32, seed=5),
+             W.stencil_27pt(64, seed=6)]
+    for (m, n, rp, c, v) in cases:
+        v = v.astype(dt)
+        A = pls.SpMat.csr(m, n, rp, c, v)
+        for k in (8, 32, 64, 128, 256):
+            Bd = rng.uniform(-1, 1, (n, k)).astype(dt)
+            Bt = torch.tensor(Bd, device="cuda")
+            out = {}
+            for path in (0, 3):
+                A.set_spmm_path(path)
+                Ct = torch.full((m, k), float("nan"), dtype=Bt.dtype, device="cuda")
+                A.spmm_dev(Bt.data_ptr(), k, k, Ct.data_ptr(), k, 1.0, 0.0)
+                torch.cuda.synchronize()
+                out[path] = (Ct.cpu().numpy(), A.spmm_info()["path"])
+            assert out[3][1] == 3, (m, k)
+            if k // vec > 2:  # the row-group kernel also keeps each row in one lane group
+                np.testing.assert_array_equal(out[0][0], out[3][0], err_msg=str((m, k)))
+            v64, B64 = v.astype(np.float64), Bd.astype(np.float64)
+            Z = np.zeros((m, k))
+            assert scaled_err(out[3][0].astype(np.float64), spmm_ref(rp, c, v64, B64, 1.0, 0.0, Z),
+                              rp, c, v64, B64, 1.0, 0.0, Z) <= tol, (m, k)
+        A.destroy()
+
+
 @pytest.mark.parametrize("dt", [np.float64, np.float32])
 def test_diagonal_form_spmm(dt):
     """The diagonal-form SpMM (entries on a few diagonals, kept per block of
