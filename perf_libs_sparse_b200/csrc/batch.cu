@@ -474,7 +474,18 @@ void capture(Batch *B, float alpha, float beta) {
         B->inst.as<InstDesc>(), B->items.as<Item>(), B->n_items, B->sitems.as<SItem>(), n_s,
         B->counter.as<unsigned long long>(), alpha, beta, beta != 0.f);
   }
-  PLS_CUDA(cudaStreamEndCapture(s, &g));
+  // A launch refused during capture invalidates the capture: end it, take
+  // the launch's error (so that it does not surface in a later call) and
+  // report it.
+  const cudaError_t launch = cudaGetLastError();
+  const cudaError_t ended = cudaStreamEndCapture(s, &g);
+  if (launch != cudaSuccess || ended != cudaSuccess) {
+    if (ended == cudaSuccess)
+      cudaGraphDestroy(g);
+    throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE,
+                std::string("batch capture: ") +
+                    cudaGetErrorString(launch != cudaSuccess ? launch : ended));
+  }
   PLS_CUDA(cudaGraphInstantiate(&B->graph, g, 0));
   cudaGraphDestroy(g);
   B->g_alpha = alpha;
