@@ -467,17 +467,18 @@ void capture(Batch *B, float alpha, float beta) {
   PLS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   cudaMemsetAsync(B->counter.p, 0, 16, s);
   const int64_t n_s = B->staging ? B->n_sitems : 0;
+  // A launch refused during capture invalidates the capture: end it, take
+  // the launch's error (so that it does not surface in a later call) and
+  // report it.
+  cudaError_t launch = cudaSuccess;
   if (B->n_items > 0 || n_s > 0) {
     auto kern = B->off32 ? k_batch_spmm<true> : k_batch_spmm<false>;
     const size_t smem = n_s > 0 ? sizeof(float) * kStageFloats : 0;
     kern<<<B->grid, kBatchThreads, smem, s>>>(
         B->inst.as<InstDesc>(), B->items.as<Item>(), B->n_items, B->sitems.as<SItem>(), n_s,
         B->counter.as<unsigned long long>(), alpha, beta, beta != 0.f);
+    launch = cudaGetLastError();
   }
-  // A launch refused during capture invalidates the capture: end it, take
-  // the launch's error (so that it does not surface in a later call) and
-  // report it.
-  const cudaError_t launch = cudaGetLastError();
   const cudaError_t ended = cudaStreamEndCapture(s, &g);
   if (launch != cudaSuccess || ended != cudaSuccess) {
     if (ended == cudaSuccess)
