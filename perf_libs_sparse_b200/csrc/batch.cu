@@ -50,7 +50,8 @@ struct InstDesc {
   float *C;
   int64_t ldb, ldc;
   int32_t m, k, bs, layout, is_bsr;  // bs / is_bsr: block-aligned items for BSR
-  int32_t lg_tk, lg_tn, path;  // path: 0 = VEC 4, 1 = VEC 1 x 1, 2 = VEC 1 x 2
+  int32_t lg_tk, lg_tn, path;  // path: 0 = VEC 4, 1 = VEC 1 x 1, 2 = VEC 1 x 2, 3 = BSR blocks
+  const int32_t *brp;  // BSR: the handle's block row pointers (path 3 reads the blocks)
 };
 
 struct Item {
@@ -88,6 +89,67 @@ __device__ __forceinline__ void batch_rows(const Rows &A, const InstDesc &d, con
     else
       spmm_row_group<1, 2, float, float, Rows, OFF32, kEntriesAhead>(
           A, row, live, d.lg_tk, d.lg_tn, d.B, d.ldb, d.C, d.ldc, d.k, alpha, beta, beta_nz, pol);
+  }
+}
+
+// bs values of one block column of the column-major copy: bs * 4 bytes at
+// a multiple of that size.
+template <int BS>
+__device__ __forceinline__ void ld_block_line_f(const float *p, float (&a)[BS]) {
+  if constexpr (BS == 2) {
+    const float2 t = __ldg(reinterpret_cast<const float2 *>(p));
+    a[0] = t.x, a[1] = t.y;
+  } else {
+#pragma unroll
+    for (int h = 0; h < BS / 4; ++h) {
+      const float4 t = __ldg(reinterpret_cast<const float4 *>(p) + h);
+      a[4 * h] = t.x, a[4 * h + 1] = t.y, a[4 * h + 2] = t.z, a[4 * h + 3] = t.w;
+    }
+  }
+}
+
+// A BSR instance's rows [w.row0, w.row1) (whole block rows) read as blocks:
+// TK = 2^lg_tk lanes per block row, one column of C each per pass, 32 / TK
+// block rows per warp. d.val is the batch's column-major copy of the blocks
+// (column j of block b at b * bs * bs + j * bs). Per block a lane takes the
+// block's columns j in order: its element of B's row col * bs + j
+// (coalesced across the lanes), the block's column j (the same addresses
+// across the block row's lanes), and one fma per row of the block. Per
+// element of C that is the order of the scalar rows the other paths read
+// (blocks in stored order, then the block's columns). B's rows are read once
+// per block instead of once per scalar row.
+template <int BS>
+__device__ __forceinline__ void batch_bsr_rows(const InstDesc &d, const Item &w, int lane,
+                                               float alpha, float beta, int beta_nz) {
+  const int TK = 1 << d.lg_tk, per = 32 >> d.lg_tk;
+  const int t = lane & (TK - 1);
+  const int32_t br1 = w.row1 / BS;
+  for (int32_t br = w.row0 / BS + (lane >> d.lg_tk); br < br1; br += per) {
+    const int32_t b0 = __ldg(d.brp + br), b1 = __ldg(d.brp + br + 1);
+    for (int kk = t; kk < d.k; kk += TK) {
+      float acc[BS];
+#pragma unroll
+      for (int i = 0; i < BS; ++i)
+        acc[i] = 0.f;
+      for (int32_t b = b0; b < b1; ++b) {
+        const float *bp = d.B + (int64_t)__ldg(d.col + b) * BS * d.ldb + kk;
+        const float *ab = d.val + (int64_t)b * BS * BS;
+#pragma unroll
+        for (int j = 0; j < BS; ++j) {
+          const float bj = __ldg(bp + (int64_t)j * d.ldb);
+          float a[BS];
+          ld_block_line_f<BS>(ab + j * BS, a);
+#pragma unroll
+          for (int i = 0; i < BS; ++i)
+            acc[i] = fmaf(a[i], bj, acc[i]);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < BS; ++i) {
+        float *cp = d.C + ((int64_t)br * BS + i) * d.ldc + kk;
+        *cp = beta_nz ? acc[i] * alpha + beta * *cp : acc[i] * alpha;
+      }
+    }
   }
 }
 
@@ -204,7 +266,7 @@ __device__ __forceinline__ void staged_item(const SItem &w, const InstDesc &d,
 // The dynamic shared memory (kStageFloats floats) is needed only when there
 // are staged items.
 template <bool OFF32>
-__global__ void __launch_bounds__(kBatchThreads)
+__global__ void __launch_bounds__(kBatchThreads, 4)  // 64 registers: 4 blocks per SM
     k_batch_spmm(const InstDesc *__restrict__ inst, const Item *__restrict__ items,
                  int64_t n_items, const SItem *__restrict__ sitems, int64_t n_sitems,
                  unsigned long long *__restrict__ counters, float alpha, float beta,
@@ -237,8 +299,17 @@ __global__ void __launch_bounds__(kBatchThreads)
       next = atomicAdd(counters, 1ull);
     const Item w = items[it];
     const InstDesc d = inst[w.inst];
-    const PackedRows A{d.rp, d.cv};
-    batch_rows<PackedRows, OFF32>(A, d, w, lane, alpha, beta, beta_nz, pol);
+    if (d.path == 3) {
+      if (d.bs == 8)
+        batch_bsr_rows<8>(d, w, lane, alpha, beta, beta_nz);
+      else if (d.bs == 4)
+        batch_bsr_rows<4>(d, w, lane, alpha, beta, beta_nz);
+      else
+        batch_bsr_rows<2>(d, w, lane, alpha, beta, beta_nz);
+    } else {
+      const PackedRows A{d.rp, d.cv};
+      batch_rows<PackedRows, OFF32>(A, d, w, lane, alpha, beta, beta_nz, pol);
+    }
     it = __shfl_sync(0xffffffffu, next, 0);
   }
 }
@@ -275,6 +346,19 @@ __global__ void __launch_bounds__(256)
     }
     out[blockIdx.x] = make_int4(lo, hi, p1 - p0, 0);
   }
+}
+
+// The blocks of a BSR instance, column-major (element (i, j) of block p at
+// p * bs * bs + j * bs + i), from either block layout.
+__global__ void k_bsr_colmajor(int64_t nnzb, int32_t bs, int rowmajor,
+                               const float *__restrict__ val, float *__restrict__ out) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t E = (int64_t)bs * bs;
+  if (e >= nnzb * E)
+    return;
+  const int64_t p = e / E;
+  const int32_t r = (int32_t)(e % E), j = r / bs, i = r % bs;
+  out[e] = val[p * E + (rowmajor ? (int64_t)i * bs + j : r)];
 }
 
 __global__ void k_pack_cv(int64_t nnz, const int32_t *__restrict__ col,
@@ -332,6 +416,7 @@ struct perflibs_b200_batch_s {
   pls::DevBuf inst, items, counter;
   pls::DevBuf packed;  // every instance's (column, value) pairs, packed at creation
   pls::DevBuf scalar_rp;  // row pointers of the BSR instances' scalar rows
+  pls::DevBuf bsr_cm;     // column-major copies of the blocks read as blocks (path 3)
   pls::DevBuf sitems;     // staged items, largest first
   // Per instance, the row ranges left to the per-warp items when staged
   // items are on (the blocks that were not staged).
@@ -415,7 +500,7 @@ void build_staged(Batch *B) {
     };
     if (d.m == 0)
       continue;
-    if (d.k < 1) {
+    if (d.k < 1 || d.path == 3) {  // BSR read as blocks: per-warp items only
       to_warps(0, d.m);
       continue;
     }
@@ -567,29 +652,56 @@ perflibs_status_t perflibs_b200_batch_create(perflibs_b200_batch_t *out, int32_t
       d.lg_tk = sh.lg_tk;
       d.lg_tn = sh.lg_tn;
       d.path = v4 ? 0 : (sh.nv == 2 ? 2 : 1);
+      if (d.is_bsr && (d.bs == 2 || d.bs == 4 || d.bs == 8) && k[i] > 0) {
+        // read as blocks: one column of C per lane, up to 32 lanes per block row
+        d.path = 3;
+        d.brp = d.rp;
+        d.lg_tk = 0;
+        while ((1 << d.lg_tk) < k[i] && d.lg_tk < 5)
+          ++d.lg_tk;
+        d.lg_tn = 0;
+      }
       // B has A->n rows of ldb, C has A->m rows of ldc
       if ((int64_t)A->n * ldb[i] >= INT32_MAX || (int64_t)A->m * ldc[i] >= INT32_MAX)
         B->off32 = false;
       B->host.push_back(d);
       B->work_per_row.push_back(((double)A->nnz / std::max(A->m, 1) + 1.0) * std::max(k[i], 1));
     }
-    // Every instance is read as scalar CSR rows whose column and value sit
-    // side by side (one 8-byte load per entry: each of a row's column lanes
-    // loads every entry, so these loads are a large share of the kernel's
-    // instructions); BSR instances are expanded to such rows here.
-    int64_t packed = 0, srows = 0;
+    // Every CSR instance, and every BSR instance not read as blocks, is read
+    // as scalar CSR rows whose column and value sit side by side (one 8-byte
+    // load per entry: each of a row's column lanes loads every entry, so
+    // these loads are a large share of the kernel's instructions); such BSR
+    // instances are expanded to scalar rows here. BSR instances read as
+    // blocks (path 3) get a column-major copy of their blocks instead.
+    int64_t packed = 0, srows = 0, cm = 0;
     for (int32_t i = 0; i < count; ++i) {
       const InstDesc &d = B->host[i];
-      packed += d.is_bsr ? mats[i]->bsr.nnzb * d.bs * d.bs : mats[i]->csr.nnz;
-      if (d.is_bsr)
+      if (d.path == 3)
+        cm += mats[i]->bsr.nnzb * d.bs * d.bs;
+      else
+        packed += d.is_bsr ? mats[i]->bsr.nnzb * d.bs * d.bs : mats[i]->csr.nnz;
+      if (d.is_bsr && d.path != 3)
         srows += (int64_t)d.m + 1;
     }
     B->packed.reserve(sizeof(int2) * std::max<int64_t>(packed, 1));
     B->scalar_rp.reserve(sizeof(int32_t) * std::max<int64_t>(srows, 1));
-    packed = srows = 0;
+    B->bsr_cm.reserve(sizeof(float) * std::max<int64_t>(cm, 1));
+    packed = srows = cm = 0;
     for (int32_t i = 0; i < count; ++i) {
       InstDesc &d = B->host[i];
       int2 *cv = B->packed.as<int2>() + packed;
+      if (d.path == 3) {
+        const BsrDev &b = mats[i]->bsr;
+        float *out = B->bsr_cm.as<float>() + cm;
+        const int64_t e = b.nnzb * b.bs * b.bs;
+        if (e > 0)
+          k_bsr_colmajor<<<(unsigned)div_up(e, 256), 256, 0, B->stream>>>(
+              b.nnzb, b.bs, d.layout == PERFLIBS_ROW_MAJOR, d.val, out);
+        d.val = out;
+        cm += e;
+        d.cv = nullptr;
+        continue;
+      }
       if (d.is_bsr) {
         const BsrDev &b = mats[i]->bsr;
         int32_t *srp = B->scalar_rp.as<int32_t>() + srows;
