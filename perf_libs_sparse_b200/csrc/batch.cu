@@ -52,6 +52,10 @@ struct InstDesc {
   int32_t m, k, bs, layout, is_bsr;  // bs / is_bsr: block-aligned items for BSR
   int32_t lg_tk, lg_tn, path;  // path: 0 = VEC 4, 1 = VEC 1 x 1, 2 = VEC 1 x 2, 3 = BSR blocks
   const int32_t *brp;  // BSR: the handle's block row pointers (path 3 reads the blocks)
+  // CSR with every row's columns consecutive (bands): the values alone, a
+  // copy made at creation; staged rows read them instead of the packed
+  // entries (null otherwise)
+  const float *band_val;
 };
 
 struct Item {
@@ -221,18 +225,44 @@ __device__ __forceinline__ void staged_item(const SItem &w, const InstDesc &d,
       acc.z = fmaf(a, b.z, acc.z);
       acc.w = fmaf(a, b.w, acc.w);
     };
-    int32_t q = s;
-    for (; q + 4 <= e; q += 4) {
-      int2 t[4];
+    if (d.band_val) {
+      // consecutive columns: the row's first column, then its values alone
+      // (4 bytes per entry), in stored order
+      if (s < e) {
+        const float4 *sp = st4 + (__ldg(d.cv + s).x - w.lo) * TK + tk;
+        const auto addv = [&](float a, const float4 b) {
+          acc.x = fmaf(a, b.x, acc.x);
+          acc.y = fmaf(a, b.y, acc.y);
+          acc.z = fmaf(a, b.z, acc.z);
+          acc.w = fmaf(a, b.w, acc.w);
+        };
+        int32_t q = s;
+        for (; q + 4 <= e; q += 4) {
+          float a[4];
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
-        t[u] = __ldg(d.cv + q + u);
+          for (int u = 0; u < 4; ++u)
+            a[u] = __ldg(d.band_val + q + u);
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
-        add(t[u]);
+          for (int u = 0; u < 4; ++u)
+            addv(a[u], sp[(q - s + u) * TK]);
+        }
+        for (; q < e; ++q)
+          addv(__ldg(d.band_val + q), sp[(q - s) * TK]);
+      }
+    } else {
+      int32_t q = s;
+      for (; q + 4 <= e; q += 4) {
+        int2 t[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          t[u] = __ldg(d.cv + q + u);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          add(t[u]);
+      }
+      for (; q < e; ++q)
+        add(__ldg(d.cv + q));
     }
-    for (; q < e; ++q)
-      add(__ldg(d.cv + q));
     float *crow = d.C + (int64_t)row * d.ldc + kk;
     const float sum[4] = {acc.x, acc.y, acc.z, acc.w};
     if (vec) {
@@ -348,6 +378,19 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Clears *flag when some row's columns are not consecutive.
+__global__ void k_rows_consecutive(int32_t m, const int32_t *__restrict__ rp,
+                                   const int32_t *__restrict__ col, int *__restrict__ flag) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= m)
+    return;
+  for (int32_t p = rp[r] + 1; p < rp[r + 1]; ++p)
+    if (col[p] != col[p - 1] + 1) {
+      atomicAnd(flag, 0);
+      return;
+    }
+}
+
 // The blocks of a BSR instance, column-major (element (i, j) of block p at
 // p * bs * bs + j * bs + i), from either block layout.
 __global__ void k_bsr_colmajor(int64_t nnzb, int32_t bs, int rowmajor,
@@ -417,6 +460,7 @@ struct perflibs_b200_batch_s {
   pls::DevBuf packed;  // every instance's (column, value) pairs, packed at creation
   pls::DevBuf scalar_rp;  // row pointers of the BSR instances' scalar rows
   pls::DevBuf bsr_cm;     // column-major copies of the blocks read as blocks (path 3)
+  pls::DevBuf band_vals;  // the values of the band instances (consecutive columns)
   pls::DevBuf sitems;     // staged items, largest first
   // Per instance, the row ranges left to the per-warp items when staged
   // items are on (the blocks that were not staged).
@@ -723,6 +767,45 @@ perflibs_status_t perflibs_b200_batch_create(perflibs_b200_batch_t *out, int32_t
       d.cv = cv;
     }
     PLS_LAUNCH_CHECK();
+    // Band instances: CSR rows of consecutive columns get a copy of their
+    // values alone, which their staged rows read.
+    {
+      DevBuf flags;
+      flags.reserve(sizeof(int) * (size_t)count);
+      std::vector<int> hf((size_t)count, 1);
+      PLS_CUDA(cudaMemcpyAsync(flags.p, hf.data(), sizeof(int) * count, cudaMemcpyHostToDevice,
+                               B->stream));
+      for (int32_t i = 0; i < count; ++i) {
+        const InstDesc &d = B->host[i];
+        if (!d.is_bsr && d.m > 0)
+          k_rows_consecutive<<<(unsigned)div_up(d.m, 256), 256, 0, B->stream>>>(
+              d.m, d.rp, d.col, flags.as<int>() + i);
+      }
+      PLS_LAUNCH_CHECK();
+      PLS_CUDA(cudaMemcpyAsync(hf.data(), flags.p, sizeof(int) * count, cudaMemcpyDeviceToHost,
+                               B->stream));
+      PLS_CUDA(cudaStreamSynchronize(B->stream));
+      int64_t nb = 0;
+      for (int32_t i = 0; i < count; ++i)
+        if (!B->host[i].is_bsr && hf[i])
+          nb += mats[i]->csr.nnz;
+      B->band_vals.reserve(sizeof(float) * std::max<int64_t>(nb, 1));
+      nb = 0;
+      for (int32_t i = 0; i < count; ++i) {
+        InstDesc &d = B->host[i];
+        d.band_val = nullptr;
+        if (d.is_bsr || !hf[i])
+          continue;
+        const int64_t nnz = mats[i]->csr.nnz;
+        float *out = B->band_vals.as<float>() + nb;
+        if (nnz > 0)
+          PLS_CUDA(cudaMemcpyAsync(out, d.val, sizeof(float) * nnz, cudaMemcpyDeviceToDevice,
+                                   B->stream));
+        d.band_val = out;
+        nb += nnz;
+      }
+      PLS_CUDA(cudaStreamSynchronize(B->stream));
+    }
     B->inst.reserve(sizeof(InstDesc) * count);
     PLS_CUDA(cudaMemcpyAsync(B->inst.p, B->host.data(), sizeof(InstDesc) * count,
                              cudaMemcpyHostToDevice, B->stream));
