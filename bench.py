@@ -542,7 +542,7 @@ def c4_config(args, timer, sp):
     b = sum(W.algorithmic_bytes_spmm(d["m"], d["n"], W.instance_nnz(d), d["k"], 4, 4, False) for d in inst)
     gbs = b / ms / 1e6
     si = bt.stage_info()
-    ktag = f"k_batch_spmm (BSR read as blocks) tile={tile} staging={bool(si.get('staging'))}"
+    ktag = f"k_batch_spmm (BSR blocks, band values) tile={tile} staging={bool(si.get('staging'))}"
     out = {"workload": "C4 512 uneven FP32 instances (banded / random / BSR bs 4-8), n in [1024, 65536], "
                        "k in [1, 64], one persistent launch per step",
            "value": gbs, "unit": "GB/s", "ms_per_step": ms, "steps": K, "max_rel_err": worst,
