@@ -219,3 +219,68 @@ def test_batch_staged_items_against_oracle_and_per_warp_items():
     assert best > 0 and ms > 0
     check(0.5, 2.0)
     bt.destroy()
+
+
+def test_batch_scattered_rows_unaligned_k_against_oracle():
+    """Scattered CSR instances whose k is not on 16-byte vectors (ldb or ldc
+    not a multiple of 4) read B by element: k = 17-64 one row at a time with
+    32 lanes over C's columns, k = 100 in two column passes, smaller k with
+    several rows per warp; an instance with aligned rows shares the batch.
+    Empty rows, ldb / ldc wider than k (padding columns untouched), items of
+    8 and 128 rows and the tuner's choice, beta != 0, and B changed in place
+    between two execs (the second sees it: B is read at exec, not copied)
+    all match the oracle."""
+    import torch
+
+    rng = np.random.default_rng(33)
+    mats, descs = [], []
+    for m, n, per_row, k, ldb, ldc in [(3000, 2500, 12, 5, 5, 5), (2000, 4000, 20, 7, 9, 8),
+                                       (1500, 1500, 6, 13, 13, 15), (2500, 3000, 18, 57, 57, 57),
+                                       (1000, 1200, 9, 3, 3, 3), (1800, 1800, 14, 20, 20, 20),
+                                       (1200, 900, 25, 33, 34, 33), (900, 1300, 30, 100, 101, 103),
+                                       (2100, 700, 40, 19, 19, 21), (600, 600, 1, 29, 29, 29)]:
+        rp, c, v = W.random_csr(m, n, per_row, rng, empty_frac=0.05)
+        v = v.astype(np.float32)
+        mats.append(pls.SpMat.csr(m, n, rp, c, v))
+        descs.append(dict(kind="csr", row_ptr=rp, col=c, vals=v, m=m, n=n, k=k, ldb=ldb, ldc=ldc))
+    Bs, Cs, C0s = [], [], []
+    for d in descs:
+        Bs.append(torch.tensor(rng.uniform(-1, 1, (d["n"], d["ldb"])).astype(np.float32), device="cuda"))
+        c0 = rng.uniform(-1, 1, (d["m"], d["ldc"])).astype(np.float32)
+        C0s.append(c0)
+        Cs.append(torch.tensor(c0, device="cuda"))
+    s = torch.cuda.Stream()
+    bt = pls.Batch(mats, [d["k"] for d in descs], [b.data_ptr() for b in Bs], [d["ldb"] for d in descs],
+                   [cm.data_ptr() for cm in Cs], [d["ldc"] for d in descs], stream=s.cuda_stream)
+    assert bt.info()["launches"] == 1
+
+    def check(alpha, beta, c_in):
+        bt.exec(alpha, beta)
+        s.synchronize()
+        outs = []
+        for d, b, cm, c0 in zip(descs, Bs, Cs, c_in):
+            k = d["k"]
+            ref, scale = _reference(dict(d, B=b.cpu().numpy()[:, :k]), alpha, beta, c0[:, :k].astype(np.float64))
+            got = cm.cpu().numpy()
+            den = np.maximum(np.abs(ref), scale)
+            den[den == 0] = 1
+            assert (np.abs(got[:, :k].astype(np.float64) - ref) / den).max() <= 1e-5, (d["m"], k)
+            np.testing.assert_array_equal(got[:, k:], c0[:, k:])
+            outs.append(got)
+        return outs
+
+    for tile in (8, 128, 0):
+        if tile:
+            bt.set_tile(tile)
+        else:
+            assert bt.tune()[0] > 0
+        for cm, c0 in zip(Cs, C0s):
+            cm.copy_(torch.tensor(c0, device="cuda"))
+        torch.cuda.synchronize()
+        c1 = check(1.25, -0.5, C0s)
+        with torch.cuda.stream(s):
+            for b in Bs:
+                b.mul_(-2.0).add_(0.25)
+        s.synchronize()
+        check(0.75, 1.0, c1)
+    bt.destroy()
