@@ -11,7 +11,8 @@ split, SELL-C-sigma C x sigma). This module:
    over the corpus fits a GPU session);
 2. for every matrix computes the features (perflibs_b200_spmat_features)
    and runs the exhaustive tuner (perflibs_spmv_optimize, tuner
-   EXHAUSTIVE) whose timing table is the label and the judge; progress is
+   EXHAUSTIVE) whose timing table is the label and the reference for
+   regret; progress is
    appended to a checkpoint file so an interrupted run resumes;
 3. trains the MLP with the library's CUDA kernels
    (perflibs_b200_selector_train) on the training split and reports, on the

@@ -68,7 +68,7 @@ def case_names(npz):
 def rel_err_rows(y, y_ref, scale):
     """Per-row error |y - y_ref| / max(|y_ref|, scale_i): the row scale is
     |alpha| * sum_j |a_ij x_j| + |beta| |y0_i|, the magnitude a summation-order
-    change can perturb, so cancelling rows are judged fairly."""
+    change can perturb, so cancelling rows are measured fairly."""
     den = np.maximum(np.abs(y_ref), scale)
     den = np.where(den == 0, 1.0, den)
     return np.abs(y - y_ref) / den

@@ -20,7 +20,7 @@ Outputs:
   (src/compressed_sparse_rows.cpp:1699-1764), BSR its CSR view
   (src/matmul.cpp:616-631).
 
-The GPU box never runs this script; tests read the fixtures.
+The tests never run this script; they read the fixtures.
 """
 from __future__ import annotations
 
