@@ -206,6 +206,9 @@ perflibs_status_t create_csr(Mat **out, int32_t m, int32_t n, const int32_t *row
   } catch (const Error &e) {
     *out = nullptr;
     return e.status;
+  } catch (...) {
+    *out = nullptr;
+    return PERFLIBS_STATUS_EXECUTION_FAILURE;
   }
   *out = A;
   return guarded(A, [&]() -> perflibs_status_t {
@@ -261,6 +264,9 @@ perflibs_status_t create_coo(Mat **out, int32_t m, int32_t n, int32_t nnz, const
   } catch (const Error &e) {
     *out = nullptr;
     return e.status;
+  } catch (...) {
+    *out = nullptr;
+    return PERFLIBS_STATUS_EXECUTION_FAILURE;
   }
   *out = A;
   return guarded(A, [&]() -> perflibs_status_t {
@@ -311,6 +317,9 @@ perflibs_status_t create_csc(Mat **out, int32_t m, int32_t n, const int32_t *row
   } catch (const Error &e) {
     *out = nullptr;
     return e.status;
+  } catch (...) {
+    *out = nullptr;
+    return PERFLIBS_STATUS_EXECUTION_FAILURE;
   }
   *out = A;
   return guarded(A, [&]() -> perflibs_status_t {
@@ -363,6 +372,9 @@ perflibs_status_t create_bsr(Mat **out, int layout, int32_t m, int32_t n, int32_
   } catch (const Error &e) {
     *out = nullptr;
     return e.status;
+  } catch (...) {
+    *out = nullptr;
+    return PERFLIBS_STATUS_EXECUTION_FAILURE;
   }
   *out = A;
   return guarded(A, [&]() -> perflibs_status_t {
@@ -414,6 +426,9 @@ perflibs_status_t create_dense(Mat **out, int layout, int32_t m, int32_t n, int3
   } catch (const Error &e) {
     *out = nullptr;
     return e.status;
+  } catch (...) {
+    *out = nullptr;
+    return PERFLIBS_STATUS_EXECUTION_FAILURE;
   }
   *out = A;
   return guarded(A, [&]() -> perflibs_status_t {
@@ -2112,7 +2127,7 @@ perflibs_status_t perflibs_b200_spmat_csr_to_bsr(perflibs_spmat_t A, int32_t bs,
     if (layout != PERFLIBS_ROW_MAJOR && layout != PERFLIBS_COL_MAJOR)
       return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
     DeviceGuard g(A->device);
-    Mat *B = new_mat(A->dt, Fmt::BSR);
+    std::unique_ptr<Mat> B(new_mat(A->dt, Fmt::BSR));  // freed if the conversion throws
     B->m = A->m;
     B->n = A->n;
     B->index_base = A->index_base;
@@ -2120,7 +2135,7 @@ perflibs_status_t perflibs_b200_spmat_csr_to_bsr(perflibs_spmat_t A, int32_t bs,
     csr_to_bsr(A->csr, A->m, A->n, bs, layout, B->bsr, stream_of(A));
     B->bsr.vt = A->csr.vt;
     B->nnz = B->bsr.nnzb * (int64_t)bs * bs;
-    *out = B;
+    *out = B.release();
     return PERFLIBS_STATUS_SUCCESS;
   });
 }
@@ -2174,6 +2189,9 @@ perflibs_status_t perflibs_b200_spmat_create_csr_d_dev(perflibs_spmat_t *out, in
   } catch (const Error &e) {
     *out = nullptr;
     return e.status;
+  } catch (...) {
+    *out = nullptr;
+    return PERFLIBS_STATUS_EXECUTION_FAILURE;
   }
   *out = A;
   return guarded(A, [&]() -> perflibs_status_t {

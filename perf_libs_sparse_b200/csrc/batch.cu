@@ -30,6 +30,7 @@
 #include <algorithm>
 #include <climits>
 #include <cstring>
+#include <memory>
 #include <numeric>
 #include <vector>
 
@@ -643,8 +644,10 @@ perflibs_status_t perflibs_b200_batch_create(perflibs_b200_batch_t *out, int32_t
                                              float *const *Cp, const int64_t *ldc, void *stream) {
   if (!out || count <= 0 || !mats || !k || !Bp || !ldb || !Cp || !ldc)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
-  try {
-    auto *B = new Batch;
+  *out = nullptr;
+  return status_guard([&]() -> perflibs_status_t {
+    std::unique_ptr<Batch> owner(new Batch);  // freed on every early return
+    Batch *B = owner.get();
     cudaGetDevice(&B->device);
     if (stream) {
       B->stream = (cudaStream_t)stream;
@@ -655,11 +658,8 @@ perflibs_status_t perflibs_b200_batch_create(perflibs_b200_batch_t *out, int32_t
     for (int32_t i = 0; i < count; ++i) {
       Mat *A = mats[i];
       if (!A || A->dt != Dt::F32 || k[i] < 0 || ldb[i] < k[i] || ldc[i] < k[i] ||
-          !(A->fmt == Fmt::CSR || A->fmt == Fmt::SELL || A->fmt == Fmt::BSR)) {
-        delete B;
-        *out = nullptr;
+          !(A->fmt == Fmt::CSR || A->fmt == Fmt::SELL || A->fmt == Fmt::BSR))
         return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
-      }
       InstDesc d{};
       d.B = Bp[i];
       d.C = Cp[i];
@@ -681,11 +681,8 @@ perflibs_status_t perflibs_b200_batch_create(perflibs_b200_batch_t *out, int32_t
         d.col = A->csr.col.as<int32_t>();
         d.val = A->csr.vals.as<float>();
       }
-      if (d.is_bsr && (int64_t)A->bsr.nnzb * d.bs * d.bs > INT32_MAX) {
-        delete B;
-        *out = nullptr;
+      if (d.is_bsr && (int64_t)A->bsr.nnzb * d.bs * d.bs > INT32_MAX)
         return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
-      }
       // Lane shape and vector width per instance: 16-byte vectors when k
       // fills at least one and its B and C rows are 16-byte aligned (one
       // vector tile per pass), else scalar columns with up to two per lane.
@@ -818,24 +815,19 @@ perflibs_status_t perflibs_b200_batch_create(perflibs_b200_batch_t *out, int32_t
         sizeof(float) * kStageFloats));
     B->grid = sms * std::max(per_sm, 1);
     build_items(B, 64);
-    *out = B;
+    *out = owner.release();
     return PERFLIBS_STATUS_SUCCESS;
-  } catch (const Error &e) {
-    *out = nullptr;
-    return e.status;
-  }
+  });
 }
 
 perflibs_status_t perflibs_b200_batch_set_tile(perflibs_b200_batch_t B, int32_t rows) {
   if (!B || rows < 0)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
-  try {
+  return status_guard([&] {
     if (rows > 0)
       build_items(B, rows);
     return PERFLIBS_STATUS_SUCCESS;
-  } catch (const Error &e) {
-    return e.status;
-  }
+  });
 }
 
 perflibs_status_t perflibs_b200_batch_tune(perflibs_b200_batch_t B, int32_t *best_tile,
@@ -843,10 +835,9 @@ perflibs_status_t perflibs_b200_batch_tune(perflibs_b200_batch_t B, int32_t *bes
   TraceRange trace("perflibs_b200_batch_tune");
   if (!B)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
-  try {
-    cudaEvent_t e0, e1;
-    PLS_CUDA(cudaEventCreate(&e0));
-    PLS_CUDA(cudaEventCreate(&e1));
+  return status_guard([&] {
+    const EventPair ev;
+    cudaEvent_t e0 = ev.e0, e1 = ev.e1;
     int32_t best = 64;
     bool best_staging = false;
     float bms = 1e30f;
@@ -875,8 +866,6 @@ perflibs_status_t perflibs_b200_batch_tune(perflibs_b200_batch_t B, int32_t *bes
         best_staging = staging;
       }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     B->staging = best_staging;
     build_items(B, best);
     if (best_tile)
@@ -884,21 +873,17 @@ perflibs_status_t perflibs_b200_batch_tune(perflibs_b200_batch_t B, int32_t *bes
     if (best_ms)
       *best_ms = bms;
     return PERFLIBS_STATUS_SUCCESS;
-  } catch (const Error &e) {
-    return e.status;
-  }
+  });
 }
 
 perflibs_status_t perflibs_b200_batch_set_staging(perflibs_b200_batch_t B, int32_t on) {
   if (!B)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
-  try {
+  return status_guard([&] {
     B->staging = on != 0;
     build_items(B, B->tile);
     return PERFLIBS_STATUS_SUCCESS;
-  } catch (const Error &e) {
-    return e.status;
-  }
+  });
 }
 
 perflibs_status_t perflibs_b200_batch_stage_info(perflibs_b200_batch_t B, int64_t *staged_items,
@@ -915,12 +900,10 @@ perflibs_status_t perflibs_b200_batch_stage_info(perflibs_b200_batch_t B, int64_
 perflibs_status_t perflibs_b200_batch_exec(perflibs_b200_batch_t B, float alpha, float beta) {
   if (!B)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
-  try {
+  return status_guard([&] {
     run(B, alpha, beta);
     return PERFLIBS_STATUS_SUCCESS;
-  } catch (const Error &e) {
-    return e.status;
-  }
+  });
 }
 
 perflibs_status_t perflibs_b200_batch_info(perflibs_b200_batch_t B, int64_t *n_items,

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -33,17 +34,14 @@ bool lower_eq(const char *a, const char *b) {
   return *a == *b;
 }
 
-}  // namespace
+struct FileCloser {
+  void operator()(FILE *f) const { std::fclose(f); }
+};
 
-extern "C" perflibs_status_t perflibs_b200_read_mtx(const char *path, int32_t *m, int32_t *n,
-                                                    int64_t *nnz, int32_t **row_ptr,
-                                                    int32_t **col_indx, double **vals) {
-  if (!path || !m || !n || !nnz || !row_ptr || !col_indx || !vals)
-    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
-  *row_ptr = nullptr;
-  *col_indx = nullptr;
-  *vals = nullptr;
-  FILE *f = std::fopen(path, "r");
+perflibs_status_t read_mtx_file(const char *path, int32_t *m, int32_t *n, int64_t *nnz,
+                                 int32_t **row_ptr, int32_t **col_indx, double **vals) {
+  std::unique_ptr<FILE, FileCloser> fh(std::fopen(path, "r"));  // closed on every exit
+  FILE *f = fh.get();
   if (!f)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
   std::vector<Entry> e;
@@ -88,7 +86,7 @@ extern "C" perflibs_status_t perflibs_b200_read_mtx(const char *path, int32_t *m
       break;
     st = PERFLIBS_STATUS_SUCCESS;
   } while (false);
-  std::fclose(f);
+  fh.reset();
   if (st != PERFLIBS_STATUS_SUCCESS)
     return st;
 
@@ -119,4 +117,24 @@ extern "C" perflibs_status_t perflibs_b200_read_mtx(const char *path, int32_t *m
   *col_indx = ci;
   *vals = vv;
   return PERFLIBS_STATUS_SUCCESS;
+}
+
+}  // namespace
+
+// A size line asking for more entries than host memory holds is an
+// execution failure, as is any other host allocation failure: no exception
+// leaves the C interface.
+extern "C" perflibs_status_t perflibs_b200_read_mtx(const char *path, int32_t *m, int32_t *n,
+                                                    int64_t *nnz, int32_t **row_ptr,
+                                                    int32_t **col_indx, double **vals) {
+  if (!path || !m || !n || !nnz || !row_ptr || !col_indx || !vals)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  *row_ptr = nullptr;
+  *col_indx = nullptr;
+  *vals = nullptr;
+  try {
+    return read_mtx_file(path, m, n, nnz, row_ptr, col_indx, vals);
+  } catch (...) {
+    return PERFLIBS_STATUS_EXECUTION_FAILURE;
+  }
 }

@@ -47,6 +47,19 @@ struct Error : std::runtime_error {
       : std::runtime_error(m), status(s) {}
 };
 
+// Runs f (which returns a status) so that no exception leaves a C entry
+// point: an Error gives its status, anything else (host allocation failure
+// included) EXECUTION_FAILURE.
+template <class F> perflibs_status_t status_guard(F &&f) noexcept {
+  try {
+    return f();
+  } catch (const Error &e) {
+    return e.status;
+  } catch (...) {
+    return PERFLIBS_STATUS_EXECUTION_FAILURE;
+  }
+}
+
 #define PLS_CUDA(call)                                                         \
   do {                                                                         \
     cudaError_t e_ = (call);                                                   \
@@ -58,6 +71,27 @@ struct Error : std::runtime_error {
   } while (0)
 
 #define PLS_LAUNCH_CHECK() PLS_CUDA(cudaGetLastError())
+
+// A pair of timing events, destroyed with the object, also when a timed run
+// throws.
+struct EventPair {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  EventPair() {
+    PLS_CUDA(cudaEventCreate(&e0));
+    const cudaError_t r = cudaEventCreate(&e1);
+    if (r != cudaSuccess) {
+      cudaEventDestroy(e0);
+      throw Error(PERFLIBS_STATUS_EXECUTION_FAILURE,
+                  std::string("cudaEventCreate: ") + cudaGetErrorString(r));
+    }
+  }
+  EventPair(const EventPair &) = delete;
+  EventPair &operator=(const EventPair &) = delete;
+  ~EventPair() {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+};
 
 // An NVTX range over a library call (optimize, host-pointer exec, SpMM,
 // batch tuning), visible in Nsight timelines; free when no tool listens.

@@ -256,8 +256,10 @@ perflibs_status_t perflibs_b200_selector_create(perflibs_b200_selector_t *out, i
                                                 uint64_t seed) {
   if (!out || K <= 0 || K > 4096)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
-  try {
-    auto *S = new Sel;
+  *out = nullptr;
+  Sel *S = nullptr;
+  const perflibs_status_t st = status_guard([&] {
+    S = new Sel;
     S->K = K;
     cudaGetDevice(&S->device);
     S->P = S->ob3() + K;
@@ -284,12 +286,14 @@ perflibs_status_t perflibs_b200_selector_create(perflibs_b200_selector_t *out, i
       h[S->oistd() + f] = 1.f;
     PLS_CUDA(cudaMemcpy(S->params.p, h.data(), 4 * S->Ptot, cudaMemcpyHostToDevice));
     PLS_CUDA(cudaDeviceSynchronize());  // legacy-stream copy, may still be in flight
-    *out = S;
     return PERFLIBS_STATUS_SUCCESS;
-  } catch (const Error &e) {
-    *out = nullptr;
-    return e.status;
+  });
+  if (st != PERFLIBS_STATUS_SUCCESS) {
+    perflibs_b200_selector_destroy(S);  // null, or what was made before the failure
+    return st;
   }
+  *out = S;
+  return PERFLIBS_STATUS_SUCCESS;
 }
 
 perflibs_status_t perflibs_b200_selector_destroy(perflibs_b200_selector_t S) {
@@ -330,7 +334,7 @@ perflibs_status_t perflibs_b200_selector_loss_grad(perflibs_b200_selector_t S, c
                                                    float *grad) {
   if (!S || !X || !T || n <= 0)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
-  try {
+  return status_guard([&]() -> perflibs_status_t {
     cudaStream_t s = S->stream;
     DevBuf xd, td;
     xd.reserve(4 * (size_t)n * NF);
@@ -347,9 +351,7 @@ perflibs_status_t perflibs_b200_selector_loss_grad(perflibs_b200_selector_t S, c
       PLS_CUDA(cudaMemcpyAsync(grad, S->grads.p, 4 * S->P, cudaMemcpyDeviceToHost, s));
     PLS_CUDA(cudaStreamSynchronize(s));
     return PERFLIBS_STATUS_SUCCESS;
-  } catch (const Error &e) {
-    return e.status;
-  }
+  });
 }
 
 perflibs_status_t perflibs_b200_selector_train(perflibs_b200_selector_t S, const float *X,
@@ -358,7 +360,7 @@ perflibs_status_t perflibs_b200_selector_train(perflibs_b200_selector_t S, const
                                                float *final_loss) {
   if (!S || !X || !T || n <= 0 || epochs <= 0 || batch <= 0)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
-  try {
+  return status_guard([&]() -> perflibs_status_t {
     cudaStream_t s = S->stream;
     const int K = S->K;
     const int B = std::min(batch, n);
@@ -437,16 +439,14 @@ perflibs_status_t perflibs_b200_selector_train(perflibs_b200_selector_t S, const
     }
     PLS_CUDA(cudaStreamSynchronize(s));
     return PERFLIBS_STATUS_SUCCESS;
-  } catch (const Error &e) {
-    return e.status;
-  }
+  });
 }
 
 perflibs_status_t perflibs_b200_selector_predict(perflibs_b200_selector_t S, const float *X,
                                                  int32_t n, float *probs, int32_t *cls) {
   if (!S || !X || n <= 0)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
-  try {
+  return status_guard([&]() -> perflibs_status_t {
     cudaStream_t s = S->stream;
     const int K = S->K;
     DevBuf xd;
@@ -466,9 +466,7 @@ perflibs_status_t perflibs_b200_selector_predict(perflibs_b200_selector_t S, con
         cls[i] = (int32_t)(std::max_element(p.begin() + (size_t)i * K, p.begin() + (size_t)(i + 1) * K) -
                            (p.begin() + (size_t)i * K));
     return PERFLIBS_STATUS_SUCCESS;
-  } catch (const Error &e) {
-    return e.status;
-  }
+  });
 }
 
 }  // extern "C"

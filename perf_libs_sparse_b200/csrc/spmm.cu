@@ -250,9 +250,8 @@ void spmm_csr(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
       DevBuf scratch;
       scratch.reserve(sizeof(X) * (size_t)m * k);
       X *sc = scratch.as<X>();
-      cudaEvent_t e0, e1;
-      PLS_CUDA(cudaEventCreate(&e0));
-      PLS_CUDA(cudaEventCreate(&e1));
+      const EventPair ev;
+      cudaEvent_t e0 = ev.e0, e1 = ev.e1;
       auto time2 = [&](auto &&run) {
         run();
         PLS_CUDA(cudaEventRecord(e0, s));
@@ -307,8 +306,6 @@ void spmm_csr(CsrDev &c, int32_t m, const X *B, int64_t ldb, X *C,
         if (mst < best)
           t.choice = 5;
       }
-      cudaEventDestroy(e0);
-      cudaEventDestroy(e1);
     }
     t.choice_sig = sig;
   }
@@ -594,9 +591,8 @@ void spmm_bsr(BsrDev &b, const X *B, int64_t ldb, X *C, int64_t ldc, int k, X al
           DevBuf scratch;
           scratch.reserve(sizeof(float) * (size_t)b.mb * b.bs * k);
           float *sc = scratch.as<float>();
-          cudaEvent_t e0, e1;
-          PLS_CUDA(cudaEventCreate(&e0));
-          PLS_CUDA(cudaEventCreate(&e1));
+          const EventPair ev;
+          cudaEvent_t e0 = ev.e0, e1 = ev.e1;
           auto time2 = [&](auto &&run) {
             run();
             PLS_CUDA(cudaEventRecord(e0, s));
@@ -610,8 +606,6 @@ void spmm_bsr(BsrDev &b, const X *B, int64_t ldb, X *C, int64_t ldc, int k, X al
           };
           b.ms_fma = time2([&] { spmm_bsr_fma<float>(b, B, ldb, sc, k, k, 1.f, 0.f, s); });
           b.ms_tc = time2([&] { spmm_bsr_tc(b, B, ldb, sc, k, k, 1.f, 0.f, s, true); });
-          cudaEventDestroy(e0);
-          cudaEventDestroy(e1);
           b.tc_choice = b.ms_tc < b.ms_fma ? 1 : 0;
           b.tc_sig = sig;
         }

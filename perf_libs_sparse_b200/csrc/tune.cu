@@ -104,9 +104,8 @@ double time_config(Mat *A, const SpmvConfig &cfg, int reps) {
   const int64_t xl = A->n, yl = A->m;
   DeviceScratch &sc = scratch(A->device);
   const bool flush = matrix_bytes(A) < (int64_t)(3 * sc.l2);
-  cudaEvent_t e0, e1;
-  PLS_CUDA(cudaEventCreate(&e0));
-  PLS_CUDA(cudaEventCreate(&e1));
+  const EventPair ev;
+  cudaEvent_t e0 = ev.e0, e1 = ev.e1;
   std::vector<float> t;
   auto run = [&]() {
     if (A->dt == Dt::F64) {
@@ -139,8 +138,6 @@ double time_config(Mat *A, const SpmvConfig &cfg, int reps) {
     PLS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
     t.push_back(ms);
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   std::sort(t.begin(), t.end());
   return t.empty() ? 0.0 : t[t.size() / 2];
 }

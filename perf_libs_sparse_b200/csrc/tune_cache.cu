@@ -136,15 +136,23 @@ void tune_cache_put(const TuneKey &key, const SpmvConfig &best,
 
 using namespace pls;
 
-extern "C" {
+namespace {
 
-perflibs_status_t perflibs_b200_tune_cache_save(const char *path) {
-  if (!path)
-    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+// Closes the file if a write or read throws (host allocation failure).
+struct CloseOnThrow {
+  FILE *f;
+  ~CloseOnThrow() {
+    if (f)
+      std::fclose(f);
+  }
+};
+
+perflibs_status_t save_cache(const char *path) {
   std::lock_guard<std::mutex> g(g_mu);
   FILE *f = std::fopen(path, "w");
   if (!f)
     return PERFLIBS_STATUS_EXECUTION_FAILURE;
+  CloseOnThrow closer{f};
   bool ok = std::fprintf(f, "%s %d %zu\n", kMagic, kVersion, g_cache.size()) > 0;
   for (const auto &kv : g_cache) {
     const TuneKey &k = kv.first;
@@ -157,19 +165,16 @@ perflibs_status_t perflibs_b200_tune_cache_save(const char *path) {
       ok = ok && std::fprintf(f, "%d %d %d %d %.9g %.9g\n", (int)t.cfg.kind, t.cfg.C,
                               t.cfg.sigma, t.cfg.tpr, t.ms, t.beta) > 0;
   }
+  closer.f = nullptr;
   ok = (std::fclose(f) == 0) && ok;
   return ok ? PERFLIBS_STATUS_SUCCESS : PERFLIBS_STATUS_EXECUTION_FAILURE;
 }
 
-// Merges the file's entries into the cache (an entry replaces one with the
-// same key). A file that is not a cache of this version, or is cut short or
-// malformed anywhere, changes nothing and is an input error.
-perflibs_status_t perflibs_b200_tune_cache_load(const char *path) {
-  if (!path)
-    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+perflibs_status_t load_cache(const char *path) {
   FILE *f = std::fopen(path, "r");
   if (!f)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  CloseOnThrow closer{f};
   std::map<TuneKey, Entry> read;
   char magic[64] = {0};
   int version = 0;
@@ -202,6 +207,7 @@ perflibs_status_t perflibs_b200_tune_cache_load(const char *path) {
     if (ok)
       read[k] = std::move(e);
   }
+  closer.f = nullptr;
   std::fclose(f);
   if (!ok)
     return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
@@ -209,6 +215,25 @@ perflibs_status_t perflibs_b200_tune_cache_load(const char *path) {
   for (auto &kv : read)
     g_cache[kv.first] = std::move(kv.second);
   return PERFLIBS_STATUS_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" {
+
+perflibs_status_t perflibs_b200_tune_cache_save(const char *path) {
+  if (!path)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  return status_guard([&] { return save_cache(path); });
+}
+
+// Merges the file's entries into the cache (an entry replaces one with the
+// same key). A file that is not a cache of this version, or is cut short or
+// malformed anywhere, changes nothing and is an input error.
+perflibs_status_t perflibs_b200_tune_cache_load(const char *path) {
+  if (!path)
+    return PERFLIBS_STATUS_INPUT_PARAMETER_ERROR;
+  return status_guard([&] { return load_cache(path); });
 }
 
 perflibs_status_t perflibs_b200_tune_cache_clear(void) {

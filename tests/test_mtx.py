@@ -82,6 +82,9 @@ def test_read_mtx_keeps_duplicates_and_rectangular(tmp_path):
     "%%MatrixMarket matrix coordinate real general\n2 2 1\n3 1 1.0\n",
     "%%MatrixMarket matrix coordinate real general\n2 2 2\n1 1 1.0\n",
     "not a matrix market file\n",
+    # more entries than any host can hold: the allocation fails inside the
+    # library and comes back as a status, not as an exception
+    "%%MatrixMarket matrix coordinate real general\n2 2 4000000000000000000\n1 1 1.0\n",
 ])
 def test_read_mtx_rejects_bad_files(tmp_path, text):
     path = tmp_path / "bad.mtx"
