@@ -502,17 +502,14 @@ SPMM_PATHS = {-1: "none", 0: "row group", 1: "staged", 2: "row group, shared ent
               3: "diagonal form", 4: "diagonal form, TMA-staged B", 5: "BSR tensor core"}
 
 
-def c4_config(args, timer, sp):
-    """C4: 512 uneven FP32 SpMMs (banded, random uniform and BSR
-    block-diagonal instances, n in [1024, 65536], k in [1, 64], seed 3) in
-    one persistent launch, replayed as a CUDA graph; tile schedule from the
-    batch autotuner. A step is one batch launch (2.9 GB, beyond L2)."""
+def make_batch(inst, sp):
+    """A batch over `inst` (dicts of workloads.batched_instances): the
+    handles, B on the device, C zeroed, one stream. Returns (batch, handles,
+    B tensors, C tensors)."""
     import torch
 
-    import oracle
     import perf_libs_sparse_b200 as pls
 
-    inst = W.batched_instances(512, seed=3)
     mats, Bs, Cs = [], [], []
     for d in inst:
         if d["kind"] == "bsr":
@@ -523,6 +520,52 @@ def c4_config(args, timer, sp):
         Cs.append(torch.zeros((d["m"], d["k"]), dtype=torch.float32, device="cuda"))
     ks = [d["k"] for d in inst]
     bt = pls.Batch(mats, ks, [b_.data_ptr() for b_ in Bs], ks, [c_.data_ptr() for c_ in Cs], ks, stream=sp)
+    return bt, mats, Bs, Cs
+
+
+def c4_kinds_config(args, timer, sp):
+    """C4's 512 instances split by kind, each part batched alone and tuned:
+    banded, random (also by k: <= 4, 5-16, > 16), BSR, then all 512. A part
+    alone holds less than the full step's bytes, so more of it stays in L2;
+    the parts show where the full step's time goes."""
+    import torch
+
+    inst = W.batched_instances(512, seed=3)
+    rnd = [d for d in inst if d["kind"] == "csr" and "band" not in d]
+    parts = [("banded", [d for d in inst if "band" in d]), ("random", rnd),
+             ("random k <= 4", [d for d in rnd if d["k"] <= 4]),
+             ("random 4 < k <= 16", [d for d in rnd if 4 < d["k"] <= 16]),
+             ("random k > 16", [d for d in rnd if d["k"] > 16]),
+             ("bsr", [d for d in inst if d["kind"] == "bsr"]), ("all", inst)]
+    out = {"workload": "C4's 512 instances by kind, each part batched alone and tuned", "parts": []}
+    for name, sel in parts:
+        bt, mats, Bs, Cs = make_batch(sel, sp)
+        tile, _ = bt.tune()
+        ms = timer(lambda: bt.exec(1.0, 0.0), max(args.steps, 10), max(args.warmup, 3))
+        torch.cuda.synchronize()
+        b = sum(W.algorithmic_bytes_spmm(d["m"], d["n"], W.instance_nnz(d), d["k"], 4, 4, False) for d in sel)
+        out["parts"].append({"part": name, "instances": len(sel), "ms_per_step": ms, "value": b / ms / 1e6,
+                             "unit": "GB/s", "algorithmic_bytes_per_step": b,
+                             "multiply_adds": int(sum(W.instance_nnz(d) * d["k"] for d in sel)),
+                             "tile_rows": tile, **bt.stage_info()})
+        bt.destroy()
+        for A in mats:
+            A.destroy()
+        del Bs, Cs
+    return out
+
+
+def c4_config(args, timer, sp):
+    """C4: 512 uneven FP32 SpMMs (banded, random uniform and BSR
+    block-diagonal instances, n in [1024, 65536], k in [1, 64], seed 3) in
+    one persistent launch, replayed as a CUDA graph; tile schedule from the
+    batch autotuner. A step is one batch launch (2.9 GB, beyond L2)."""
+    import torch
+
+    import oracle
+
+    inst = W.batched_instances(512, seed=3)
+    bt, mats, Bs, Cs = make_batch(inst, sp)
     tile, _ = bt.tune()
     K = max(args.steps, 10)
     ms = timer(lambda: bt.exec(1.0, 0.0), K, max(args.warmup, 3), timed_label(args))
@@ -832,7 +875,8 @@ def run_b200(args):
 
 def run_extra(args):
     """One configuration alone, as its own JSON line (N = 1): c1, c3 (k =
-    --k, storage --storage), c4, c3spmv (FP64 SpMV, tuned, on C3's
+    --k, storage --storage), c4, c4kinds (C4's instance kinds batched
+    apart), c3spmv (FP64 SpMV, tuned, on C3's
     matrix: the structured counterpart of C2), lap2d (FP64 SpMV, tuned, on
     the 5-point Laplacian 4096^2) or c2local (C2's row lengths
     with every column drawn from 8192, so that x's gathers hit L1: what the
@@ -854,6 +898,8 @@ def run_extra(args):
         sub = c3_config(args, timer, sp, [(args.k, args.storage)])["arms"][0]
     elif args.workload == "c4":
         sub = c4_config(args, timer, sp)
+    elif args.workload == "c4kinds":
+        sub = c4_kinds_config(args, timer, sp)
     else:
         if args.workload == "c2local":
             # C2's row lengths and uniform random columns, drawn from 8192
@@ -920,7 +966,7 @@ def emit(line, args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="c2",
-                    choices=["c1", "c2", "c3", "c3spmv", "c2local", "lap2d", "c4", "bsr8"],
+                    choices=["c1", "c2", "c3", "c3spmv", "c2local", "lap2d", "c4", "c4kinds", "bsr8"],
                     help="c2 (default: the headline line, with c1 / c3 / c4 inside it) or one "
                          "configuration alone")
     ap.add_argument("--k", type=int, default=32, help="right-hand sides for --workload c3")
