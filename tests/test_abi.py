@@ -111,3 +111,37 @@ def test_reference_driver_links_against_drop_in():
         pytest.skip("reference sources not present")
     assert r.returncode == 0, r.stdout + r.stderr
     assert os.path.exists(os.path.join(here, "oracle", "_build", "ref_driver_on_b200"))
+
+
+def test_extension_entry_points_reject_missing_arguments_on_the_host():
+    """Missing handles, output pointers and paths are input errors returned
+    before any device work, so they behave the same with or without a GPU;
+    a tune-cache file that does not exist changes nothing."""
+    L = ctypes.CDLL(pls.LIB_PATH)
+    v, i32, i64, f32 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_float
+    L.perflibs_b200_batch_create.argtypes = [v, i32, v, v, v, v, v, v, v]
+    L.perflibs_b200_batch_exec.argtypes = [v, f32, f32]
+    L.perflibs_b200_batch_tune.argtypes = [v, v, v]
+    L.perflibs_b200_batch_set_tile.argtypes = [v, i32]
+    L.perflibs_b200_batch_info.argtypes = [v, v, v, v]
+    L.perflibs_b200_selector_create.argtypes = [v, i32, ctypes.c_uint64]
+    L.perflibs_b200_selector_predict.argtypes = [v, v, i32, v, v]
+    L.perflibs_b200_tune_cache_load.argtypes = [ctypes.c_char_p]
+    L.perflibs_b200_tune_cache_save.argtypes = [ctypes.c_char_p]
+    L.perflibs_b200_read_mtx.argtypes = [ctypes.c_char_p, v, v, v, v, v, v]
+    L.perflibs_b200_tune_cache_size.restype = i64
+    bad = pls.STATUS_INPUT_PARAMETER_ERROR
+    out = v()
+    assert L.perflibs_b200_batch_create(None, 1, None, None, None, None, None, None, None) == bad
+    assert L.perflibs_b200_batch_create(ctypes.byref(out), 0, None, None, None, None, None, None, None) == bad
+    assert L.perflibs_b200_batch_exec(None, 1.0, 0.0) == bad
+    assert L.perflibs_b200_batch_tune(None, None, None) == bad
+    assert L.perflibs_b200_batch_set_tile(None, 8) == bad
+    assert L.perflibs_b200_batch_info(None, None, None, None) == bad
+    assert L.perflibs_b200_selector_create(ctypes.byref(out), 0, 1) == bad
+    assert L.perflibs_b200_selector_predict(None, None, 1, None, None) == bad
+    n0 = L.perflibs_b200_tune_cache_size()
+    assert L.perflibs_b200_tune_cache_load(b"/nonexistent/dir/cache.txt") == bad
+    assert L.perflibs_b200_tune_cache_size() == n0
+    assert L.perflibs_b200_tune_cache_save(None) == bad
+    assert L.perflibs_b200_read_mtx(None, None, None, None, None, None, None) == bad
