@@ -35,3 +35,14 @@ def test_reference_arm_line():
     e2e = line["e2e"]
     assert e2e["value"] == line["value"] and e2e["h2d_bytes_per_step"] == 0
     assert e2e["d2h_bytes_per_step"] == 0
+
+
+def test_reference_arm_other_ranks_exit_without_work():
+    """Under torchrun the reference arm runs on rank 0 alone: any other rank
+    exits 0 at once and prints no result line."""
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                        "--gpus", "2", "--steps", "1", "--warmup", "1"],
+                       capture_output=True, text=True, timeout=300, cwd=ROOT, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert not [l for l in r.stdout.splitlines() if l.startswith("{")]
